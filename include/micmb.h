@@ -1,0 +1,330 @@
+/*
+ * micmb.h -- C ABI of the B200-native Rosenbrock chemistry solver.
+ *
+ * Plain C types only (pointers, sizes, doubles, 32/64-bit integers): this is
+ * the boundary a Fortran/C/Python host or micm's own C++ layer binds to.  No
+ * exceptions cross it; every call returns MICMB_OK (0) or a negative status
+ * and micmb_last_error() gives the message of the last failure on the calling
+ * thread.
+ *
+ * Each entry point names the micm (NCAR/micm 3.13.0) interface it replaces.
+ * Paths are relative to the micm source tree.
+ *
+ * Data layout at the boundary is micm's own vector ordering with L cells per
+ * group (include/micm/util/vector_matrix.hpp:254-345): element (cell c,
+ * column j) of an n-column dense matrix lives at
+ *     (c / L) * L * n + j * L + c % L
+ * and element e of the LU-filled sparse Jacobian at
+ *     (c / L) * L * nnz + e * L + c % L
+ * (sparse_matrix_vector_ordering_compressed_sparse_row.hpp:79-88), with the
+ * nonzeros in row-major order.  Columns of `variables` follow micm's species
+ * map after Markowitz reordering, columns of `rate_constants` follow micm's
+ * reaction order after the stable sort by rate-constant type, exactly as the
+ * reference solver numbers them.
+ */
+#ifndef MICMB_H
+#define MICMB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* status codes                                                        */
+/* ------------------------------------------------------------------ */
+#define MICMB_OK 0
+#define MICMB_ERR_INVALID_ARGUMENT (-1)
+#define MICMB_ERR_CUDA (-2)
+#define MICMB_ERR_UNSUPPORTED (-3)
+#define MICMB_ERR_OUT_OF_MEMORY (-4)
+#define MICMB_ERR_INTERNAL (-5)
+#define MICMB_ERR_NO_DEVICE (-6)
+#define MICMB_ERR_TIMEOUT (-7)
+
+/* micm::SolverState values (include/micm/solver/solver_result.hpp:13-35) */
+#define MICMB_SOLVER_NOT_YET_CALLED 0
+#define MICMB_SOLVER_RUNNING 1
+#define MICMB_SOLVER_CONVERGED 2
+#define MICMB_SOLVER_CONVERGENCE_EXCEEDED_MAX_STEPS 3
+#define MICMB_SOLVER_STEP_SIZE_TOO_SMALL 4
+#define MICMB_SOLVER_REPEATEDLY_SINGULAR_MATRIX 5
+#define MICMB_SOLVER_NAN_DETECTED 6
+#define MICMB_SOLVER_INF_DETECTED 7
+
+/* ------------------------------------------------------------------ */
+/* mechanism description                                               */
+/* ------------------------------------------------------------------ */
+
+/* Rate-constant kinds; the numeric value is micm's sort key
+ * (include/micm/solver/solver_builder.inl:274-329). */
+#define MICMB_RATE_ARRHENIUS 0
+#define MICMB_RATE_TROE 1
+#define MICMB_RATE_TERNARY_CHEMICAL_ACTIVATION 2
+#define MICMB_RATE_BRANCHED 3
+#define MICMB_RATE_TUNNELING 4
+#define MICMB_RATE_TAYLOR_SERIES 5
+#define MICMB_RATE_REVERSIBLE 6
+#define MICMB_RATE_USER_DEFINED 7
+#define MICMB_RATE_SURFACE 8
+
+/* doubles per reaction in micmb_mechanism_desc::rate_params */
+#define MICMB_RATE_PARAM_STRIDE 24
+/* maximum parameterized reactants per reaction
+ * (include/micm/process/reaction_rate_store.hpp:57-76, kMaxFuncs) */
+#define MICMB_MAX_PARAMETERIZED 4
+
+/*
+ * A chemical mechanism in flat form.  Species are numbered 0..n_species-1 in
+ * the order of micm's gas phase (System::UniqueNames,
+ * include/micm/system/system.hpp:38-63).  Reactions are numbered
+ * 0..n_reactions-1 in the order given to SolverBuilder::SetReactions.
+ *
+ * rate_params[r * MICMB_RATE_PARAM_STRIDE + i] by rate_type[r]:
+ *   ARRHENIUS   A, B, C, D, E             (arrhenius_rate_constant.hpp:9-22)
+ *   TROE        k0_A k0_B k0_C kinf_A kinf_B kinf_C Fc N (troe_rate_constant.hpp)
+ *   TERNARY_CHEMICAL_ACTIVATION  same eight as TROE
+ *   BRANCHED    branch(0 alkoxy, 1 nitrate), X, Y, a0, n
+ *   TUNNELING   A, B, C
+ *   TAYLOR_SERIES A, B, C, D, E, n_coefficients, c0 .. c15
+ *   REVERSIBLE  A, C, k_r
+ *   USER_DEFINED scaling_factor            (one custom rate parameter)
+ *   SURFACE     diffusion_coefficient [m2 s-1], molecular_weight [kg mol-1],
+ *               reaction_probability       (two custom rate parameters)
+ *
+ * reactant_species[i] >= 0 is a species index; a value -(p+1) names
+ * parameterized reactant p whose concentration is
+ *   c0 + cT*T + cP*P + crho*air_density   (parameterized_function.hpp)
+ * with coefficients parameterized_coef[4p .. 4p+3].
+ */
+typedef struct micmb_mechanism_desc {
+  int32_t n_species;
+  int32_t n_reactions;
+  const int32_t* rate_type;        /* [n_reactions] */
+  const double* rate_params;       /* [n_reactions * MICMB_RATE_PARAM_STRIDE] */
+  const int32_t* reactant_start;   /* [n_reactions + 1] */
+  const int32_t* reactant_species; /* [reactant_start[n_reactions]] */
+  const int32_t* product_start;    /* [n_reactions + 1] */
+  const int32_t* product_species;  /* [product_start[n_reactions]] */
+  const double* product_yield;     /* [product_start[n_reactions]] */
+  int32_t n_parameterized;
+  const double* parameterized_coef; /* [4 * n_parameterized] */
+  int32_t reorder_state;            /* SolverBuilder::SetReorderState, default 1 */
+} micmb_mechanism_desc;
+
+/* Rosenbrock tableau and step control
+ * (include/micm/solver/rosenbrock_solver_parameters.hpp:22-67). */
+typedef struct micmb_rosenbrock_params {
+  int32_t stages;
+  int32_t max_number_of_steps;
+  double round_off;
+  double factor_min;
+  double factor_max;
+  double rejection_factor_decrease;
+  double safety_factor;
+  double h_min;
+  double h_max;
+  double h_start;
+  int32_t new_function_evaluation[6];
+  double estimator_of_local_order;
+  double a[15];
+  double c[15];
+  double m[6];
+  double e[6];
+  double alpha[6];
+  double gamma[6];
+} micmb_rosenbrock_params;
+
+/* micm::SolverStats (include/micm/solver/solver_result.hpp:37-57), summed
+ * over cells in per-cell step control. */
+typedef struct micmb_solver_stats {
+  int64_t function_calls;
+  int64_t jacobian_updates;
+  int64_t number_of_steps;
+  int64_t accepted;
+  int64_t rejected;
+  int64_t decompositions;
+  int64_t solves;
+  double final_time;
+  int32_t state; /* MICMB_SOLVER_*: worst over cells in per-cell mode */
+  int32_t cells_not_converged;
+} micmb_solver_stats;
+
+typedef struct micmb_mechanism_info {
+  int32_t n_species;
+  int32_t n_reactions;
+  int32_t n_custom_params;
+  int32_t jacobian_nnz;       /* LU-filled nonzeros per cell */
+  int32_t jacobian_nnz_unfilled;
+  int32_t lu_updates;         /* a_jk -= a_ji * a_ik terms per factorisation */
+  int32_t lu_lower;           /* multipliers a_ji per factorisation */
+  int32_t n_jacobian_terms;   /* product/reactant contributions to -J */
+  int32_t n_forcing_terms;
+  int32_t n_jacobian_infos;   /* (independent species, process) pairs */
+  int32_t lu_levels;
+  int32_t forward_levels;
+  int32_t backward_levels;
+} micmb_mechanism_info;
+
+typedef struct micmb_mechanism micmb_mechanism;
+typedef struct micmb_solver micmb_solver;
+typedef struct micmb_state micmb_state;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* micmb_last_error(void);
+
+/* Symbolic compile of a mechanism: reaction sort by rate type, Markowitz
+ * species order, Jacobian sparsity with diagonal, LU fill and the level
+ * schedules of every kernel.  Host only, needs no GPU.
+ * Replaces SolverBuilder::Build (include/micm/solver/solver_builder.inl:227-548),
+ * DiagonalMarkowitzReorder (include/micm/solver/linear_solver.inl:30-124),
+ * ProcessSet ctor (include/micm/process/process_set.hpp:256-422),
+ * LuDecompositionMozartInPlace::Initialize/GetLUMatrix
+ * (include/micm/solver/lu_decomposition_mozart_in_place.inl:60-169). */
+int micmb_mechanism_create(const micmb_mechanism_desc* desc, micmb_mechanism** out);
+void micmb_mechanism_destroy(micmb_mechanism* mech);
+int micmb_mechanism_get_info(const micmb_mechanism* mech, micmb_mechanism_info* out);
+/* column of each system species in `variables` (micm State::variable_map_) */
+int micmb_mechanism_species_columns(const micmb_mechanism* mech, int32_t* out /*[n_species]*/);
+/* column of each input reaction in `rate_constants` */
+int micmb_mechanism_reaction_columns(const micmb_mechanism* mech, int32_t* out /*[n_reactions]*/);
+/* first custom-parameter column of each input reaction, -1 if it has none
+ * (SolverBuilder::GetCustomParameterMap, solver_builder.inl:129-188) */
+int micmb_mechanism_custom_param_columns(const micmb_mechanism* mech, int32_t* out /*[n_reactions]*/);
+/* LU-filled sparsity in storage order (row-major), in state columns */
+int micmb_mechanism_jacobian_pattern(const micmb_mechanism* mech, int32_t* rows, int32_t* cols);
+/* the unfilled Jacobian sparsity (ProcessSet::NonZeroJacobianElements + diagonal) */
+int micmb_mechanism_jacobian_pattern_unfilled(const micmb_mechanism* mech, int32_t* rows, int32_t* cols);
+/* 64-bit FNV-1a hash of the compiled tables (autotuner cache key) */
+uint64_t micmb_mechanism_hash(const micmb_mechanism* mech);
+
+/* Rosenbrock tableaus, identical to RosenbrockSolverParameters::*Parameters()
+ * (rosenbrock_solver_parameters.hpp:152-434): stages 2, 3, 4 (L-stable
+ * order 4), 40 (4-stage DAE variant), 60 (6-stage DAE variant). */
+int micmb_rosenbrock_params_default(int32_t kind, micmb_rosenbrock_params* out);
+
+/* Device: the solver uploads the mechanism tables to the current CUDA device.
+ * Replaces CudaProcessSet::InitDevStruct / CopyConstData
+ * (include/micm/cuda/process/cuda_process_set.hpp:141-157, src/process/process_set.cu:154-227),
+ * CudaLuDecompositionMozartInPlace and CudaLinearSolverInPlace ctors
+ * (include/micm/cuda/solver/cuda_lu_decomposition_mozart_in_place.hpp:12-96,
+ *  include/micm/cuda/solver/cuda_linear_solver_in_place.hpp:51-84). */
+int micmb_solver_create(const micmb_mechanism* mech, const micmb_rosenbrock_params* params,
+                        micmb_solver** out);
+void micmb_solver_destroy(micmb_solver* solver);
+int micmb_solver_set_params(micmb_solver* solver, const micmb_rosenbrock_params* params);
+/* per-reaction multiplicative scale of the rate constant, in input reaction
+ * order (1.0 = as given).  d(log k)/d(log scale) = 1, so gradients reported
+ * by micmb_solve_adjoint are also d loss / d log(scale). */
+int micmb_solver_set_rate_scale(micmb_solver* solver, const double* scale /*[n_reactions]*/);
+
+/* Device state for n_cells grid cells with vector length L.
+ * Replaces Solver::GetState / CudaState ctor
+ * (include/micm/solver/solver.hpp:174-195, include/micm/cuda/solver/cuda_state.hpp:40-78). */
+int micmb_state_create(micmb_solver* solver, int64_t n_cells, int32_t vector_length,
+                       micmb_state** out);
+void micmb_state_destroy(micmb_state* state);
+/* run this state's work on `stream` (a cudaStream_t); NULL restores the
+ * state's own stream. */
+int micmb_state_set_stream(micmb_state* state, void* stream);
+int micmb_state_synchronize(micmb_state* state);
+
+/* Host <-> device copies, all in micm's vector layout of the state's L.
+ * variables: CudaState::SyncInputsToDevice / SyncOutputsToHost
+ * (include/micm/cuda/solver/cuda_state.hpp:132-148). */
+#define MICMB_BUF_VARIABLES 0
+#define MICMB_BUF_CUSTOM_PARAMS 1
+#define MICMB_BUF_RATE_CONSTANTS 2
+#define MICMB_BUF_JACOBIAN 3
+#define MICMB_BUF_CONDITIONS 4 /* 3 columns: temperature, pressure, air density */
+#define MICMB_BUF_ABSOLUTE_TOLERANCE 5 /* [n_species], one per column */
+#define MICMB_BUF_FORCING 6    /* initial forcing scratch, n_species columns */
+#define MICMB_BUF_SCRATCH_Y 7  /* Ynew scratch, n_species columns */
+int micmb_state_upload(micmb_state* state, int32_t buffer, const double* host);
+int micmb_state_download(micmb_state* state, int32_t buffer, double* host);
+/* device pointer and element count of a state buffer (zero-copy interop) */
+int micmb_state_device_buffer(micmb_state* state, int32_t buffer, double** ptr, int64_t* count);
+int micmb_state_set_relative_tolerance(micmb_state* state, double rtol);
+
+/* Rate constants on the GPU from conditions and custom parameters.
+ * Replaces Solver::UpdateStateParameters -> CudaProcessSet::GpuCalculateRateConstants
+ * (include/micm/solver/solver.hpp:217-247, include/micm/cuda/process/cuda_process_set.hpp:88-114,
+ *  src/process/cuda_rate_constant_kernel.cu:97-170). */
+int micmb_update_state_parameters(micmb_solver* solver, micmb_state* state);
+
+/* Step control: one step size for all cells (micm's own semantics,
+ * rosenbrock.inl:353-402) or an independent adaptive solve per cell. */
+#define MICMB_STEP_GLOBAL 0
+#define MICMB_STEP_PER_CELL 1
+/* Methods: one kernel per stage over all cells, or one persistent kernel. */
+#define MICMB_METHOD_PLAIN 0
+#define MICMB_METHOD_FUSED 1
+
+/* Solve(time_step, state): advance every cell by dt and clamp at zero.
+ * Replaces Solver::Solve -> AbstractRosenbrockSolver::Solve and
+ * Solver::PostSolveClamp (include/micm/solver/solver.hpp:133-142, 275-297,
+ * include/micm/solver/rosenbrock.inl:12-304).  per_cell_status (device
+ * results copied to host, may be NULL) receives MICMB_SOLVER_* per cell and
+ * per_cell_steps the accepted-step count per cell. */
+int micmb_solve(micmb_solver* solver, micmb_state* state, double dt, int32_t method,
+                int32_t step_control, micmb_solver_stats* stats, int32_t* per_cell_status,
+                int32_t* per_cell_accepted);
+
+/* Fused-kernel launch configuration (autotuner knobs). */
+typedef struct micmb_fused_config {
+  int32_t cells_per_cta;   /* warps (one cell each) per CTA */
+  int32_t lu_in_shared;    /* 1: LU staged in shared memory, 0: streamed through global */
+  int32_t ctas_per_sm;     /* persistent grid = ctas_per_sm * SM count (0 = occupancy) */
+} micmb_fused_config;
+int micmb_solver_set_fused_config(micmb_solver* solver, const micmb_fused_config* config);
+int micmb_solver_get_fused_config(micmb_solver* solver, micmb_fused_config* config);
+/* Time candidate fused configurations on this state (its current inputs are
+ * preserved) and keep the fastest; the choice is cached in `cache_path`
+ * (may be NULL) under the mechanism hash. */
+int micmb_autotune(micmb_solver* solver, micmb_state* state, double dt, const char* cache_path,
+                   micmb_fused_config* chosen);
+
+/* CUDA-graph replay of repeated Solve calls with the fused method: captures
+ * UpdateStateParameters + Solve once per (state, dt) and replays it. */
+int micmb_solve_graph(micmb_solver* solver, micmb_state* state, double dt, int32_t n_repeats);
+
+/* Discrete adjoint of the accepted Rosenbrock steps of one per-cell solve
+ * (no counterpart in micm).  Runs the forward solve from the current
+ * variables, checkpoints every accepted step, then sweeps back.
+ *   dloss_dy_final: [vector layout, n_species columns] dL/d(final clamped y)
+ *   dloss_dy0:      [vector layout] dL/d(initial y), may be NULL
+ *   dloss_dlogk:    [n_reactions, input order] sum over cells of dL/d log k_r,
+ *                   may be NULL
+ * Buffers are host pointers.  The state's variables hold the final values
+ * afterwards, as after micmb_solve.  max_checkpoints bounds accepted steps
+ * per cell (cells beyond it report MICMB_SOLVER_CONVERGENCE_EXCEEDED_MAX_STEPS). */
+int micmb_solve_adjoint(micmb_solver* solver, micmb_state* state, double dt,
+                        const double* dloss_dy_final, double* dloss_dy0, double* dloss_dlogk,
+                        int32_t max_checkpoints, micmb_solver_stats* stats);
+
+/* ---- single-stage entry points (per-kernel parity with micm's drivers) ---- */
+/* ProcessSet::AddForcingTerms (process_set.hpp:524-590; src/process/process_set.cu:10-74):
+ * forcing += f(y) with y = state variables; forcing is MICMB_BUF_FORCING */
+int micmb_add_forcing_terms(micmb_solver* solver, micmb_state* state);
+/* ProcessSet::SubtractJacobianTerms (process_set.hpp:594-670; process_set.cu:77-149):
+ * jacobian -= J(y) into MICMB_BUF_JACOBIAN (add to existing values) */
+int micmb_subtract_jacobian_terms(micmb_solver* solver, micmb_state* state);
+/* AlphaMinusJacobian (rosenbrock.inl:308-326; src/solver/rosenbrock.cu:37-68) */
+int micmb_alpha_minus_jacobian(micmb_solver* solver, micmb_state* state, double alpha);
+/* LuDecompositionMozartInPlace::Decompose (lu_decomposition_mozart_in_place.inl:171-210) */
+int micmb_lu_decompose(micmb_solver* solver, micmb_state* state);
+/* LinearSolverInPlace::Solve (linear_solver_in_place.inl:113-167): x = (LU)^-1 b,
+ * b and x in MICMB_BUF_FORCING */
+int micmb_linear_solve(micmb_solver* solver, micmb_state* state);
+/* NormalizedError (rosenbrock.inl:353-402): y = variables, ynew = MICMB_BUF_SCRATCH_Y,
+ * errors = MICMB_BUF_FORCING; global (all cells) or per cell into per_cell_out */
+int micmb_normalized_error(micmb_solver* solver, micmb_state* state, double* global_out,
+                           double* per_cell_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MICMB_H */

@@ -1,0 +1,791 @@
+// capi.cu -- the extern "C" boundary (include/micmb.h): handle management,
+// device table upload, host<->device copies and dispatch to the kernels.
+// No exception crosses the boundary; failures become a status code plus a
+// thread-local message.
+#include "runtime.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+namespace micmb
+{
+  thread_local std::string g_last_error;
+
+  void CudaCheck(cudaError_t e, const char* what)
+  {
+    if (e != cudaSuccess)
+    {
+      const int code = (e == cudaErrorMemoryAllocation) ? MICMB_ERR_OUT_OF_MEMORY
+                       : (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? MICMB_ERR_NO_DEVICE
+                                                                                       : MICMB_ERR_CUDA;
+      throw Error(code, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+  }
+
+  DeviceMemory::DeviceMemory(size_t b)
+      : bytes(b)
+  {
+    if (b)
+      CudaCheck(cudaMalloc(&p, b), "cudaMalloc");
+  }
+
+  DeviceMemory::~DeviceMemory()
+  {
+    if (p)
+      cudaFree(p);
+  }
+
+  DeviceMemory& DeviceMemory::operator=(DeviceMemory&& o) noexcept
+  {
+    if (this != &o)
+    {
+      if (p)
+        cudaFree(p);
+      p = o.p;
+      bytes = o.bytes;
+      o.p = nullptr;
+      o.bytes = 0;
+    }
+    return *this;
+  }
+
+  DevParams ToDevParams(const micmb_rosenbrock_params& p)
+  {
+    if (p.stages < 1 || p.stages > 6)
+      throw Error(MICMB_ERR_INVALID_ARGUMENT, "stages must be 1..6");
+    DevParams d{};
+    d.stages = p.stages;
+    d.max_steps = p.max_number_of_steps;
+    d.round_off = p.round_off;
+    d.factor_min = p.factor_min;
+    d.factor_max = p.factor_max;
+    d.rejection_factor_decrease = p.rejection_factor_decrease;
+    d.safety_factor = p.safety_factor;
+    d.h_min_param = p.h_min;
+    d.h_max_param = p.h_max;
+    d.h_start_param = p.h_start;
+    for (int i = 0; i < 6; ++i)
+    {
+      d.new_f[i] = p.new_function_evaluation[i];
+      d.m[i] = p.m[i];
+      d.e[i] = p.e[i];
+    }
+    for (int i = 0; i < 15; ++i)
+    {
+      d.a[i] = p.a[i];
+      d.c[i] = p.c[i];
+    }
+    d.inv_order = 1 / p.estimator_of_local_order;
+    d.gamma0 = p.gamma[0];
+    return d;
+  }
+
+  namespace
+  {
+    // packs host arrays into one device allocation (256-byte aligned pieces)
+    struct Packer
+    {
+      std::vector<char> bytes;
+      template<class T>
+      size_t add(const std::vector<T>& v)
+      {
+        size_t off = (bytes.size() + 255) & ~size_t(255);
+        bytes.resize(off + std::max<size_t>(v.size() * sizeof(T), sizeof(T)), 0);
+        if (!v.empty())
+          std::memcpy(bytes.data() + off, v.data(), v.size() * sizeof(T));
+        return off;
+      }
+    };
+
+    struct SchedOffsets
+    {
+      size_t ls, tg, ax, ts, ta, tb;
+      int32_t n_levels;
+    };
+
+    SchedOffsets AddSchedule(Packer& pk, const LevelSchedule& s)
+    {
+      SchedOffsets o;
+      o.ls = pk.add(s.level_start);
+      o.tg = pk.add(s.item_target);
+      o.ax = pk.add(s.item_aux);
+      o.ts = pk.add(s.term_start);
+      o.ta = pk.add(s.term_a);
+      o.tb = pk.add(s.term_b);
+      o.n_levels = s.n_levels();
+      return o;
+    }
+
+    DevSchedule Resolve(const char* base, const SchedOffsets& o)
+    {
+      DevSchedule d;
+      d.n_levels = o.n_levels;
+      d.level_start = reinterpret_cast<const int32_t*>(base + o.ls);
+      d.target = reinterpret_cast<const int32_t*>(base + o.tg);
+      d.aux = reinterpret_cast<const int32_t*>(base + o.ax);
+      d.term_start = reinterpret_cast<const int32_t*>(base + o.ts);
+      d.ta = reinterpret_cast<const int32_t*>(base + o.ta);
+      d.tb = reinterpret_cast<const int32_t*>(base + o.tb);
+      return d;
+    }
+
+    void UploadTables(micmb_solver& s)
+    {
+      const CompiledMechanism& m = *s.mech;
+      Packer pk;
+      std::vector<int32_t> kind(m.R), pcol(m.R), nmult(m.R);
+      std::vector<double> rp((size_t)m.R * MICMB_RATE_PARAM_STRIDE), mult((size_t)m.R * MICMB_MAX_PARAMETERIZED * 4);
+      for (int32_t r = 0; r < m.R; ++r)
+      {
+        kind[r] = m.rates[r].kind;
+        pcol[r] = m.rates[r].param_col;
+        nmult[r] = m.rates[r].n_mult;
+        for (int i = 0; i < MICMB_RATE_PARAM_STRIDE; ++i)
+          rp[(size_t)r * MICMB_RATE_PARAM_STRIDE + i] = m.rates[r].p[i];
+        for (int i = 0; i < MICMB_MAX_PARAMETERIZED; ++i)
+          for (int q = 0; q < 4; ++q)
+            mult[((size_t)r * MICMB_MAX_PARAMETERIZED + i) * 4 + q] = m.rates[r].mult[i][q];
+      }
+      std::vector<int32_t> diag_row_of(m.nnz, -1);
+      for (int32_t i = 0; i < m.S; ++i)
+        diag_row_of[m.diag_pos[i]] = i;
+      const size_t o_kind = pk.add(kind), o_rp = pk.add(rp), o_pcol = pk.add(pcol), o_nm = pk.add(nmult),
+                   o_mult = pk.add(mult);
+      const size_t o_rs = pk.add(m.react_start), o_ri = pk.add(m.react_ids);
+      const size_t o_fs = pk.add(m.f_start), o_fr = pk.add(m.f_rxn), o_fc = pk.add(m.f_coef);
+      const size_t o_ir = pk.add(m.info_rxn), o_ids = pk.add(m.info_dep_start), o_idi = pk.add(m.info_dep_ids);
+      const size_t o_js = pk.add(m.j_start), o_ji = pk.add(m.j_info), o_jc = pk.add(m.j_coef);
+      const size_t o_dp = pk.add(m.diag_pos), o_dro = pk.add(diag_row_of);
+      const SchedOffsets lu = AddSchedule(pk, m.lu), fw = AddSchedule(pk, m.fwd), bw = AddSchedule(pk, m.bwd),
+                         fwt = AddSchedule(pk, m.fwd_t), bwt = AddSchedule(pk, m.bwd_t);
+      s.tables = DeviceMemory(pk.bytes.size());
+      MICMB_CUDA(cudaMemcpy(s.tables.p, pk.bytes.data(), pk.bytes.size(), cudaMemcpyHostToDevice));
+      std::vector<double> ones(std::max<int32_t>(m.R, 1), 1.0);
+      s.scale_dev = DeviceMemory(ones.size() * sizeof(double));
+      MICMB_CUDA(cudaMemcpy(s.scale_dev.p, ones.data(), ones.size() * sizeof(double), cudaMemcpyHostToDevice));
+      const char* b = s.tables.as<const char>();
+      DevMech& d = s.dev;
+      d.S = m.S;
+      d.R = m.R;
+      d.P = m.P;
+      d.nnz = m.nnz;
+      d.n_info = (int32_t)m.info_rxn.size();
+      d.rate_kind = reinterpret_cast<const int32_t*>(b + o_kind);
+      d.rate_p = reinterpret_cast<const double*>(b + o_rp);
+      d.rate_param_col = reinterpret_cast<const int32_t*>(b + o_pcol);
+      d.rate_n_mult = reinterpret_cast<const int32_t*>(b + o_nm);
+      d.rate_mult = reinterpret_cast<const double*>(b + o_mult);
+      d.rate_scale = s.scale_dev.as<const double>();
+      d.react_start = reinterpret_cast<const int32_t*>(b + o_rs);
+      d.react_ids = reinterpret_cast<const int32_t*>(b + o_ri);
+      d.f_start = reinterpret_cast<const int32_t*>(b + o_fs);
+      d.f_rxn = reinterpret_cast<const int32_t*>(b + o_fr);
+      d.f_coef = reinterpret_cast<const double*>(b + o_fc);
+      d.info_rxn = reinterpret_cast<const int32_t*>(b + o_ir);
+      d.info_dep_start = reinterpret_cast<const int32_t*>(b + o_ids);
+      d.info_dep_ids = reinterpret_cast<const int32_t*>(b + o_idi);
+      d.j_start = reinterpret_cast<const int32_t*>(b + o_js);
+      d.j_info = reinterpret_cast<const int32_t*>(b + o_ji);
+      d.j_coef = reinterpret_cast<const double*>(b + o_jc);
+      d.diag_pos = reinterpret_cast<const int32_t*>(b + o_dp);
+      d.diag_row_of = reinterpret_cast<const int32_t*>(b + o_dro);
+      d.lu = Resolve(b, lu);
+      d.fwd = Resolve(b, fw);
+      d.bwd = Resolve(b, bw);
+      d.fwd_t = Resolve(b, fwt);
+      d.bwd_t = Resolve(b, bwt);
+      s.diag_row_of = d.diag_row_of;
+    }
+
+    template<class F>
+    int Guard(F&& f)
+    {
+      try
+      {
+        f();
+        g_last_error.clear();
+        return MICMB_OK;
+      }
+      catch (const Error& e)
+      {
+        g_last_error = e.what();
+        return e.code;
+      }
+      catch (const std::bad_alloc&)
+      {
+        g_last_error = "host allocation failed";
+        return MICMB_ERR_OUT_OF_MEMORY;
+      }
+      catch (const std::exception& e)
+      {
+        g_last_error = e.what();
+        return MICMB_ERR_INVALID_ARGUMENT;
+      }
+      catch (...)
+      {
+        g_last_error = "unknown error";
+        return MICMB_ERR_INTERNAL;
+      }
+    }
+
+    void Need(bool ok, const char* what)
+    {
+      if (!ok)
+        throw Error(MICMB_ERR_INVALID_ARGUMENT, what);
+    }
+
+    // buffer descriptor: device pointer and number of doubles
+    std::pair<double*, size_t> BufferOf(micmb_state& st, int32_t which)
+    {
+      const auto& m = *st.solver->mech;
+      switch (which)
+      {
+        case MICMB_BUF_VARIABLES: return { st.variables.as<double>(), st.variables.bytes / sizeof(double) };
+        case MICMB_BUF_CUSTOM_PARAMS: return { st.custom_params.as<double>(), (size_t)st.n_pad * m.P };
+        case MICMB_BUF_RATE_CONSTANTS: return { st.rate_constants.as<double>(), (size_t)st.n_pad * m.R };
+        case MICMB_BUF_CONDITIONS: return { st.conditions.as<double>(), (size_t)st.n_pad * 3 };
+        case MICMB_BUF_ABSOLUTE_TOLERANCE: return { st.atol.as<double>(), (size_t)m.S };
+        case MICMB_BUF_JACOBIAN: EnsurePlainBuffers(st); return { st.jacobian.as<double>(), (size_t)st.n_pad * m.nnz };
+        case MICMB_BUF_FORCING: EnsurePlainBuffers(st); return { st.forcing0.as<double>(), (size_t)st.n_pad * m.S };
+        case MICMB_BUF_SCRATCH_Y: EnsurePlainBuffers(st); return { st.ynew.as<double>(), (size_t)st.n_pad * m.S };
+      }
+      throw Error(MICMB_ERR_INVALID_ARGUMENT, "unknown buffer id");
+    }
+
+    void SetDevice(const micmb_solver& s)
+    {
+      MICMB_CUDA(cudaSetDevice(s.device));
+    }
+  }  // namespace
+}  // namespace micmb
+
+using namespace micmb;
+
+extern "C"
+{
+  const char* micmb_last_error(void)
+  {
+    return g_last_error.c_str();
+  }
+
+  int micmb_mechanism_create(const micmb_mechanism_desc* desc, micmb_mechanism** out)
+  {
+    return Guard([&] {
+      Need(desc && out, "null argument");
+      auto* h = new micmb_mechanism{ Compile(*desc) };
+      *out = h;
+    });
+  }
+
+  void micmb_mechanism_destroy(micmb_mechanism* mech)
+  {
+    delete mech;
+  }
+
+  int micmb_mechanism_get_info(const micmb_mechanism* mech, micmb_mechanism_info* out)
+  {
+    return Guard([&] {
+      Need(mech && out, "null argument");
+      const auto& m = mech->m;
+      out->n_species = m.S;
+      out->n_reactions = m.R;
+      out->n_custom_params = m.P;
+      out->jacobian_nnz = m.nnz;
+      out->jacobian_nnz_unfilled = (int32_t)m.pattern_unfilled.size();
+      out->lu_updates = m.lu_updates;
+      out->lu_lower = m.lu_lower;
+      out->n_jacobian_terms = (int32_t)m.j_info.size();
+      out->n_forcing_terms = (int32_t)m.f_rxn.size();
+      out->n_jacobian_infos = (int32_t)m.info_rxn.size();
+      out->lu_levels = m.lu.n_levels();
+      out->forward_levels = m.fwd.n_levels();
+      out->backward_levels = m.bwd.n_levels();
+    });
+  }
+
+  int micmb_mechanism_species_columns(const micmb_mechanism* mech, int32_t* out)
+  {
+    return Guard([&] {
+      Need(mech && out, "null argument");
+      std::copy(mech->m.species_column.begin(), mech->m.species_column.end(), out);
+    });
+  }
+
+  int micmb_mechanism_reaction_columns(const micmb_mechanism* mech, int32_t* out)
+  {
+    return Guard([&] {
+      Need(mech && out, "null argument");
+      std::copy(mech->m.reaction_column.begin(), mech->m.reaction_column.end(), out);
+    });
+  }
+
+  int micmb_mechanism_custom_param_columns(const micmb_mechanism* mech, int32_t* out)
+  {
+    return Guard([&] {
+      Need(mech && out, "null argument");
+      std::copy(mech->m.param_column.begin(), mech->m.param_column.end(), out);
+    });
+  }
+
+  int micmb_mechanism_jacobian_pattern(const micmb_mechanism* mech, int32_t* rows, int32_t* cols)
+  {
+    return Guard([&] {
+      Need(mech && rows && cols, "null argument");
+      std::copy(mech->m.nz_row.begin(), mech->m.nz_row.end(), rows);
+      std::copy(mech->m.nz_col.begin(), mech->m.nz_col.end(), cols);
+    });
+  }
+
+  int micmb_mechanism_jacobian_pattern_unfilled(const micmb_mechanism* mech, int32_t* rows, int32_t* cols)
+  {
+    return Guard([&] {
+      Need(mech && rows && cols, "null argument");
+      for (size_t i = 0; i < mech->m.pattern_unfilled.size(); ++i)
+      {
+        rows[i] = mech->m.pattern_unfilled[i].first;
+        cols[i] = mech->m.pattern_unfilled[i].second;
+      }
+    });
+  }
+
+  uint64_t micmb_mechanism_hash(const micmb_mechanism* mech)
+  {
+    return mech ? mech->m.hash : 0;
+  }
+
+  int micmb_rosenbrock_params_default(int32_t kind, micmb_rosenbrock_params* out)
+  {
+    return Guard([&] {
+      Need(out != nullptr, "null argument");
+      micmb_rosenbrock_params p{};
+      p.max_number_of_steps = 1000;
+      p.round_off = 2.220446049250313080847e-16;  // std::numeric_limits<double>::epsilon()
+      p.factor_min = 0.2;
+      p.factor_max = 6;
+      p.rejection_factor_decrease = 0.1;
+      p.safety_factor = 0.9;
+      // Published tableaus (Hairer & Wanner; Sandu et al. 1997), as tabulated in
+      // micm's rosenbrock_solver_parameters.hpp:152-434.
+      switch (kind)
+      {
+        case 2:
+        {
+          const double g = 1.0 + 1.0 / 1.41421356237309504880;  // 1 + 1/sqrt(2)
+          p.stages = 2;
+          p.a[0] = 1.0 / g;
+          p.c[0] = -2.0 / g;
+          for (int i = 0; i < 6; ++i)
+            p.new_function_evaluation[i] = 1;
+          p.m[0] = (3.0) / (2.0 * g);
+          p.m[1] = (1.0) / (2.0 * g);
+          p.e[0] = 1.0 / (2.0 * g);
+          p.e[1] = 1.0 / (2.0 * g);
+          p.estimator_of_local_order = 2.0;
+          p.alpha[1] = 1.0;
+          p.gamma[0] = g;
+          p.gamma[1] = -g;
+          break;
+        }
+        case 3:
+          p.stages = 3;
+          p.a[0] = 1;
+          p.a[1] = 1;
+          p.c[0] = -0.10156171083877702091975600115545e+01;
+          p.c[1] = 0.40759956452537699824805835358067e+01;
+          p.c[2] = 0.92076794298330791242156818474003e+01;
+          p.new_function_evaluation[0] = 1;
+          p.new_function_evaluation[1] = 1;
+          p.m[0] = 0.1e+01;
+          p.m[1] = 0.61697947043828245592553615689730e+01;
+          p.m[2] = -0.42772256543218573326238373806514;
+          p.e[0] = 0.5;
+          p.e[1] = -0.29079558716805469821718236208017e+01;
+          p.e[2] = 0.22354069897811569627360909276199;
+          p.estimator_of_local_order = 3;
+          p.alpha[1] = 0.43586652150845899941601945119356;
+          p.alpha[2] = 0.43586652150845899941601945119356;
+          p.gamma[0] = 0.43586652150845899941601945119356;
+          p.gamma[1] = 0.24291996454816804366592249683314;
+          p.gamma[2] = 0.21851380027664058511513169485832e+01;
+          break;
+        case 4:
+          p.stages = 4;
+          p.a[0] = 0.2000000000000000E+01;
+          p.a[1] = 0.1867943637803922E+01;
+          p.a[2] = 0.2344449711399156;
+          p.a[3] = p.a[1];
+          p.a[4] = p.a[2];
+          p.c[0] = -0.7137615036412310E+01;
+          p.c[1] = 0.2580708087951457E+01;
+          p.c[2] = 0.6515950076447975;
+          p.c[3] = -0.2137148994382534E+01;
+          p.c[4] = -0.3214669691237626;
+          p.c[5] = -0.6949742501781779;
+          p.new_function_evaluation[0] = 1;
+          p.new_function_evaluation[1] = 1;
+          p.new_function_evaluation[2] = 1;
+          p.m[0] = 0.2255570073418735E+01;
+          p.m[1] = 0.2870493262186792;
+          p.m[2] = 0.4353179431840180;
+          p.m[3] = 0.1093502252409163E+01;
+          p.e[0] = -0.2815431932141155;
+          p.e[1] = -0.7276199124938920E-01;
+          p.e[2] = -0.1082196201495311;
+          p.e[3] = -0.1093502252409163E+01;
+          p.estimator_of_local_order = 4.0;
+          p.alpha[1] = 0.1145640000000000E+01;
+          p.alpha[2] = 0.6552168638155900;
+          p.alpha[3] = p.alpha[2];
+          p.gamma[0] = 0.5728200000000000;
+          p.gamma[1] = -0.1769193891319233E+01;
+          p.gamma[2] = 0.7592633437920482;
+          p.gamma[3] = -0.1049021087100450;
+          break;
+        case 40:
+          p.stages = 4;
+          p.a[1] = 2.0;
+          p.a[3] = 2.0;
+          p.a[5] = 1.0;
+          p.c[0] = 4.0;
+          p.c[1] = 1.0;
+          p.c[2] = -1.0;
+          p.c[3] = 1.0;
+          p.c[4] = -1.0;
+          p.c[5] = -(8.0 / 3.0);
+          p.new_function_evaluation[0] = 1;
+          p.new_function_evaluation[2] = 1;
+          p.new_function_evaluation[3] = 1;
+          p.m[0] = 2.0;
+          p.m[2] = 1.0;
+          p.m[3] = 1.0;
+          p.e[3] = 1.0;
+          p.estimator_of_local_order = 3.0;
+          p.alpha[2] = 1.0;
+          p.alpha[3] = 1.0;
+          p.gamma[0] = 0.5;
+          p.gamma[1] = 1.5;
+          break;
+        case 60:
+          p.stages = 6;
+          p.alpha[1] = 0.386;
+          p.alpha[2] = 0.210;
+          p.alpha[3] = 0.630;
+          p.alpha[4] = 1.000;
+          p.alpha[5] = 1.000;
+          p.gamma[0] = 0.2500000000000000;
+          p.gamma[1] = -0.1043000000000000;
+          p.gamma[2] = 0.1035000000000000;
+          p.gamma[3] = -0.3620000000000023E-01;
+          p.a[0] = 0.1544000000000000E+01;
+          p.a[1] = 0.9466785280815826;
+          p.a[2] = 0.2557011698983284;
+          p.a[3] = 0.3314825187068521E+01;
+          p.a[4] = 0.2896124015972201E+01;
+          p.a[5] = 0.9986419139977817;
+          p.a[6] = 0.1221224509226641E+01;
+          p.a[7] = 0.6019134481288629E+01;
+          p.a[8] = 0.1253708332932087E+02;
+          p.a[9] = -0.6878860361058950;
+          p.a[10] = p.a[6];
+          p.a[11] = p.a[7];
+          p.a[12] = p.a[8];
+          p.a[13] = p.a[9];
+          p.a[14] = 1.0;
+          p.c[0] = -0.5668800000000000E+01;
+          p.c[1] = -0.2430093356833875E+01;
+          p.c[2] = -0.2063599157091915;
+          p.c[3] = -0.1073529058151375;
+          p.c[4] = -0.9594562251023355E+01;
+          p.c[5] = -0.2047028614809616E+02;
+          p.c[6] = 0.7496443313967647E+01;
+          p.c[7] = -0.1024680431464352E+02;
+          p.c[8] = -0.3399990352819905E+02;
+          p.c[9] = 0.1170890893206160E+02;
+          p.c[10] = 0.8083246795921522E+01;
+          p.c[11] = -0.7981132988064893E+01;
+          p.c[12] = -0.3152159432874371E+02;
+          p.c[13] = 0.1631930543123136E+02;
+          p.c[14] = -0.6058818238834054E+01;
+          p.m[0] = p.a[6];
+          p.m[1] = p.a[7];
+          p.m[2] = p.a[8];
+          p.m[3] = p.a[9];
+          p.m[4] = 1.0;
+          p.m[5] = 1.0;
+          p.e[5] = 1.0;
+          for (int i = 0; i < 6; ++i)
+            p.new_function_evaluation[i] = 1;
+          p.estimator_of_local_order = 4.0;
+          break;
+        default: throw Error(MICMB_ERR_INVALID_ARGUMENT, "unknown tableau kind (use 2, 3, 4, 40 or 60)");
+      }
+      *out = p;
+    });
+  }
+
+  int micmb_solver_create(const micmb_mechanism* mech, const micmb_rosenbrock_params* params, micmb_solver** out)
+  {
+    return Guard([&] {
+      Need(mech && params && out, "null argument");
+      int count = 0;
+      cudaError_t e = cudaGetDeviceCount(&count);
+      if (e != cudaSuccess || count == 0)
+        throw Error(MICMB_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+      auto s = std::make_unique<micmb_solver>();
+      MICMB_CUDA(cudaGetDevice(&s->device));
+      cudaDeviceProp prop{};
+      MICMB_CUDA(cudaGetDeviceProperties(&prop, s->device));
+      if (prop.major < 10)
+        throw Error(MICMB_ERR_UNSUPPORTED, "this library is built for sm_100a (B200) only");
+      s->sm_count = prop.multiProcessorCount;
+      s->smem_optin = prop.sharedMemPerBlockOptin;
+      s->mech = std::make_shared<CompiledMechanism>(mech->m);
+      s->host_params = *params;
+      s->params = ToDevParams(*params);
+      UploadTables(*s);
+      *out = s.release();
+    });
+  }
+
+  void micmb_solver_destroy(micmb_solver* solver)
+  {
+    delete solver;
+  }
+
+  int micmb_solver_set_params(micmb_solver* solver, const micmb_rosenbrock_params* params)
+  {
+    return Guard([&] {
+      Need(solver && params, "null argument");
+      solver->params = ToDevParams(*params);
+      solver->host_params = *params;
+    });
+  }
+
+  int micmb_solver_set_rate_scale(micmb_solver* solver, const double* scale)
+  {
+    return Guard([&] {
+      Need(solver && scale, "null argument");
+      SetDevice(*solver);
+      const auto& m = *solver->mech;
+      std::vector<double> by_col(std::max<int32_t>(m.R, 1), 1.0);
+      for (int32_t r = 0; r < m.R; ++r)
+        by_col[m.reaction_column[r]] = scale[r];
+      MICMB_CUDA(cudaMemcpy(solver->scale_dev.p, by_col.data(), by_col.size() * sizeof(double),
+                            cudaMemcpyHostToDevice));
+    });
+  }
+
+  int micmb_solver_set_fused_config(micmb_solver* solver, const micmb_fused_config* config)
+  {
+    return Guard([&] {
+      Need(solver && config, "null argument");
+      Need(config->cells_per_cta >= 0 && config->cells_per_cta <= 8, "cells_per_cta must be 0..8");
+      solver->fused = *config;
+    });
+  }
+
+  int micmb_solver_get_fused_config(micmb_solver* solver, micmb_fused_config* config)
+  {
+    return Guard([&] {
+      Need(solver && config, "null argument");
+      *config = solver->fused;
+    });
+  }
+
+  int micmb_state_create(micmb_solver* solver, int64_t n_cells, int32_t vector_length, micmb_state** out)
+  {
+    return Guard([&] {
+      Need(solver && out, "null argument");
+      Need(n_cells >= 0, "negative cell count");
+      Need(vector_length >= 1 && vector_length <= 4096, "vector length must be 1..4096");
+      SetDevice(*solver);
+      const auto& m = *solver->mech;
+      auto st = std::make_unique<micmb_state>();
+      st->solver = solver;
+      st->n_cells = n_cells;
+      st->L = vector_length;
+      st->n_groups = (n_cells + vector_length - 1) / vector_length;
+      st->n_pad = st->n_groups * vector_length;
+      MICMB_CUDA(cudaStreamCreateWithFlags(&st->own_stream, cudaStreamNonBlocking));
+      st->stream = st->own_stream;
+      st->variables = DeviceMemory(st->dense_bytes(m.S));
+      st->custom_params = DeviceMemory(st->dense_bytes(std::max<int32_t>(m.P, 1)));
+      st->rate_constants = DeviceMemory(st->dense_bytes(std::max<int32_t>(m.R, 1)));
+      st->conditions = DeviceMemory(st->dense_bytes(3));
+      st->atol = DeviceMemory(sizeof(double) * m.S);
+      st->counters = DeviceMemory(256);
+      MICMB_CUDA(cudaMallocHost(&st->host_counters, 64));
+      MICMB_CUDA(cudaMemsetAsync(st->variables.p, 0, st->variables.bytes, st->stream));
+      MICMB_CUDA(cudaMemsetAsync(st->custom_params.p, 0, st->custom_params.bytes, st->stream));
+      MICMB_CUDA(cudaMemsetAsync(st->rate_constants.p, 0, st->rate_constants.bytes, st->stream));
+      MICMB_CUDA(cudaMemsetAsync(st->conditions.p, 0, st->conditions.bytes, st->stream));
+      std::vector<double> atol(m.S, 1e-3);  // SolverBuilder default (solver_builder.inl:208)
+      MICMB_CUDA(cudaMemcpyAsync(st->atol.p, atol.data(), sizeof(double) * m.S, cudaMemcpyHostToDevice, st->stream));
+      MICMB_CUDA(cudaStreamSynchronize(st->stream));
+      *out = st.release();
+    });
+  }
+
+  void micmb_state_destroy(micmb_state* state)
+  {
+    if (!state)
+      return;
+    cudaSetDevice(state->solver->device);
+    if (state->stream)
+      cudaStreamSynchronize(state->stream);
+    if (state->host_counters)
+      cudaFreeHost(state->host_counters);
+    if (state->own_stream)
+      cudaStreamDestroy(state->own_stream);
+    delete state;
+  }
+
+  int micmb_state_set_stream(micmb_state* state, void* stream)
+  {
+    return Guard([&] {
+      Need(state != nullptr, "null argument");
+      state->stream = stream ? static_cast<cudaStream_t>(stream) : state->own_stream;
+    });
+  }
+
+  int micmb_state_synchronize(micmb_state* state)
+  {
+    return Guard([&] {
+      Need(state != nullptr, "null argument");
+      MICMB_CUDA(cudaStreamSynchronize(state->stream));
+    });
+  }
+
+  int micmb_state_upload(micmb_state* state, int32_t buffer, const double* host)
+  {
+    return Guard([&] {
+      Need(state && host, "null argument");
+      SetDevice(*state->solver);
+      auto b = BufferOf(*state, buffer);
+      MICMB_CUDA(cudaMemcpyAsync(b.first, host, b.second * sizeof(double), cudaMemcpyHostToDevice, state->stream));
+      MICMB_CUDA(cudaStreamSynchronize(state->stream));
+    });
+  }
+
+  int micmb_state_download(micmb_state* state, int32_t buffer, double* host)
+  {
+    return Guard([&] {
+      Need(state && host, "null argument");
+      SetDevice(*state->solver);
+      auto b = BufferOf(*state, buffer);
+      MICMB_CUDA(cudaMemcpyAsync(host, b.first, b.second * sizeof(double), cudaMemcpyDeviceToHost, state->stream));
+      MICMB_CUDA(cudaStreamSynchronize(state->stream));
+    });
+  }
+
+  int micmb_state_device_buffer(micmb_state* state, int32_t buffer, double** ptr, int64_t* count)
+  {
+    return Guard([&] {
+      Need(state && ptr && count, "null argument");
+      auto b = BufferOf(*state, buffer);
+      *ptr = b.first;
+      *count = (int64_t)b.second;
+    });
+  }
+
+  int micmb_state_set_relative_tolerance(micmb_state* state, double rtol)
+  {
+    return Guard([&] {
+      Need(state != nullptr, "null argument");
+      Need(rtol > 0, "relative tolerance must be positive");
+      state->rtol = rtol;
+    });
+  }
+
+  int micmb_update_state_parameters(micmb_solver* solver, micmb_state* state)
+  {
+    return Guard([&] {
+      Need(solver && state && state->solver == solver, "state does not belong to this solver");
+      SetDevice(*solver);
+      LaunchRateConstants(*solver, *state);
+    });
+  }
+
+  int micmb_solve(micmb_solver* solver, micmb_state* state, double dt, int32_t method, int32_t step_control,
+                  micmb_solver_stats* stats, int32_t* per_cell_status, int32_t* per_cell_accepted)
+  {
+    return Guard([&] {
+      Need(solver && state && state->solver == solver, "state does not belong to this solver");
+      Need(dt > 0 && std::isfinite(dt), "time step must be positive and finite");
+      Need(method == MICMB_METHOD_PLAIN || method == MICMB_METHOD_FUSED, "unknown method");
+      Need(step_control == MICMB_STEP_GLOBAL || step_control == MICMB_STEP_PER_CELL, "unknown step control");
+      SetDevice(*solver);
+      if (method == MICMB_METHOD_FUSED)
+      {
+        Need(step_control == MICMB_STEP_PER_CELL, "the fused method solves each cell independently (per-cell step control)");
+        SolveFused(*solver, *state, dt, stats, per_cell_status, per_cell_accepted, nullptr);
+      }
+      else
+        SolvePlain(*solver, *state, dt, step_control, stats, per_cell_status, per_cell_accepted);
+    });
+  }
+
+  int micmb_add_forcing_terms(micmb_solver* solver, micmb_state* state)
+  {
+    return Guard([&] {
+      Need(solver && state && state->solver == solver, "state does not belong to this solver");
+      SetDevice(*solver);
+      LaunchAddForcing(*solver, *state);
+      MICMB_CUDA(cudaStreamSynchronize(state->stream));
+    });
+  }
+
+  int micmb_subtract_jacobian_terms(micmb_solver* solver, micmb_state* state)
+  {
+    return Guard([&] {
+      Need(solver && state && state->solver == solver, "state does not belong to this solver");
+      SetDevice(*solver);
+      LaunchSubtractJacobian(*solver, *state);
+      MICMB_CUDA(cudaStreamSynchronize(state->stream));
+    });
+  }
+
+  int micmb_alpha_minus_jacobian(micmb_solver* solver, micmb_state* state, double alpha)
+  {
+    return Guard([&] {
+      Need(solver && state && state->solver == solver, "state does not belong to this solver");
+      SetDevice(*solver);
+      LaunchAlphaMinusJacobian(*solver, *state, alpha);
+      MICMB_CUDA(cudaStreamSynchronize(state->stream));
+    });
+  }
+
+  int micmb_lu_decompose(micmb_solver* solver, micmb_state* state)
+  {
+    return Guard([&] {
+      Need(solver && state && state->solver == solver, "state does not belong to this solver");
+      SetDevice(*solver);
+      LaunchDecompose(*solver, *state);
+      MICMB_CUDA(cudaStreamSynchronize(state->stream));
+    });
+  }
+
+  int micmb_linear_solve(micmb_solver* solver, micmb_state* state)
+  {
+    return Guard([&] {
+      Need(solver && state && state->solver == solver, "state does not belong to this solver");
+      SetDevice(*solver);
+      LaunchLinearSolve(*solver, *state);
+      MICMB_CUDA(cudaStreamSynchronize(state->stream));
+    });
+  }
+
+  int micmb_normalized_error(micmb_solver* solver, micmb_state* state, double* global_out, double* per_cell_out)
+  {
+    return Guard([&] {
+      Need(solver && state && state->solver == solver, "state does not belong to this solver");
+      SetDevice(*solver);
+      NormalizedError(*solver, *state, global_out, per_cell_out);
+    });
+  }
+}

@@ -1,0 +1,459 @@
+// device.cuh -- per-cell building blocks of the Rosenbrock solve, shared by the
+// per-stage ("plain") kernels and the persistent fused kernel.
+//
+// Every function works on one grid cell with `nl` cooperating lanes (`lane` in
+// [0, nl)): the plain kernels call them with nl = 1 and data in global memory
+// in micm's vector layout (stride L between columns), the fused kernel with a
+// warp (nl = 32) and data staged in shared memory (stride 1).  Each output
+// value is produced by exactly one lane, summing its terms in the order micm's
+// scatter loops apply them (process_set.hpp:524-670,
+// lu_decomposition_mozart_in_place.inl:171-210, linear_solver_in_place.inl:113-167),
+// so results do not depend on nl.  The library is compiled with -fmad=false:
+// each multiply and add rounds separately, as micm's CPU build does.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/micmb.h"
+
+namespace micmb
+{
+  // ---------------------------------------------------------------------
+  // device tables
+  // ---------------------------------------------------------------------
+  struct DevSchedule
+  {
+    int32_t n_levels;
+    const int32_t* level_start;
+    const int32_t* target;
+    const int32_t* aux;
+    const int32_t* term_start;
+    const int32_t* ta;
+    const int32_t* tb;
+  };
+
+  struct DevMech
+  {
+    int32_t S, R, P, nnz, n_info;
+    // rate constants by rate column
+    const int32_t* rate_kind;
+    const double* rate_p;      // [R][MICMB_RATE_PARAM_STRIDE]
+    const int32_t* rate_param_col;
+    const int32_t* rate_n_mult;
+    const double* rate_mult;   // [R][MICMB_MAX_PARAMETERIZED][4]
+    const double* rate_scale;  // [R] multiplicative scale (1.0 by default)
+    // reactants by rate column
+    const int32_t* react_start;
+    const int32_t* react_ids;
+    // forcing gather by species
+    const int32_t* f_start;
+    const int32_t* f_rxn;
+    const double* f_coef;
+    // jacobian infos and gather by nonzero
+    const int32_t* info_rxn;
+    const int32_t* info_dep_start;
+    const int32_t* info_dep_ids;
+    const int32_t* j_start;
+    const int32_t* j_info;
+    const double* j_coef;
+    const int32_t* diag_pos;     // [S] storage position of a_ii
+    const int32_t* diag_row_of;  // [nnz] row i if the position holds a_ii, else -1
+    DevSchedule lu, fwd, bwd, fwd_t, bwd_t;
+  };
+
+  // Rosenbrock tableau in device-friendly form
+  struct DevParams
+  {
+    int32_t stages;
+    int32_t max_steps;
+    double round_off, factor_min, factor_max, rejection_factor_decrease, safety_factor;
+    double h_min_param, h_max_param, h_start_param;
+    int32_t new_f[6];
+    double inv_order;  // 1 / estimator_of_local_order
+    double a[15], c[15], m[6], e[6], gamma0;
+  };
+
+  // column accessor with a runtime stride (global vector layout) or unit stride (shared)
+  struct Strided
+  {
+    double* p;
+    int32_t s;
+    __device__ __forceinline__ double& operator[](int32_t i) const
+    {
+      return p[(size_t)i * (size_t)s];
+    }
+  };
+  struct Unit
+  {
+    double* p;
+    __device__ __forceinline__ double& operator[](int32_t i) const
+    {
+      return p[i];
+    }
+  };
+
+  template<int NL>
+  __device__ __forceinline__ void lane_sync()
+  {
+    if constexpr (NL > 1)
+      __syncwarp();
+  }
+
+  // ---------------------------------------------------------------------
+  // rate constants (rate_constant_functions.hpp:52-136)
+  // ---------------------------------------------------------------------
+  __device__ __forceinline__ double falloff(const double* p, double T, double rho, double numerator_scale)
+  {
+    const double k0 = p[0] * exp(p[2] / T) * pow(T / 300.0, p[1]);
+    const double kinf = p[3] * exp(p[5] / T) * pow(T / 300.0, p[4]);
+    const double ratio = k0 * rho / kinf;
+    return k0 * numerator_scale / (1.0 + ratio) * pow(p[6], p[7] / (p[7] + pow(log10(ratio), 2.0)));
+  }
+
+  // k for rate column r given the cell's conditions and custom-parameter column reader
+  template<class ParamFn>
+  __device__ __forceinline__ double rate_constant(const DevMech& M, int32_t r, double T, double Pr, double rho,
+                                                  ParamFn param)
+  {
+    const double* p = M.rate_p + (size_t)r * MICMB_RATE_PARAM_STRIDE;
+    double k;
+    switch (M.rate_kind[r])
+    {
+      case MICMB_RATE_ARRHENIUS: k = p[0] * exp(p[2] / T) * pow(T / p[3], p[1]) * (1.0 + p[4] * Pr); break;
+      case MICMB_RATE_TROE: k = falloff(p, T, rho, rho); break;
+      case MICMB_RATE_TERNARY_CHEMICAL_ACTIVATION: k = falloff(p, T, rho, 1.0); break;
+      case MICMB_RATE_BRANCHED:
+      {
+        const double a = p[5] * rho;
+        const double b = 0.43 * pow(T / 298.0, -8.0);
+        const double A_val = a / (1.0 + a / b) * pow(0.41, 1.0 / (1.0 + pow(log10(a / b), 2.0)));
+        const double pre = p[1] * exp(-p[2] / T);
+        k = (p[0] == 0.0) ? pre * (p[6] / (p[6] + A_val)) : pre * (A_val / (A_val + p[6]));
+        break;
+      }
+      case MICMB_RATE_TUNNELING: k = p[0] * exp(-p[1] / T + p[2] / (T * T * T)); break;
+      case MICMB_RATE_TAYLOR_SERIES:
+      {
+        double poly = 0.0, t_pow = 1.0;
+        const int32_t n = (int32_t)p[5];
+        for (int32_t j = 0; j < n; ++j, t_pow *= T)
+          poly += p[6 + j] * t_pow;
+        k = poly * p[0] * exp(p[2] / T) * pow(T / p[3], p[1]) * (1.0 + p[4] * Pr);
+        break;
+      }
+      case MICMB_RATE_REVERSIBLE: k = p[0] * exp(p[1] / T) * p[2]; break;
+      case MICMB_RATE_USER_DEFINED: k = param(M.rate_param_col[r]) * p[0]; break;
+      case MICMB_RATE_SURFACE:
+      {
+        const double radius = param(M.rate_param_col[r]);
+        const double num_conc = param(M.rate_param_col[r] + 1);
+        const double mean_free_speed = sqrt(p[1] * T);
+        k = 4.0 * num_conc * 3.14159265358979323846 * radius * radius /
+            (radius / p[0] + 4.0 / (mean_free_speed * p[2]));
+        break;
+      }
+      default: k = 0.0;
+    }
+    const int32_t nm = M.rate_n_mult[r];
+    if (nm > 0)
+    {
+      double v = 1.0;
+      const double* c = M.rate_mult + (size_t)r * MICMB_MAX_PARAMETERIZED * 4;
+      for (int32_t i = 0; i < nm; ++i)
+        v *= c[4 * i + 0] + c[4 * i + 1] * T + c[4 * i + 2] * Pr + c[4 * i + 3] * rho;
+      k *= v;
+    }
+    const double scale = M.rate_scale[r];
+    if (scale != 1.0)
+      k *= scale;
+    return k;
+  }
+
+  // ---------------------------------------------------------------------
+  // forcing: rate_r = k_r * prod(y reactants); f_s = sum_terms coef * rate
+  // ---------------------------------------------------------------------
+  template<int NL, class KV, class YV, class RV>
+  __device__ __forceinline__ void reaction_rates(const DevMech& M, KV k, YV y, RV rate, int lane)
+  {
+    for (int32_t r = lane; r < M.R; r += NL)
+    {
+      double v = k[r];
+      for (int32_t i = M.react_start[r]; i < M.react_start[r + 1]; ++i)
+        v *= y[M.react_ids[i]];
+      rate[r] = v;
+    }
+  }
+
+  template<int NL, class RV, class FV>
+  __device__ __forceinline__ void forcing_gather(const DevMech& M, RV rate, FV f, int lane)
+  {
+    for (int32_t s = lane; s < M.S; s += NL)
+    {
+      double acc = 0.0;
+      for (int32_t t = M.f_start[s]; t < M.f_start[s + 1]; ++t)
+        acc += M.f_coef[t] * rate[M.f_rxn[t]];
+      f[s] = acc;
+    }
+  }
+
+  // ---------------------------------------------------------------------
+  // -J + alpha I: d_rate per info, then gather per nonzero
+  // ---------------------------------------------------------------------
+  template<int NL, class KV, class YV, class DV>
+  __device__ __forceinline__ void jacobian_rates(const DevMech& M, KV k, YV y, DV drate, int lane)
+  {
+    for (int32_t i = lane; i < M.n_info; i += NL)
+    {
+      double v = k[M.info_rxn[i]];
+      for (int32_t d = M.info_dep_start[i]; d < M.info_dep_start[i + 1]; ++d)
+        v *= y[M.info_dep_ids[d]];
+      drate[i] = v;
+    }
+  }
+
+  // jac[e] = sum_terms coef * drate (+ alpha on the diagonal when add_alpha)
+  template<int NL, class DV, class JV>
+  __device__ __forceinline__ void jacobian_gather(const DevMech& M, DV drate, JV jac, double alpha, bool add_alpha,
+                                                  int lane)
+  {
+    for (int32_t e = lane; e < M.nnz; e += NL)
+    {
+      double acc = 0.0;
+      for (int32_t t = M.j_start[e]; t < M.j_start[e + 1]; ++t)
+        acc += M.j_coef[t] * drate[M.j_info[t]];
+      if (add_alpha && M.diag_row_of[e] >= 0)
+        acc += alpha;
+      jac[e] = acc;
+    }
+  }
+
+  // ---------------------------------------------------------------------
+  // in-place LU (Crout order of micm's Mozart updates); inv = 1/a_kk scratch [S]
+  // ---------------------------------------------------------------------
+  template<int NL, class AV, class IV>
+  __device__ __forceinline__ void lu_decompose(const DevSchedule& sch, const int32_t* diag_row, AV A, IV inv,
+                                               int lane)
+  {
+    for (int32_t l = 0; l < sch.n_levels; ++l)
+    {
+      const int32_t end = sch.level_start[l + 1];
+      for (int32_t it = sch.level_start[l] + lane; it < end; it += NL)
+      {
+        const int32_t e = sch.target[it];
+        double v = A[e];
+        for (int32_t t = sch.term_start[it]; t < sch.term_start[it + 1]; ++t)
+          v -= A[sch.ta[t]] * A[sch.tb[t]];
+        const int32_t aux = sch.aux[it];
+        if (aux >= 0)
+          v *= inv[diag_row[aux]];
+        A[e] = v;
+        const int32_t dr = diag_row[e];
+        if (dr >= 0)
+          inv[dr] = 1.0 / v;
+      }
+      lane_sync<NL>();
+    }
+  }
+
+  // L y = b (unit diagonal), in place
+  template<int NL, class AV, class XV>
+  __device__ __forceinline__ void solve_lower(const DevSchedule& sch, AV A, XV x, int lane)
+  {
+    for (int32_t l = 0; l < sch.n_levels; ++l)
+    {
+      const int32_t end = sch.level_start[l + 1];
+      for (int32_t it = sch.level_start[l] + lane; it < end; it += NL)
+      {
+        const int32_t i = sch.target[it];
+        double v = x[i];
+        for (int32_t t = sch.term_start[it]; t < sch.term_start[it + 1]; ++t)
+          v -= A[sch.ta[t]] * x[sch.tb[t]];
+        x[i] = v;
+      }
+      lane_sync<NL>();
+    }
+  }
+
+  // upper solve with division by the diagonal (aux), in place
+  template<int NL, class AV, class XV>
+  __device__ __forceinline__ void solve_upper(const DevSchedule& sch, AV A, XV x, int lane)
+  {
+    for (int32_t l = 0; l < sch.n_levels; ++l)
+    {
+      const int32_t end = sch.level_start[l + 1];
+      for (int32_t it = sch.level_start[l] + lane; it < end; it += NL)
+      {
+        const int32_t i = sch.target[it];
+        double v = x[i];
+        for (int32_t t = sch.term_start[it]; t < sch.term_start[it + 1]; ++t)
+          v -= A[sch.ta[t]] * x[sch.tb[t]];
+        x[i] = v / A[sch.aux[it]];
+      }
+      lane_sync<NL>();
+    }
+  }
+
+  // ---------------------------------------------------------------------
+  // normalized error (rosenbrock.inl:353-402), lane-striped partial sums
+  // combined in butterfly order; the one-lane version reproduces the order.
+  // ---------------------------------------------------------------------
+  __device__ __forceinline__ double scaled_sq(double y, double ynew, double err, double atol, double rtol)
+  {
+    const double ay = fabs(y), an = fabs(ynew);
+    const double ymax = ay > an ? ay : an;
+    const double q = err / (atol + rtol * ymax);
+    return q * q;
+  }
+
+  // Partial sum of lane `lane` of a 32-lane stripe over S species.
+  template<class YV, class NV, class EV>
+  __device__ __forceinline__ double error_partial(int32_t S, YV y, NV ynew, EV err, const double* atol, double rtol,
+                                                  int lane)
+  {
+    double acc = 0.0;
+    for (int32_t s = lane; s < S; s += 32)
+      acc += scaled_sq(y[s], ynew[s], err[s], atol[s], rtol);
+    return acc;
+  }
+
+  // warp butterfly sum (all lanes get the total)
+  __device__ __forceinline__ double warp_sum(double v)
+  {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+      v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+  }
+
+  // the same sum computed by one thread: partial[l] for l in 0..31, butterfly order
+  __device__ __forceinline__ double butterfly_sum_serial(double* part)
+  {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+      double nxt[32];
+#pragma unroll
+      for (int l = 0; l < 32; ++l)
+        nxt[l] = part[l] + part[l ^ off];
+#pragma unroll
+      for (int l = 0; l < 32; ++l)
+        part[l] = nxt[l];
+    }
+    return part[0];
+  }
+
+  // ---------------------------------------------------------------------
+  // step control (rosenbrock.inl:80-293)
+  // ---------------------------------------------------------------------
+  struct CellCtl
+  {
+    double t;
+    double H;
+    int32_t reject_last;
+    int32_t reject_more;
+    int32_t state;  // MICMB_SOLVER_*
+    int32_t new_step;
+    int32_t function_calls, jacobian_updates, number_of_steps, accepted, rejected, decompositions, solves;
+  };
+
+  struct StepBounds
+  {
+    double dt, h_min, h_max, h_start;
+  };
+
+  __host__ __device__ inline StepBounds step_bounds(const DevParams& p, double dt)
+  {
+    StepBounds b;
+    b.dt = dt;
+    // rosenbrock.inl:33-36, with std::min(a,b) = (b<a)?b:a and std::max(a,b) = (a<b)?b:a
+    b.h_min = p.h_min_param == 0.0 ? 1.0e-15 * dt : p.h_min_param;
+    b.h_max = p.h_max_param == 0.0 ? dt : ((p.h_max_param < dt) ? p.h_max_param : dt);
+    const double hs = p.h_start_param == 0.0 ? 1.0e-6 * dt : ((p.h_start_param < b.h_max) ? p.h_start_param : b.h_max);
+    const double ahs = fabs(hs), ahm = fabs(b.h_max);
+    const double lo = (b.h_min < ahs) ? ahs : b.h_min;
+    b.h_start = (ahm < lo) ? ahm : lo;
+    return b;
+  }
+
+  __host__ __device__ inline void ctl_init(CellCtl& c, const StepBounds& b)
+  {
+    c.t = 0.0;
+    c.H = b.h_start;
+    c.reject_last = 0;
+    c.reject_more = 0;
+    c.state = MICMB_SOLVER_RUNNING;
+    c.new_step = 1;
+    c.function_calls = c.jacobian_updates = c.number_of_steps = 0;
+    c.accepted = c.rejected = c.decompositions = c.solves = 0;
+  }
+
+  // Top of micm's outer loop: returns false (and sets state) when the cell is done.
+  __host__ __device__ inline bool ctl_begin_step(CellCtl& c, const DevParams& p, const StepBounds& b)
+  {
+    if (!((c.t - b.dt + p.round_off) <= 0))
+    {
+      if (c.state == MICMB_SOLVER_RUNNING)
+        c.state = MICMB_SOLVER_CONVERGED;
+      return false;
+    }
+    if (c.number_of_steps > p.max_steps)
+    {
+      c.state = MICMB_SOLVER_CONVERGENCE_EXCEEDED_MAX_STEPS;
+      return false;
+    }
+    if (((c.t + 0.1 * c.H) == c.t) || (c.H <= p.round_off))
+    {
+      c.state = MICMB_SOLVER_STEP_SIZE_TOO_SMALL;
+      return false;
+    }
+    const double rem = fabs(b.dt - c.t);
+    c.H = (rem < c.H) ? rem : c.H;  // std::min(H, |dt - t|)
+    return true;
+  }
+
+  // Accept/reject after the error norm. Returns 1 accepted, 0 rejected, -1 stopped (NaN/Inf).
+  __host__ __device__ inline int ctl_after_error(CellCtl& c, const DevParams& p, const StepBounds& b, double error)
+  {
+    // std::min(factor_max, std::max(factor_min, safety / pow(error, 1/order)))
+    const double x = p.safety_factor / pow(error, p.inv_order);
+    const double lo = (p.factor_min < x) ? x : p.factor_min;
+    const double fac = (lo < p.factor_max) ? lo : p.factor_max;
+    double Hnew = c.H * fac;
+    c.number_of_steps += 1;
+    if (isnan(error))
+    {
+      c.state = MICMB_SOLVER_NAN_DETECTED;
+      return -1;
+    }
+    if (isinf(error))
+    {
+      c.state = MICMB_SOLVER_INF_DETECTED;
+      return -1;
+    }
+    if ((error < 1) || (c.H < b.h_min))
+    {
+      c.accepted += 1;
+      c.t = c.t + c.H;
+      Hnew = (b.h_max < Hnew) ? b.h_max : Hnew;  // std::max(h_min, std::min(Hnew, h_max))
+      Hnew = (b.h_min < Hnew) ? Hnew : b.h_min;
+      if (c.reject_last)
+        Hnew = (c.H < Hnew) ? c.H : Hnew;        // std::min(Hnew, H)
+      c.reject_last = 0;
+      c.reject_more = 0;
+      c.H = Hnew;
+      c.new_step = 1;
+      return 1;
+    }
+    if (c.reject_more)
+      Hnew = c.H * p.rejection_factor_decrease;
+    c.reject_more = c.reject_last;
+    c.reject_last = 1;
+    c.H = Hnew;
+    if (c.accepted >= 1)
+      c.rejected += 1;
+    c.jacobian_updates += 1;
+    c.new_step = 0;
+    return 0;
+  }
+}  // namespace micmb

@@ -1,0 +1,350 @@
+// fused.cu -- the whole adaptive Rosenbrock solve of a cell in one persistent
+// kernel.  Each warp owns one grid cell at a time: the cell's state, stage
+// vectors, rate constants and (when it fits) its LU factor live in the warp's
+// slice of shared memory for the entire solve, and the 32 lanes split every
+// stage (forcing, -J assembly, LU, triangular solves, error norm) by the level
+// schedules of the mechanism compiler.  When a warp finishes its cell it takes
+// the next unsolved cell from a global atomic counter, so cells with uneven
+// step counts balance across the GPU without any host involvement.
+#include "runtime.hpp"
+
+#include <algorithm>
+
+namespace micmb
+{
+  namespace
+  {
+    constexpr int kWarp = 32;
+
+    __device__ __forceinline__ size_t cell_base(int64_t c, int32_t L, int32_t ncol)
+    {
+      return (size_t)(c / L) * (size_t)L * (size_t)ncol + (size_t)(c % L);
+    }
+
+    struct WarpLayout
+    {
+      int32_t S, R, stages, scratch_cols, nnz;
+      int32_t per_warp;  // doubles per warp in shared memory
+    };
+
+    __host__ __device__ inline int32_t RoundUp2(int32_t v)
+    {
+      return (v + 1) & ~1;
+    }
+
+    __host__ __device__ inline WarpLayout MakeLayout(int32_t S, int32_t R, int32_t stages, int32_t n_info, int32_t nnz,
+                                                     bool lu_shared)
+    {
+      WarpLayout w;
+      w.S = S;
+      w.R = R;
+      w.stages = stages;
+      w.scratch_cols = R > n_info ? R : n_info;
+      w.nnz = nnz;
+      w.per_warp = RoundUp2(S * (5 + stages) + R + w.scratch_cols + (lu_shared ? nnz : 0));
+      return w;
+    }
+
+    __device__ __forceinline__ void count_attempt(CellCtl& cc, const DevParams& P)
+    {
+      cc.decompositions += 1;
+      cc.solves += P.stages;
+      for (int32_t s = 1; s < P.stages; ++s)
+        cc.function_calls += P.new_f[s] ? 1 : 0;
+    }
+
+    template<bool LU_SHARED>
+    __global__ void __launch_bounds__(256) k_fused(DevMech M, DevParams P, StepBounds B, FusedArgs A, WarpLayout W)
+    {
+      extern __shared__ __align__(16) double smem[];
+      const int warp = threadIdx.x >> 5;
+      const int lane = threadIdx.x & 31;
+      const int warps = blockDim.x >> 5;
+      const int32_t S = M.S, R = M.R, L = A.L;
+      double* base = smem + (size_t)warp * W.per_warp;
+      double* Y = base;
+      double* Yn = Y + S;
+      double* F0 = Yn + S;
+      double* Fc = F0 + S;
+      double* inv = Fc + S;
+      double* K = inv + S;
+      double* kk = K + (size_t)P.stages * S;
+      double* scr = kk + R;
+      double* LU = LU_SHARED ? (scr + W.scratch_cols)
+                             : A.lu_global + ((size_t)blockIdx.x * warps + warp) * (size_t)A.lu_slot_stride;
+      long long acc[8] = { 0 };
+
+      for (;;)
+      {
+        int cell = 0;
+        if (lane == 0)
+          cell = atomicAdd(A.next_cell, 1);
+        cell = __shfl_sync(0xffffffffu, cell, 0);
+        if (cell >= A.n_cells)
+          break;
+        const size_t by = cell_base(cell, L, S);
+        const size_t bk = cell_base(cell, L, R);
+        for (int32_t i = lane; i < S; i += kWarp)
+          Y[i] = A.variables_in[by + (size_t)i * L];
+        for (int32_t r = lane; r < R; r += kWarp)
+          kk[r] = A.rate_constants[bk + (size_t)r * L];
+        __syncwarp();
+
+        CellCtl c;
+        ctl_init(c, B);
+        int32_t n_ckpt = 0;
+        while (ctl_begin_step(c, P, B))
+        {
+          c.function_calls += 1;
+          c.jacobian_updates += 1;
+          if (A.ckpt_y)
+          {
+            if (n_ckpt >= A.max_ckpt)
+            {
+              c.state = MICMB_SOLVER_CONVERGENCE_EXCEEDED_MAX_STEPS;
+              break;
+            }
+          }
+          reaction_rates<kWarp>(M, Unit{ kk }, Unit{ Y }, Unit{ scr }, lane);
+          __syncwarp();
+          forcing_gather<kWarp>(M, Unit{ scr }, Unit{ F0 }, lane);
+          __syncwarp();
+          for (;;)
+          {
+            const double alpha = 1.0 / (c.H * P.gamma0);
+            jacobian_rates<kWarp>(M, Unit{ kk }, Unit{ Y }, Unit{ scr }, lane);
+            __syncwarp();
+            jacobian_gather<kWarp>(M, Unit{ scr }, Unit{ LU }, alpha, true, lane);
+            __syncwarp();
+            lu_decompose<kWarp>(M.lu, M.diag_row_of, Unit{ LU }, Unit{ inv }, lane);
+            const double* Fsrc = F0;
+            for (int32_t st = 0; st < P.stages; ++st)
+            {
+              const int32_t sc = st * (st - 1) / 2;
+              if (st > 0 && P.new_f[st])
+              {
+                for (int32_t i = lane; i < S; i += kWarp)
+                {
+                  double v = Y[i];
+                  for (int32_t j = 0; j < st; ++j)
+                    v += P.a[sc + j] * K[(size_t)j * S + i];
+                  Yn[i] = v;
+                }
+                __syncwarp();
+                reaction_rates<kWarp>(M, Unit{ kk }, Unit{ Yn }, Unit{ scr }, lane);
+                __syncwarp();
+                forcing_gather<kWarp>(M, Unit{ scr }, Unit{ Fc }, lane);
+                __syncwarp();
+                Fsrc = Fc;
+              }
+              double* Ks = K + (size_t)st * S;
+              for (int32_t i = lane; i < S; i += kWarp)
+              {
+                double v = Fsrc[i];
+                for (int32_t j = 0; j < st; ++j)
+                {
+                  const double c_over_h = P.c[sc + j] / c.H;
+                  v += c_over_h * K[(size_t)j * S + i];
+                }
+                Ks[i] = v;
+              }
+              __syncwarp();
+              solve_lower<kWarp>(M.fwd, Unit{ LU }, Unit{ Ks }, lane);
+              solve_upper<kWarp>(M.bwd, Unit{ LU }, Unit{ Ks }, lane);
+            }
+            double part = 0.0;
+            for (int32_t i = lane; i < S; i += kWarp)
+            {
+              double v = Y[i];
+              double e = 0.0;
+              for (int32_t st = 0; st < P.stages; ++st)
+              {
+                const double kv = K[(size_t)st * S + i];
+                v += P.m[st] * kv;
+                e += P.e[st] * kv;
+              }
+              Yn[i] = v;
+              part += scaled_sq(Y[i], v, e, A.atol[i], A.rtol);
+            }
+            const double sum = warp_sum(part);
+            const double rms = sqrt(sum / (double)S);
+            const double error = (rms < 1.0e-10) ? 1.0e-10 : rms;
+            count_attempt(c, P);
+            const double h_used = c.H;
+            const int res = ctl_after_error(c, P, B, error);
+            __syncwarp();
+            if (res == 1)
+            {
+              if (A.ckpt_y)
+              {
+                // checkpoint the accepted step: its starting state and step size
+                double* dst = A.ckpt_y + ((size_t)cell * A.max_ckpt + n_ckpt) * S;
+                for (int32_t i = lane; i < S; i += kWarp)
+                  dst[i] = Y[i];
+                if (lane == 0)
+                  A.ckpt_h[(size_t)cell * A.max_ckpt + n_ckpt] = h_used;
+                ++n_ckpt;
+              }
+              for (int32_t i = lane; i < S; i += kWarp)
+                Y[i] = Yn[i];
+              __syncwarp();
+              break;
+            }
+            if (res < 0)
+              break;
+          }
+          if (c.state != MICMB_SOLVER_RUNNING)
+            break;
+        }
+        for (int32_t i = lane; i < S; i += kWarp)
+        {
+          const double v = Y[i];
+          A.variables_out[by + (size_t)i * L] = (v < 0.0) ? 0.0 : v;
+        }
+        if (lane == 0)
+        {
+          if (A.cell_status)
+            A.cell_status[cell] = c.state;
+          if (A.cell_accepted)
+            A.cell_accepted[cell] = A.ckpt_y ? n_ckpt : c.accepted;
+          acc[0] += c.function_calls;
+          acc[1] += c.jacobian_updates;
+          acc[2] += c.number_of_steps;
+          acc[3] += c.accepted;
+          acc[4] += c.rejected;
+          acc[5] += c.decompositions;
+          acc[6] += c.solves;
+          acc[7] += (c.state == MICMB_SOLVER_CONVERGED) ? 0 : 1;
+        }
+        __syncwarp();
+      }
+      if (lane == 0)
+        for (int q = 0; q < 8; ++q)
+          if (acc[q])
+            atomicAdd(A.stats + q, (unsigned long long)acc[q]);
+    }
+  }  // namespace
+
+  size_t FusedSharedBytes(const micmb_solver& s, bool lu_in_shared)
+  {
+    const auto& m = *s.mech;
+    WarpLayout w = MakeLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz, lu_in_shared);
+    return (size_t)w.per_warp * sizeof(double);
+  }
+
+  int FusedWarpsPerCta(const micmb_solver& s, const micmb_fused_config& cfg)
+  {
+    const size_t per = FusedSharedBytes(s, cfg.lu_in_shared != 0);
+    int w = per == 0 ? 8 : (int)std::min<size_t>(8, s.smem_optin / per);
+    if (cfg.cells_per_cta > 0)
+      w = std::min(w, cfg.cells_per_cta);
+    return w;
+  }
+
+  void SolveFused(micmb_solver& s, micmb_state& st, double dt, micmb_solver_stats* stats, int32_t* per_cell_status,
+                  int32_t* per_cell_accepted, const FusedArgs* adj)
+  {
+    const auto& m = *s.mech;
+    micmb_fused_config cfg = s.fused;
+    if (cfg.lu_in_shared && FusedWarpsPerCta(s, cfg) < 1)
+      cfg.lu_in_shared = 0;
+    const int warps = FusedWarpsPerCta(s, cfg);
+    if (warps < 1)
+      throw Error(MICMB_ERR_UNSUPPORTED, "mechanism too large for the fused kernel's shared-memory working set");
+    const bool lu_shared = cfg.lu_in_shared != 0;
+    WarpLayout W = MakeLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz, lu_shared);
+    const size_t smem = (size_t)W.per_warp * sizeof(double) * warps;
+    const int threads = warps * kWarp;
+    auto kernel = lu_shared ? k_fused<true> : k_fused<false>;
+    MICMB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    MICMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+    if (per_sm < 1)
+      throw Error(MICMB_ERR_UNSUPPORTED, "fused kernel cannot be resident with this configuration");
+    if (cfg.ctas_per_sm > 0)
+      per_sm = std::min(per_sm, cfg.ctas_per_sm);
+    int64_t grid = (int64_t)per_sm * s.sm_count;
+    const int64_t n = st.n_cells;
+    grid = std::max<int64_t>(1, std::min<int64_t>(grid, (n + warps - 1) / warps));
+
+    FusedArgs A{};
+    if (adj)
+      A = *adj;
+    A.n_cells = n;
+    A.L = st.L;
+    if (!adj)
+    {
+      A.variables_in = st.variables.as<double>();
+      A.variables_out = st.variables.as<double>();
+    }
+    A.rate_constants = st.rate_constants.as<double>();
+    A.atol = st.atol.as<double>();
+    A.rtol = st.rtol;
+    char* cbase = st.counters.as<char>();
+    A.next_cell = reinterpret_cast<int32_t*>(cbase + 8);
+    A.stats = reinterpret_cast<unsigned long long*>(cbase + 64);
+    if (!st.status.p)
+    {
+      st.status = DeviceMemory(sizeof(int32_t) * std::max<int64_t>(n, 1));
+    }
+    if (!st.accepted.p)
+      st.accepted = DeviceMemory(sizeof(int32_t) * std::max<int64_t>(n, 1));
+    A.cell_status = st.status.as<int32_t>();
+    A.cell_accepted = st.accepted.as<int32_t>();
+    if (!lu_shared)
+    {
+      const int64_t slots = grid * warps;
+      const int64_t stride = ((int64_t)m.nnz + 31) & ~31ll;
+      if (st.lu_slot_count < slots || !st.lu_slots.p)
+      {
+        st.lu_slots = DeviceMemory(sizeof(double) * (size_t)(slots * stride));
+        st.lu_slot_count = slots;
+      }
+      A.lu_global = st.lu_slots.as<double>();
+      A.lu_slot_stride = stride;
+    }
+    MICMB_CUDA(cudaMemsetAsync(cbase, 0, 128, st.stream));
+    if (n > 0)
+    {
+      const StepBounds B = step_bounds(s.params, dt);
+      kernel<<<(unsigned)grid, threads, smem, st.stream>>>(s.dev, s.params, B, A, W);
+      MICMB_CUDA(cudaGetLastError());
+    }
+    if (stats || per_cell_status || per_cell_accepted)
+    {
+      unsigned long long hs[8];
+      MICMB_CUDA(cudaMemcpyAsync(hs, A.stats, sizeof(hs), cudaMemcpyDeviceToHost, st.stream));
+      if (per_cell_status)
+        MICMB_CUDA(cudaMemcpyAsync(per_cell_status, A.cell_status, sizeof(int32_t) * n, cudaMemcpyDeviceToHost,
+                                   st.stream));
+      if (per_cell_accepted)
+        MICMB_CUDA(cudaMemcpyAsync(per_cell_accepted, A.cell_accepted, sizeof(int32_t) * n, cudaMemcpyDeviceToHost,
+                                   st.stream));
+      MICMB_CUDA(cudaStreamSynchronize(st.stream));
+      if (stats)
+      {
+        stats->function_calls = (int64_t)hs[0];
+        stats->jacobian_updates = (int64_t)hs[1];
+        stats->number_of_steps = (int64_t)hs[2];
+        stats->accepted = (int64_t)hs[3];
+        stats->rejected = (int64_t)hs[4];
+        stats->decompositions = (int64_t)hs[5];
+        stats->solves = (int64_t)hs[6];
+        stats->cells_not_converged = (int32_t)hs[7];
+        stats->final_time = dt;
+        stats->state = hs[7] ? MICMB_SOLVER_CONVERGENCE_EXCEEDED_MAX_STEPS : MICMB_SOLVER_CONVERGED;
+        if (hs[7])
+        {
+          std::vector<int32_t> stv(n);
+          MICMB_CUDA(cudaMemcpy(stv.data(), A.cell_status, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+          for (auto v : stv)
+            if (v != MICMB_SOLVER_CONVERGED)
+            {
+              stats->state = v;
+              break;
+            }
+        }
+      }
+    }
+  }
+}  // namespace micmb

@@ -1,0 +1,549 @@
+// mechanism.cpp -- symbolic compile (see mechanism.hpp).
+#include "mechanism.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <set>
+#include <stdexcept>
+
+namespace micmb
+{
+  namespace
+  {
+    constexpr double kAvogadro = 6.02214076e23;           // micm::constants::AVOGADRO_CONSTANT
+    constexpr double kBoltzmann = 1.380649e-23;           // micm::constants::BOLTZMANN_CONSTANT
+    constexpr double kGas = kBoltzmann * kAvogadro;       // micm::constants::GAS_CONSTANT
+    constexpr double kPi = 3.14159265358979323846;
+
+    void Require(bool ok, const std::string& what)
+    {
+      if (!ok)
+        throw std::runtime_error(what);
+    }
+
+    // Longest-path levels for a DAG whose items are visited in a dependency-
+    // respecting order; returns the schedule with items grouped by level.
+    struct RawItem
+    {
+      int32_t target;
+      int32_t aux;
+      std::vector<std::pair<int32_t, int32_t>> terms;
+      std::vector<int32_t> deps;  // item indices (in visit order) this item reads
+    };
+
+    LevelSchedule Schedule(const std::vector<RawItem>& items)
+    {
+      const int32_t n = (int32_t)items.size();
+      std::vector<int32_t> level(n, 0);
+      int32_t max_level = -1;
+      for (int32_t i = 0; i < n; ++i)
+      {
+        int32_t l = 0;
+        for (int32_t d : items[i].deps)
+        {
+          if (d >= i)
+            throw std::runtime_error("schedule: dependency visited after its user");
+          l = std::max(l, level[d] + 1);
+        }
+        level[i] = l;
+        max_level = std::max(max_level, l);
+      }
+      std::vector<int32_t> order(n);
+      std::iota(order.begin(), order.end(), 0);
+      // by level, then longer term lists first so lanes finish together
+      std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+        if (level[a] != level[b])
+          return level[a] < level[b];
+        return items[a].terms.size() > items[b].terms.size();
+      });
+      LevelSchedule s;
+      s.level_start.assign(max_level + 2, 0);
+      for (int32_t i = 0; i < n; ++i)
+        s.level_start[level[i] + 1]++;
+      for (int32_t l = 0; l <= max_level; ++l)
+        s.level_start[l + 1] += s.level_start[l];
+      s.term_start.push_back(0);
+      for (int32_t idx : order)
+      {
+        const auto& it = items[idx];
+        s.item_target.push_back(it.target);
+        s.item_aux.push_back(it.aux);
+        for (const auto& t : it.terms)
+        {
+          s.term_a.push_back(t.first);
+          s.term_b.push_back(t.second);
+        }
+        s.term_start.push_back((int32_t)s.term_a.size());
+      }
+      if (n == 0)
+        s.level_start.assign(1, 0);
+      return s;
+    }
+
+    uint64_t Fnv(uint64_t h, const void* data, size_t bytes)
+    {
+      const unsigned char* p = static_cast<const unsigned char*>(data);
+      for (size_t i = 0; i < bytes; ++i)
+      {
+        h ^= p[i];
+        h *= 1099511628211ull;
+      }
+      return h;
+    }
+    template<class T>
+    uint64_t FnvVec(uint64_t h, const std::vector<T>& v)
+    {
+      return v.empty() ? h : Fnv(h, v.data(), v.size() * sizeof(T));
+    }
+  }  // namespace
+
+  std::vector<int32_t> DiagonalMarkowitz(int32_t n, const std::vector<std::pair<int32_t, int32_t>>& nonzeros)
+  {
+    // Same selection rule and tie-break as micm's sparse Markowitz scan: the
+    // live node with the smallest (row_deg-1)*(col_deg-1), computed in
+    // unsigned 64-bit arithmetic (micm::Index), first index wins ties.
+    std::vector<std::set<int32_t>> out(n), in(n);
+    for (const auto& e : nonzeros)
+    {
+      out[e.first].insert(e.second);
+      in[e.second].insert(e.first);
+    }
+    std::vector<uint64_t> row_deg(n), col_deg(n);
+    for (int32_t v = 0; v < n; ++v)
+    {
+      row_deg[v] = out[v].size();
+      col_deg[v] = in[v].size();
+    }
+    std::vector<char> alive(n, 1);
+    std::vector<int32_t> perm;
+    perm.reserve(n);
+    for (int32_t step = 0; step < n; ++step)
+    {
+      int32_t pivot = n;
+      uint64_t best = ~0ull;
+      for (int32_t v = 0; v < n; ++v)
+      {
+        if (!alive[v])
+          continue;
+        const uint64_t cost = (row_deg[v] - 1ull) * (col_deg[v] - 1ull);
+        if (pivot == n || cost < best)
+        {
+          best = cost;
+          pivot = v;
+        }
+      }
+      perm.push_back(pivot);
+      alive[pivot] = 0;
+      std::vector<int32_t> cols, ins;
+      for (int32_t c : out[pivot])
+        if (c != pivot && alive[c])
+          cols.push_back(c);
+      for (int32_t i : in[pivot])
+        if (i != pivot && alive[i])
+          ins.push_back(i);
+      for (int32_t i : ins)
+        for (int32_t c : cols)
+          if (out[i].insert(c).second)
+          {
+            ++row_deg[i];
+            in[c].insert(i);
+            ++col_deg[c];
+          }
+      for (int32_t c : cols)
+      {
+        in[c].erase(pivot);
+        --col_deg[c];
+      }
+      for (int32_t i : ins)
+      {
+        out[i].erase(pivot);
+        --row_deg[i];
+      }
+    }
+    return perm;
+  }
+
+  CompiledMechanism Compile(const micmb_mechanism_desc& d)
+  {
+    Require(d.n_species > 0, "mechanism has no species");
+    Require(d.n_reactions >= 0, "negative reaction count");
+    Require(d.n_species < 32768, "too many species (limit 32767)");
+    const int32_t S = d.n_species, R = d.n_reactions;
+    Require(R == 0 || (d.rate_type && d.rate_params && d.reactant_start && d.product_start),
+            "null mechanism arrays");
+    for (int32_t r = 0; r < R; ++r)
+    {
+      Require(d.rate_type[r] >= 0 && d.rate_type[r] <= MICMB_RATE_SURFACE,
+              "reaction " + std::to_string(r) + ": unsupported rate-constant kind");
+      Require(d.reactant_start[r] <= d.reactant_start[r + 1] && d.product_start[r] <= d.product_start[r + 1],
+              "reaction " + std::to_string(r) + ": bad reactant/product offsets");
+      int nparam = 0;
+      for (int32_t i = d.reactant_start[r]; i < d.reactant_start[r + 1]; ++i)
+      {
+        const int32_t s = d.reactant_species[i];
+        Require(s < S && (s >= 0 || -s - 1 < d.n_parameterized),
+                "reaction " + std::to_string(r) + ": reactant index out of range");
+        if (s < 0)
+          ++nparam;
+      }
+      Require(nparam <= MICMB_MAX_PARAMETERIZED,
+              "reaction " + std::to_string(r) + ": more parameterized reactants than supported");
+      for (int32_t i = d.product_start[r]; i < d.product_start[r + 1]; ++i)
+        Require(d.product_species[i] >= 0 && d.product_species[i] < S,
+                "reaction " + std::to_string(r) + ": product index out of range");
+    }
+
+    CompiledMechanism m;
+    m.S = S;
+    m.R = R;
+
+    // 1. stable sort by rate-constant kind (solver_builder.inl:274-329)
+    std::vector<int32_t> order(R);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return d.rate_type[a] < d.rate_type[b]; });
+    m.reaction_column.assign(R, 0);
+    for (int32_t i = 0; i < R; ++i)
+      m.reaction_column[order[i]] = i;
+
+    // 2. species columns (solver_builder.inl:78-119)
+    m.species_column.resize(S);
+    std::iota(m.species_column.begin(), m.species_column.end(), 0);
+    auto collect_nonzeros = [&](const std::vector<int32_t>& col) {
+      std::set<std::pair<int32_t, int32_t>> ids;
+      for (int32_t r = 0; r < R; ++r)
+      {
+        std::vector<int32_t> re, pr;
+        for (int32_t i = d.reactant_start[r]; i < d.reactant_start[r + 1]; ++i)
+          if (d.reactant_species[i] >= 0)
+            re.push_back(col[d.reactant_species[i]]);
+        for (int32_t i = d.product_start[r]; i < d.product_start[r + 1]; ++i)
+          pr.push_back(col[d.product_species[i]]);
+        for (int32_t ind : re)
+        {
+          for (int32_t dep : re)
+            ids.insert({ dep, ind });
+          for (int32_t dep : pr)
+            ids.insert({ dep, ind });
+        }
+      }
+      return ids;
+    };
+    if (d.reorder_state)
+    {
+      auto ids = collect_nonzeros(m.species_column);
+      std::vector<std::pair<int32_t, int32_t>> nz(ids.begin(), ids.end());
+      auto perm = DiagonalMarkowitz(S, nz);
+      for (int32_t i = 0; i < S; ++i)
+        m.species_column[perm[i]] = i;
+    }
+
+    // 3. rate definitions and reactant/product tables by rate column
+    int32_t next_param = 0;
+    m.param_column.assign(R, -1);
+    m.rates.resize(R);
+    m.react_start.push_back(0);
+    m.prod_start.push_back(0);
+    for (int32_t rc = 0; rc < R; ++rc)
+    {
+      const int32_t r = order[rc];
+      RateDef& def = m.rates[rc];
+      def.kind = d.rate_type[r];
+      def.input_index = r;
+      const double* p = d.rate_params + (size_t)r * MICMB_RATE_PARAM_STRIDE;
+      for (int i = 0; i < MICMB_RATE_PARAM_STRIDE; ++i)
+        def.p[i] = p[i];
+      switch (def.kind)
+      {
+        case MICMB_RATE_BRANCHED:
+        {
+          // ReactionRateConstantStore::BuildFrom precomputation (reaction_rate_store.hpp:268-281):
+          // p = [branch, X, Y, a0, n] -> [branch, X, Y, a0, n, k0, z]
+          const double n = std::floor(p[4]);
+          const double k0 = 2.0e-22 * kAvogadro * 1.0e-6 * std::exp(n);
+          const double air_ref = 2.45e19 / kAvogadro * 1.0e6;
+          const double a = k0 * air_ref;
+          const double b = 0.43 * std::pow(293.0 / 298.0, -8.0);
+          const double A_val = a / (1.0 + a / b) * std::pow(0.41, 1.0 / (1.0 + std::pow(std::log10(a / b), 2.0)));
+          def.p[5] = k0;
+          def.p[6] = A_val * (1.0 - p[3]) / p[3];
+          break;
+        }
+        case MICMB_RATE_TAYLOR_SERIES:
+          Require(p[5] >= 1 && p[5] <= 16, "TaylorSeries needs 1..16 coefficients");
+          break;
+        case MICMB_RATE_USER_DEFINED:
+          def.param_col = next_param;
+          next_param += 1;
+          break;
+        case MICMB_RATE_SURFACE:
+          // p = [D_g, MW, gamma] -> [D_g, 8R/(pi MW), gamma] (reaction_rate_store.hpp:300-314)
+          Require(p[1] > 0, "surface reaction needs a positive molecular weight");
+          def.p[1] = 8.0 * kGas / (kPi * p[1]);
+          def.param_col = next_param;
+          next_param += 2;
+          break;
+        default: break;
+      }
+      m.param_column[r] = def.param_col;
+      for (int32_t i = d.reactant_start[r]; i < d.reactant_start[r + 1]; ++i)
+      {
+        const int32_t s = d.reactant_species[i];
+        if (s >= 0)
+          m.react_ids.push_back(m.species_column[s]);
+        else
+        {
+          const double* c = d.parameterized_coef + 4 * (size_t)(-s - 1);
+          for (int q = 0; q < 4; ++q)
+            def.mult[def.n_mult][q] = c[q];
+          def.n_mult++;
+        }
+      }
+      m.react_start.push_back((int32_t)m.react_ids.size());
+      for (int32_t i = d.product_start[r]; i < d.product_start[r + 1]; ++i)
+      {
+        m.prod_ids.push_back(m.species_column[d.product_species[i]]);
+        m.prod_yield.push_back(d.product_yield[i]);
+      }
+      m.prod_start.push_back((int32_t)m.prod_ids.size());
+    }
+    m.P = next_param;
+
+    // 4. Jacobian infos: (independent column, process) stably sorted by column
+    //    (process_set.hpp:329-391)
+    std::vector<std::pair<int32_t, int32_t>> columns;
+    for (int32_t rc = 0; rc < R; ++rc)
+      for (int32_t i = m.react_start[rc]; i < m.react_start[rc + 1]; ++i)
+        columns.push_back({ m.react_ids[i], rc });
+    std::stable_sort(columns.begin(), columns.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    m.info_dep_start.push_back(0);
+    for (const auto& c : columns)
+    {
+      m.info_ind.push_back(c.first);
+      m.info_rxn.push_back(c.second);
+      bool found = false;
+      for (int32_t i = m.react_start[c.second]; i < m.react_start[c.second + 1]; ++i)
+      {
+        if (m.react_ids[i] == c.first && !found)
+        {
+          found = true;
+          continue;
+        }
+        m.info_dep_ids.push_back(m.react_ids[i]);
+      }
+      m.info_dep_start.push_back((int32_t)m.info_dep_ids.size());
+    }
+
+    // 5. sparsity: ProcessSet::NonZeroJacobianElements + diagonal, then LU fill
+    std::set<std::pair<int32_t, int32_t>> nz;
+    for (int32_t rc = 0; rc < R; ++rc)
+      for (int32_t i = m.react_start[rc]; i < m.react_start[rc + 1]; ++i)
+      {
+        const int32_t ind = m.react_ids[i];
+        for (int32_t j = m.react_start[rc]; j < m.react_start[rc + 1]; ++j)
+          nz.insert({ m.react_ids[j], ind });
+        for (int32_t j = m.prod_start[rc]; j < m.prod_start[rc + 1]; ++j)
+          nz.insert({ m.prod_ids[j], ind });
+      }
+    for (int32_t i = 0; i < S; ++i)
+      nz.insert({ i, i });
+    m.pattern_unfilled.assign(nz.begin(), nz.end());
+    std::vector<std::set<int32_t>> row_cols(S), col_rows(S);
+    for (const auto& e : nz)
+    {
+      row_cols[e.first].insert(e.second);
+      col_rows[e.second].insert(e.first);
+    }
+    for (int32_t i = 0; i < S; ++i)
+    {
+      std::vector<int32_t> U(row_cols[i].upper_bound(i), row_cols[i].end());
+      std::vector<int32_t> Lr(col_rows[i].upper_bound(i), col_rows[i].end());
+      for (int32_t k : U)
+        for (int32_t j : Lr)
+          if (row_cols[j].insert(k).second)
+            col_rows[k].insert(j);
+    }
+    for (int32_t i = 0; i < S; ++i)
+      for (int32_t j : row_cols[i])
+      {
+        m.position[{ i, j }] = (int32_t)m.nz_row.size();
+        m.nz_row.push_back(i);
+        m.nz_col.push_back(j);
+      }
+    m.nnz = (int32_t)m.nz_row.size();
+    Require(m.nnz < (1 << 30), "Jacobian too large");
+    m.diag_pos.resize(S);
+    for (int32_t i = 0; i < S; ++i)
+      m.diag_pos[i] = m.position.at({ i, i });
+    auto pos = [&](int32_t r, int32_t c) { return m.position.at({ r, c }); };
+
+    // 6. forcing gather per species (process_set.hpp:524-590 order)
+    {
+      std::vector<std::vector<std::pair<int32_t, double>>> terms(S);
+      for (int32_t rc = 0; rc < R; ++rc)
+      {
+        for (int32_t i = m.react_start[rc]; i < m.react_start[rc + 1]; ++i)
+          terms[m.react_ids[i]].push_back({ rc, -1.0 });
+        for (int32_t i = m.prod_start[rc]; i < m.prod_start[rc + 1]; ++i)
+          terms[m.prod_ids[i]].push_back({ rc, m.prod_yield[i] });
+      }
+      m.f_start.push_back(0);
+      for (int32_t s = 0; s < S; ++s)
+      {
+        for (const auto& t : terms[s])
+        {
+          m.f_rxn.push_back(t.first);
+          m.f_coef.push_back(t.second);
+        }
+        m.f_start.push_back((int32_t)m.f_rxn.size());
+      }
+    }
+
+    // 7. -J gather per nonzero (process_set.hpp:594-670 order)
+    {
+      std::vector<std::vector<std::pair<int32_t, double>>> terms(m.nnz);
+      for (int32_t info = 0; info < (int32_t)m.info_rxn.size(); ++info)
+      {
+        const int32_t ind = m.info_ind[info], rc = m.info_rxn[info];
+        for (int32_t i = m.info_dep_start[info]; i < m.info_dep_start[info + 1]; ++i)
+          terms[pos(m.info_dep_ids[i], ind)].push_back({ info, 1.0 });
+        terms[pos(ind, ind)].push_back({ info, 1.0 });
+        for (int32_t i = m.prod_start[rc]; i < m.prod_start[rc + 1]; ++i)
+          terms[pos(m.prod_ids[i], ind)].push_back({ info, -m.prod_yield[i] });
+      }
+      m.j_start.push_back(0);
+      for (int32_t e = 0; e < m.nnz; ++e)
+      {
+        for (const auto& t : terms[e])
+        {
+          m.j_info.push_back(t.first);
+          m.j_coef.push_back(t.second);
+        }
+        m.j_start.push_back((int32_t)m.j_info.size());
+      }
+    }
+
+    // 8. LU in Crout form (same per-entry update order as
+    //    lu_decomposition_mozart_in_place.inl:171-210)
+    {
+      std::vector<RawItem> items;
+      std::map<int32_t, int32_t> item_of_pos;
+      for (int32_t mn = 0; mn < S; ++mn)
+      {
+        auto add = [&](int32_t j, int32_t k) {
+          RawItem it;
+          it.target = pos(j, k);
+          it.aux = j > k ? pos(k, k) : -1;
+          const int32_t lim = std::min(j, k);
+          for (int32_t i : row_cols[j])
+          {
+            if (i >= lim)
+              break;
+            auto f = m.position.find({ i, k });
+            if (f == m.position.end())
+              continue;
+            it.terms.push_back({ pos(j, i), f->second });
+            it.deps.push_back(item_of_pos.at(pos(j, i)));
+            it.deps.push_back(item_of_pos.at(f->second));
+          }
+          if (j > k)
+          {
+            it.deps.push_back(item_of_pos.at(pos(k, k)));
+            m.lu_lower++;
+          }
+          m.lu_updates += (int32_t)it.terms.size();
+          item_of_pos[it.target] = (int32_t)items.size();
+          items.push_back(std::move(it));
+        };
+        for (int32_t k : row_cols[mn])
+          if (k >= mn)
+            add(mn, k);
+        for (int32_t j : col_rows[mn])
+          if (j > mn)
+            add(j, mn);
+      }
+      m.lu = Schedule(items);
+    }
+
+    // 9. triangular solves (linear_solver_in_place.inl:49-103, 113-167) and
+    //    their transposes for the adjoint
+    {
+      std::vector<RawItem> f, b, ft, bt;
+      for (int32_t i = 0; i < S; ++i)
+      {
+        RawItem it;
+        it.target = i;
+        it.aux = -1;
+        for (int32_t j : row_cols[i])
+        {
+          if (j >= i)
+            break;
+          it.terms.push_back({ pos(i, j), j });
+          it.deps.push_back(j);
+        }
+        f.push_back(std::move(it));
+      }
+      m.fwd = Schedule(f);
+      // backward: visit i = S-1 .. 0; item index v = S-1-i
+      for (int32_t v = 0; v < S; ++v)
+      {
+        const int32_t i = S - 1 - v;
+        RawItem it;
+        it.target = i;
+        it.aux = pos(i, i);
+        for (int32_t j : row_cols[i])
+          if (j > i)
+          {
+            it.terms.push_back({ pos(i, j), j });
+            it.deps.push_back(S - 1 - j);
+          }
+        b.push_back(std::move(it));
+      }
+      m.bwd = Schedule(b);
+      for (int32_t i = 0; i < S; ++i)
+      {
+        RawItem it;
+        it.target = i;
+        it.aux = pos(i, i);
+        for (int32_t j : col_rows[i])
+        {
+          if (j >= i)
+            break;
+          it.terms.push_back({ pos(j, i), j });
+          it.deps.push_back(j);
+        }
+        ft.push_back(std::move(it));
+      }
+      m.fwd_t = Schedule(ft);
+      for (int32_t v = 0; v < S; ++v)
+      {
+        const int32_t i = S - 1 - v;
+        RawItem it;
+        it.target = i;
+        it.aux = -1;
+        for (int32_t j : col_rows[i])
+          if (j > i)
+          {
+            it.terms.push_back({ pos(j, i), j });
+            it.deps.push_back(S - 1 - j);
+          }
+        bt.push_back(std::move(it));
+      }
+      m.bwd_t = Schedule(bt);
+    }
+
+    // 10. hash of everything the device sees
+    uint64_t h = 1469598103934665603ull;
+    h = Fnv(h, &m.S, sizeof(m.S));
+    h = Fnv(h, &m.R, sizeof(m.R));
+    h = FnvVec(h, m.nz_row);
+    h = FnvVec(h, m.nz_col);
+    h = FnvVec(h, m.react_ids);
+    h = FnvVec(h, m.prod_ids);
+    h = FnvVec(h, m.prod_yield);
+    for (const auto& r : m.rates)
+      h = Fnv(h, &r.kind, sizeof(r.kind));
+    m.hash = h;
+    return m;
+  }
+}  // namespace micmb

@@ -1,0 +1,107 @@
+// mechanism.hpp -- symbolic compile of a chemical mechanism for the B200 solver.
+//
+// Reproduces micm's numbering exactly, so every column and nonzero lines up
+// with the reference solver:
+//   * reactions stably sorted by rate-constant kind (solver_builder.inl:274-329)
+//   * species order from diagonal Markowitz reordering of the Jacobian
+//     sparsity (linear_solver.inl:30-124, solver_builder.inl:78-119)
+//   * Jacobian sparsity (process_set.hpp:425-457) plus the diagonal
+//     (util/jacobian.hpp:15-32), LU fill (lu_decomposition_mozart_in_place.inl:121-169)
+//   * custom-parameter columns (solver_builder.inl:129-188)
+// and then emits the device work lists in *gather* form with level schedules:
+// every output value (forcing of a species, -J nonzero, LU nonzero, solution
+// component) is one item whose terms are summed in exactly the order micm's
+// scatter loops apply them, so a single lane can own an item and the result
+// does not depend on how items are spread over lanes.
+#pragma once
+
+#include "../../include/micmb.h"
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace micmb
+{
+  struct LevelSchedule
+  {
+    // items are grouped by level; level l holds items [level_start[l], level_start[l+1])
+    std::vector<int32_t> level_start;
+    std::vector<int32_t> item_target;  // value written by the item
+    std::vector<int32_t> item_aux;     // diagonal position / -1
+    std::vector<int32_t> term_start;   // [n_items + 1]
+    std::vector<int32_t> term_a;       // first operand position
+    std::vector<int32_t> term_b;       // second operand position
+    int32_t n_items() const
+    {
+      return (int32_t)item_target.size();
+    }
+    int32_t n_levels() const
+    {
+      return level_start.empty() ? 0 : (int32_t)level_start.size() - 1;
+    }
+  };
+
+  struct RateDef
+  {
+    int32_t kind = 0;
+    double p[MICMB_RATE_PARAM_STRIDE] = { 0 };  // derived parameters, see rates.cuh
+    int32_t param_col = -1;                     // first custom-parameter column
+    int32_t input_index = 0;                    // reaction index in the input description
+    int32_t n_mult = 0;                         // parameterized reactants
+    double mult[MICMB_MAX_PARAMETERIZED][4] = { { 0 } };
+  };
+
+  struct CompiledMechanism
+  {
+    int32_t S = 0;  // species (state columns)
+    int32_t R = 0;  // reactions (rate columns)
+    int32_t P = 0;  // custom parameters
+    std::vector<int32_t> species_column;   // system species -> column
+    std::vector<int32_t> reaction_column;  // input reaction -> rate column
+    std::vector<int32_t> param_column;     // input reaction -> first custom column or -1
+    std::vector<RateDef> rates;            // [R] by rate column
+
+    // reactants / products per rate column, state columns (parameterized excluded)
+    std::vector<int32_t> react_start, react_ids;
+    std::vector<int32_t> prod_start, prod_ids;
+    std::vector<double> prod_yield;
+
+    // Jacobian: unfilled pattern and LU-filled pattern (row-major storage order)
+    std::vector<std::pair<int32_t, int32_t>> pattern_unfilled;
+    std::vector<int32_t> nz_row, nz_col;  // filled, storage order
+    std::map<std::pair<int32_t, int32_t>, int32_t> position;
+    std::vector<int32_t> diag_pos;  // [S]
+    int32_t nnz = 0;
+
+    // ProcessSet jacobian infos (process_set.hpp:329-391): (independent column, rate column)
+    std::vector<int32_t> info_rxn, info_ind;
+    std::vector<int32_t> info_dep_start, info_dep_ids;  // dependent reactants per info
+
+    // forcing gather: item = species (target column), terms (rate column, coefficient)
+    std::vector<int32_t> f_start, f_rxn;
+    std::vector<double> f_coef;
+    // -J gather: item = nonzero position, terms (info index, coefficient)
+    std::vector<int32_t> j_start, j_info;
+    std::vector<double> j_coef;
+
+    LevelSchedule lu;      // Crout form: target a_jk, aux = diag pos of column k for j > k
+    LevelSchedule fwd;     // L y = b (unit diagonal): target row i, terms (L_ij pos, j)
+    LevelSchedule bwd;     // U x = y: target row i, aux = U_ii pos, terms (U_ij pos, j)
+    LevelSchedule fwd_t;   // U^T w = g: target i, aux = U_ii pos, terms (U_ji pos, j)
+    LevelSchedule bwd_t;   // L^T z = w: target i, terms (L_ji pos, j)
+
+    int32_t lu_updates = 0;
+    int32_t lu_lower = 0;
+    uint64_t hash = 0;
+  };
+
+  // Throws std::runtime_error on invalid input.
+  CompiledMechanism Compile(const micmb_mechanism_desc& desc);
+
+  // Markowitz reorder of a square 0/1 pattern given as per-row column sets;
+  // returns perm with perm[new] = old (linear_solver.inl:30-124).
+  std::vector<int32_t> DiagonalMarkowitz(int32_t n, const std::vector<std::pair<int32_t, int32_t>>& nonzeros);
+}  // namespace micmb

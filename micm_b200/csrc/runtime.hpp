@@ -1,0 +1,145 @@
+// runtime.hpp -- host-side objects behind the C ABI handles.
+#pragma once
+
+#include "device.cuh"
+#include "mechanism.hpp"
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+struct micmb_mechanism
+{
+  micmb::CompiledMechanism m;
+};
+
+namespace micmb
+{
+  // exception carrying a C-ABI status code
+  struct Error : std::runtime_error
+  {
+    int code;
+    Error(int c, const std::string& what)
+        : std::runtime_error(what),
+          code(c)
+    {
+    }
+  };
+
+  void CudaCheck(cudaError_t e, const char* what);
+#define MICMB_CUDA(call) ::micmb::CudaCheck((call), #call)
+
+  // owning device allocation
+  struct DeviceMemory
+  {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DeviceMemory() = default;
+    explicit DeviceMemory(size_t b);
+    ~DeviceMemory();
+    DeviceMemory(const DeviceMemory&) = delete;
+    DeviceMemory& operator=(const DeviceMemory&) = delete;
+    DeviceMemory(DeviceMemory&& o) noexcept
+        : p(o.p),
+          bytes(o.bytes)
+    {
+      o.p = nullptr;
+      o.bytes = 0;
+    }
+    DeviceMemory& operator=(DeviceMemory&& o) noexcept;
+    template<class T>
+    T* as() const
+    {
+      return static_cast<T*>(p);
+    }
+  };
+
+  DevParams ToDevParams(const micmb_rosenbrock_params& p);
+
+  // per-launch arguments of the fused kernel
+  struct FusedArgs
+  {
+    int64_t n_cells;
+    int32_t L;
+    const double* variables_in;
+    double* variables_out;
+    const double* rate_constants;
+    const double* atol;
+    double rtol;
+    int32_t* next_cell;          // work-stealing counter
+    int32_t* cell_status;        // [n_cells] or null
+    int32_t* cell_accepted;      // [n_cells] or null
+    unsigned long long* stats;   // [8] accumulators
+    double* lu_global;           // per-warp LU slots when not staged in shared memory
+    int64_t lu_slot_stride;      // doubles per slot
+    // adjoint checkpoints (null for a plain forward solve)
+    double* ckpt_y;              // [n_cells][max_ckpt][S]
+    double* ckpt_h;              // [n_cells][max_ckpt]
+    int32_t max_ckpt;
+  };
+}  // namespace micmb
+
+struct micmb_solver
+{
+  std::shared_ptr<const micmb::CompiledMechanism> mech;
+  int device = 0;
+  int sm_count = 0;
+  size_t smem_optin = 0;
+  micmb::DeviceMemory tables;
+  micmb::DeviceMemory scale_dev;  // [R] by rate column
+  micmb::DevMech dev{};
+  const int32_t* diag_row_of = nullptr;  // [nnz]: row if diagonal, else -1
+  micmb_rosenbrock_params host_params{};
+  micmb::DevParams params{};
+  micmb_fused_config fused{ 0, 1, 0 };
+};
+
+struct micmb_state
+{
+  micmb_solver* solver = nullptr;
+  int64_t n_cells = 0;
+  int32_t L = 1;
+  int64_t n_groups = 0;
+  int64_t n_pad = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  double rtol = 1e-6;
+
+  micmb::DeviceMemory variables, custom_params, rate_constants, conditions, atol;
+  // plain-path working set (allocated on first use)
+  micmb::DeviceMemory jacobian, forcing0, fcur, ynew, stages, scratch, inv_diag, err_cell;
+  micmb::DeviceMemory ctl, status, accepted;
+  micmb::DeviceMemory counters;  // device counters / stats accumulators
+  int32_t* host_counters = nullptr;  // pinned
+  // fused path
+  micmb::DeviceMemory lu_slots;
+  int64_t lu_slot_count = 0;
+
+  size_t dense_bytes(int32_t ncols) const
+  {
+    return (size_t)n_pad * (size_t)ncols * sizeof(double);
+  }
+};
+
+namespace micmb
+{
+  void EnsurePlainBuffers(micmb_state& st);
+  // plain path: one kernel per stage; returns after the whole solve
+  void SolvePlain(micmb_solver& s, micmb_state& st, double dt, int32_t step_control, micmb_solver_stats* stats,
+                  int32_t* per_cell_status, int32_t* per_cell_accepted);
+  void SolveFused(micmb_solver& s, micmb_state& st, double dt, micmb_solver_stats* stats, int32_t* per_cell_status,
+                  int32_t* per_cell_accepted, const FusedArgs* adjoint_ckpt);
+  void LaunchRateConstants(micmb_solver& s, micmb_state& st);
+  // single-stage launchers (per-kernel parity entry points)
+  void LaunchAddForcing(micmb_solver& s, micmb_state& st);
+  void LaunchSubtractJacobian(micmb_solver& s, micmb_state& st);
+  void LaunchAlphaMinusJacobian(micmb_solver& s, micmb_state& st, double alpha);
+  void LaunchDecompose(micmb_solver& s, micmb_state& st);
+  void LaunchLinearSolve(micmb_solver& s, micmb_state& st);
+  void NormalizedError(micmb_solver& s, micmb_state& st, double* global_out, double* per_cell_out);
+  size_t FusedSharedBytes(const micmb_solver& s, bool lu_in_shared);
+  int FusedWarpsPerCta(const micmb_solver& s, const micmb_fused_config& cfg);
+}  // namespace micmb

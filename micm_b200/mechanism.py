@@ -1,0 +1,200 @@
+"""Mechanism description in micm's vocabulary, flattened for the C ABI.
+
+A :class:`Mechanism` is what micm builds from ``System`` + ``std::vector<Process>``
+(include/micm/system/system.hpp, include/micm/process/chemical_reaction_builder.hpp):
+species in gas-phase order, reactions with a rate-constant kind and its
+parameters, reactants (possibly parameterized, e.g. a third body M) and
+products with yields.  :meth:`Mechanism.flat` turns it into the arrays of
+``micmb_mechanism_desc`` (include/micmb.h).
+
+Rate-constant kinds use micm's sort key (solver_builder.inl:274-329) so the
+column order of ``rate_constants`` matches the reference solver.
+"""
+from __future__ import annotations
+
+import dataclasses
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+ARRHENIUS = 0
+TROE = 1
+TERNARY_CHEMICAL_ACTIVATION = 2
+BRANCHED = 3
+TUNNELING = 4
+TAYLOR_SERIES = 5
+REVERSIBLE = 6
+USER_DEFINED = 7
+SURFACE = 8
+
+RATE_PARAM_STRIDE = 24
+
+# micm::constants (include/micm/util/constants.hpp)
+BOLTZMANN_CONSTANT = 1.380649e-23
+AVOGADRO_CONSTANT = 6.02214076e23
+GAS_CONSTANT = BOLTZMANN_CONSTANT * AVOGADRO_CONSTANT
+
+
+def arrhenius(A=1.0, B=0.0, C=0.0, D=300.0, E=0.0):
+    """ArrheniusRateConstantParameters (arrhenius_rate_constant.hpp:9-22)."""
+    return (ARRHENIUS, [A, B, C, D, E])
+
+
+def troe(k0_A=1.0, k0_B=0.0, k0_C=0.0, kinf_A=1.0, kinf_B=0.0, kinf_C=0.0, Fc=0.6, N=1.0):
+    """TroeRateConstantParameters (troe_rate_constant.hpp)."""
+    return (TROE, [k0_A, k0_B, k0_C, kinf_A, kinf_B, kinf_C, Fc, N])
+
+
+def ternary(k0_A=1.0, k0_B=0.0, k0_C=0.0, kinf_A=1.0, kinf_B=0.0, kinf_C=0.0, Fc=0.6, N=1.0):
+    """TernaryChemicalActivationRateConstantParameters."""
+    return (TERNARY_CHEMICAL_ACTIVATION, [k0_A, k0_B, k0_C, kinf_A, kinf_B, kinf_C, Fc, N])
+
+
+def branched(branch, X, Y, a0, n):
+    """BranchedRateConstantParameters; branch 0 = alkoxy, 1 = nitrate."""
+    return (BRANCHED, [float(branch), X, Y, a0, float(n)])
+
+
+def tunneling(A=1.0, B=0.0, C=0.0):
+    """TunnelingRateConstantParameters."""
+    return (TUNNELING, [A, B, C])
+
+
+def taylor_series(A=1.0, B=0.0, C=0.0, D=300.0, E=0.0, coefficients=(1.0,)):
+    """TaylorSeriesRateConstantParameters (up to 16 coefficients)."""
+    coefficients = list(coefficients)
+    if not 1 <= len(coefficients) <= 16:
+        raise ValueError("TaylorSeries takes 1..16 coefficients")
+    return (TAYLOR_SERIES, [A, B, C, D, E, float(len(coefficients))] + coefficients)
+
+
+def reversible(A=1.0, C=0.0, k_r=0.0):
+    """ReversibleRateConstantParameters."""
+    return (REVERSIBLE, [A, C, k_r])
+
+
+def user_defined(label, scaling_factor=1.0):
+    """UserDefinedRateConstantParameters: k = custom parameter * scaling."""
+    return (USER_DEFINED, [scaling_factor], label)
+
+
+def surface(label, diffusion_coefficient, molecular_weight, reaction_probability=1.0):
+    """SurfaceRateConstantParameters; custom parameters
+    ``label.effective radius [m]`` and ``label.particle number concentration [# m-3]``."""
+    return (SURFACE, [diffusion_coefficient, molecular_weight, reaction_probability], label)
+
+
+@dataclasses.dataclass
+class Reaction:
+    kind: int
+    params: List[float]
+    reactants: List[int]                   # >=0 species, -(p+1) parameterized p
+    products: List[Tuple[int, float]]      # (species, yield)
+    label: Optional[str] = None            # custom parameter label (UD / surface)
+
+
+@dataclasses.dataclass
+class Mechanism:
+    species: List[str]
+    reactions: List[Reaction]
+    parameterized: List[Tuple[float, float, float, float]] = dataclasses.field(default_factory=list)
+    absolute_tolerance: Optional[np.ndarray] = None   # per species, system order
+    relative_tolerance: float = 1e-6
+    reorder_state: bool = True
+    name: str = "mechanism"
+
+    @property
+    def n_species(self) -> int:
+        return len(self.species)
+
+    @property
+    def n_reactions(self) -> int:
+        return len(self.reactions)
+
+    def add(self, rate, reactants: Sequence[int], products: Sequence[Tuple[int, float]]):
+        kind, params = rate[0], list(rate[1])
+        label = rate[2] if len(rate) > 2 else None
+        self.reactions.append(Reaction(kind, params, list(reactants), list(products), label))
+
+    def custom_param_labels(self) -> List[str]:
+        """Labels in micm's order: reactions stably sorted by kind, UD then
+        surface labels in that order (solver_builder.inl:129-188)."""
+        order = sorted(range(self.n_reactions), key=lambda r: self.reactions[r].kind)
+        labels: List[str] = []
+        for r in order:
+            rx = self.reactions[r]
+            if rx.kind == USER_DEFINED:
+                labels.append(rx.label)
+            elif rx.kind == SURFACE:
+                labels.append(rx.label + ".effective radius [m]")
+                labels.append(rx.label + ".particle number concentration [# m-3]")
+        if len(set(labels)) != len(labels):
+            raise ValueError("duplicate custom parameter labels")
+        return labels
+
+    def flat(self) -> Dict[str, np.ndarray]:
+        """Arrays of micmb_mechanism_desc (include/micmb.h)."""
+        R = self.n_reactions
+        rate_type = np.array([rx.kind for rx in self.reactions], dtype=np.int32)
+        rate_params = np.zeros((R, RATE_PARAM_STRIDE), dtype=np.float64)
+        for r, rx in enumerate(self.reactions):
+            rate_params[r, : len(rx.params)] = rx.params
+        rstart = np.zeros(R + 1, dtype=np.int32)
+        pstart = np.zeros(R + 1, dtype=np.int32)
+        rs, ps, py = [], [], []
+        for r, rx in enumerate(self.reactions):
+            rs.extend(rx.reactants)
+            for s, y in rx.products:
+                ps.append(s)
+                py.append(y)
+            rstart[r + 1] = len(rs)
+            pstart[r + 1] = len(ps)
+        pc = np.array(self.parameterized, dtype=np.float64).reshape(-1)
+        return dict(
+            n_species=self.n_species,
+            n_reactions=R,
+            rate_type=rate_type,
+            rate_params=rate_params.reshape(-1).copy(),
+            reactant_start=rstart,
+            reactant_species=np.array(rs, dtype=np.int32),
+            product_start=pstart,
+            product_species=np.array(ps, dtype=np.int32),
+            product_yield=np.array(py, dtype=np.float64),
+            n_parameterized=len(self.parameterized),
+            parameterized_coef=pc if pc.size else np.zeros(1, dtype=np.float64),
+            reorder_state=1 if self.reorder_state else 0,
+        )
+
+    def atol(self) -> np.ndarray:
+        if self.absolute_tolerance is None:
+            return np.full(self.n_species, 1e-3)   # SolverBuilder default (solver_builder.inl:208)
+        return np.asarray(self.absolute_tolerance, dtype=np.float64)
+
+
+def ideal_air_density(pressure, temperature):
+    """Conditions::CalculateIdealAirDensity (include/micm/system/conditions.hpp:20-23)."""
+    return np.asarray(pressure) / (GAS_CONSTANT * np.asarray(temperature))
+
+
+# --------------------------------------------------------------------------
+# Vector-ordered layout helpers (include/micm/util/vector_matrix.hpp:254-345)
+# --------------------------------------------------------------------------
+
+def padded_cells(n_cells: int, L: int) -> int:
+    return -(-n_cells // L) * L
+
+
+def to_vector_layout(a: np.ndarray, L: int) -> np.ndarray:
+    """[cell][col] -> flat vector-ordered array with groups of L cells."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    n, m = a.shape
+    npad = padded_cells(n, L)
+    buf = np.zeros((npad, m), dtype=np.float64)
+    buf[:n] = a
+    return buf.reshape(npad // L, L, m).transpose(0, 2, 1).reshape(-1).copy()
+
+
+def from_vector_layout(buf: np.ndarray, n_cells: int, n_cols: int, L: int) -> np.ndarray:
+    npad = padded_cells(n_cells, L)
+    a = np.asarray(buf).reshape(npad // L, n_cols, L).transpose(0, 2, 1).reshape(npad, n_cols)
+    return a[:n_cells].copy()

@@ -1,0 +1,200 @@
+"""TEST INFRASTRUCTURE: checkers for the B200 solver.  Only tests/,
+__graft_entry__.smoke() and bench.py's CPU-baseline leg import this package;
+the product never does.
+
+Two checkers live here:
+
+* :class:`Reference` -- micm itself (oracle/_ref/libmicm_ref.so, built from the
+  reference's own headers by oracle/Makefile through ref_bridge.cpp).
+* :class:`Restatement` -- oracle.c, a plain-C restatement of micm's Rosenbrock
+  path plus the discrete adjoint micm does not have (oracle/liboracle.so).
+
+Arrays at these interfaces are row-major [cell][column] in state columns
+(species after Markowitz reordering, reactions after the type sort).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Dict, Optional
+
+import numpy as np
+
+from micm_b200._abi import DescHolder
+from micm_b200.mechanism import Mechanism
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(HERE, "_ref", "libmicm_ref.so")
+ORACLE_LIB = os.path.join(HERE, "liboracle.so")
+
+_f64p = C.POINTER(C.c_double)
+_i32p = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+
+STATS_FIELDS = ("function_calls", "jacobian_updates", "number_of_steps", "accepted", "rejected",
+                "decompositions", "solves", "state")
+
+
+def _p(a, t=C.c_double):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+_ref = None
+
+
+def reference_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def _load_ref():
+    global _ref
+    if _ref is None:
+        lib = C.CDLL(REF_LIB)
+        lib.mref_last_error.restype = C.c_char_p
+        lib.mref_create.restype = C.c_void_p
+        lib.mref_create.argtypes = [C.c_void_p, _f64p, C.c_double, C.c_int]
+        lib.mref_destroy.argtypes = [C.c_void_p]
+        for name in ("mref_species_columns", "mref_reaction_columns", "mref_custom_param_columns"):
+            getattr(lib, name).argtypes = [C.c_void_p, _i32p]
+        lib.mref_n_custom_params.argtypes = [C.c_void_p]
+        lib.mref_jacobian_pattern.argtypes = [C.c_void_p, _i32p, _i32p]
+        lib.mref_rate_constants.argtypes = [C.c_void_p, C.c_int, _f64p, _f64p, _f64p, _f64p, _f64p]
+        lib.mref_forcing.argtypes = [C.c_void_p, C.c_int, _f64p, _f64p, _f64p]
+        lib.mref_jacobian.argtypes = [C.c_void_p, C.c_int, _f64p, _f64p, _f64p]
+        lib.mref_decompose.argtypes = [C.c_void_p, C.c_int, _f64p]
+        lib.mref_linear_solve.argtypes = [C.c_void_p, C.c_int, _f64p, _f64p]
+        lib.mref_normalized_error.restype = C.c_double
+        lib.mref_normalized_error.argtypes = [C.c_void_p, C.c_int, _f64p, _f64p, _f64p, _f64p, C.c_double]
+        lib.mref_solve_global.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, _f64p, _f64p, _f64p,
+                                          _f64p, _f64p, _i64p]
+        lib.mref_solve_per_cell.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, _f64p, _f64p, _f64p,
+                                            _f64p, _f64p, _i64p, C.c_int]
+        _ref = lib
+    return _ref
+
+
+def _stats_rows(raw: np.ndarray):
+    out = []
+    for row in raw:
+        d = {k: int(row[i]) for i, k in enumerate(STATS_FIELDS)}
+        d["final_time"] = float(row[8:9].view(np.float64)[0])
+        out.append(d)
+    return out
+
+
+class Reference:
+    """micm's own CPU Rosenbrock (in-place Mozart LU, vector ordering)."""
+
+    def __init__(self, mech: Mechanism, tableau: int = 3):
+        self.lib = _load_ref()
+        self.mech = mech
+        self._desc = DescHolder(mech.flat())
+        atol = np.ascontiguousarray(mech.atol())
+        self.handle = self.lib.mref_create(C.byref(self._desc.desc), _p(atol), mech.relative_tolerance,
+                                           int(tableau))
+        if not self.handle:
+            raise RuntimeError("mref_create: " + self.lib.mref_last_error().decode())
+        S, R = mech.n_species, mech.n_reactions
+        self.S, self.R = S, R
+        self.species_columns = np.zeros(S, np.int32)
+        self.lib.mref_species_columns(self.handle, _p(self.species_columns, C.c_int32))
+        self.reaction_columns = np.zeros(R, np.int32)
+        self.lib.mref_reaction_columns(self.handle, _p(self.reaction_columns, C.c_int32))
+        self.param_columns = np.zeros(R, np.int32)
+        self.lib.mref_custom_param_columns(self.handle, _p(self.param_columns, C.c_int32))
+        self.n_params = self.lib.mref_n_custom_params(self.handle)
+        nnz = self.lib.mref_jacobian_pattern(self.handle, None, None)
+        self.rows = np.zeros(nnz, np.int32)
+        self.cols = np.zeros(nnz, np.int32)
+        self.lib.mref_jacobian_pattern(self.handle, _p(self.rows, C.c_int32), _p(self.cols, C.c_int32))
+        self.nnz = nnz
+        self.atol_columns = np.zeros(S)
+        self.atol_columns[self.species_columns] = atol
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            self.lib.mref_destroy(self.handle)
+            self.handle = None
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RuntimeError(self.lib.mref_last_error().decode())
+
+    # system order -> state columns
+    def y_to_columns(self, y_sys: np.ndarray) -> np.ndarray:
+        out = np.zeros_like(y_sys)
+        out[:, self.species_columns] = y_sys
+        return np.ascontiguousarray(out)
+
+    def y_from_columns(self, y_cols: np.ndarray) -> np.ndarray:
+        return np.ascontiguousarray(y_cols[:, self.species_columns])
+
+    def params_to_columns(self, params_labels: np.ndarray) -> np.ndarray:
+        """custom params in label order (Mechanism.custom_param_labels) -> micm columns.
+        Label order and micm's column order coincide by construction; kept explicit."""
+        return np.ascontiguousarray(params_labels.reshape(len(params_labels), -1))
+
+    def rate_constants(self, T, P, rho, params):
+        n = len(T)
+        k = np.zeros((n, self.R))
+        params = np.ascontiguousarray(params if params.size else np.zeros((n, 1)))
+        self._check(self.lib.mref_rate_constants(self.handle, n, _p(np.ascontiguousarray(T)),
+                                                 _p(np.ascontiguousarray(P)), _p(np.ascontiguousarray(rho)),
+                                                 _p(params), _p(k)))
+        return k
+
+    def forcing(self, k, y_cols):
+        n = len(k)
+        f = np.zeros((n, self.S))
+        self._check(self.lib.mref_forcing(self.handle, n, _p(np.ascontiguousarray(k)),
+                                          _p(np.ascontiguousarray(y_cols)), _p(f)))
+        return f
+
+    def jacobian(self, k, y_cols):
+        n = len(k)
+        j = np.zeros((n, self.nnz))
+        self._check(self.lib.mref_jacobian(self.handle, n, _p(np.ascontiguousarray(k)),
+                                           _p(np.ascontiguousarray(y_cols)), _p(j)))
+        return j
+
+    def decompose(self, a):
+        lu = np.ascontiguousarray(a, dtype=np.float64).copy()
+        self._check(self.lib.mref_decompose(self.handle, len(lu), _p(lu)))
+        return lu
+
+    def linear_solve(self, lu, b):
+        x = np.ascontiguousarray(b, dtype=np.float64).copy()
+        self._check(self.lib.mref_linear_solve(self.handle, len(x), _p(np.ascontiguousarray(lu)), _p(x)))
+        return x
+
+    def normalized_error(self, y, ynew, err, rtol=None):
+        rtol = self.mech.relative_tolerance if rtol is None else rtol
+        return self.lib.mref_normalized_error(self.handle, len(y), _p(np.ascontiguousarray(y)),
+                                              _p(np.ascontiguousarray(ynew)), _p(np.ascontiguousarray(err)),
+                                              _p(self.atol_columns), float(rtol))
+
+    def solve_global(self, inputs: Dict[str, np.ndarray], dt: float, n_solves: int = 1):
+        """One multi-cell State, micm's single step size for all cells."""
+        y = self.y_to_columns(inputs["concentrations"])
+        n = len(y)
+        stats = np.zeros((n_solves, 10), np.int64)
+        params = np.ascontiguousarray(inputs["custom_params"] if inputs["custom_params"].size
+                                      else np.zeros((n, 1)))
+        self._check(self.lib.mref_solve_global(
+            self.handle, n, float(dt), int(n_solves), _p(inputs["temperature"]), _p(inputs["pressure"]),
+            _p(inputs["air_density"]), _p(params), _p(y), _p(stats, C.c_int64)))
+        return self.y_from_columns(y), _stats_rows(stats)
+
+    def solve_per_cell(self, inputs: Dict[str, np.ndarray], dt: float, n_solves: int = 1,
+                       threads: int = 0):
+        """A 1-cell State per cell; returns (y_final [n,S] system order, stats rows per cell)."""
+        y = self.y_to_columns(inputs["concentrations"])
+        n = len(y)
+        stats = np.zeros((n, 10), np.int64)
+        params = np.ascontiguousarray(inputs["custom_params"] if inputs["custom_params"].size
+                                      else np.zeros((n, 1)))
+        threads = threads or (os.cpu_count() or 1)
+        self._check(self.lib.mref_solve_per_cell(
+            self.handle, n, float(dt), int(n_solves), _p(inputs["temperature"]), _p(inputs["pressure"]),
+            _p(inputs["air_density"]), _p(params), _p(y), _p(stats, C.c_int64), int(threads)))
+        return self.y_from_columns(y), stats
