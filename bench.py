@@ -1,0 +1,308 @@
+"""Benchmark: cell-solves/s of the Rosenbrock chemistry solve on the GPU.
+
+Workload (the metric's configuration): seeded 210-species / 440-reaction
+mechanism, 1,048,576 grid cells, half of them at night (photolysis off),
+T ~ U(200, 310) K, four-stage Rosenbrock, one Solve(dt = 600 s) per step,
+per-cell step control.  A step restores the initial concentrations (device
+copy) and solves every cell; inputs (1.8 GB state + 3.7 GB rate constants)
+exceed the 126 MB L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs under torchrun: each rank solves its own 1M-cell shard (weak
+scaling; cells are independent, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-solves/s @1M cells, FP64 rtol1e-6 (fused vs plain); adjoint/forward time"
+UNIT = "cell-solves/s"
+CONFIG_NAME = "c210_uneven"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cells", type=int, default=1048576)
+    ap.add_argument("--plain-cells", type=int, default=262144,
+                    help="cells for the plain-method comparison line (0 = skip)")
+    ap.add_argument("--cpu-sample", type=int, default=4096, help="cells timed on the host CPU")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def workload(cells: int, rank: int = 0):
+    from micm_b200 import synthetic
+    cfg = synthetic.CONFIGS[CONFIG_NAME]
+    mech = cfg["mech"]()
+    inputs = synthetic.cell_inputs(mech, cells, cfg["seed"] + 1000 * rank, **cfg["inputs"])
+    return cfg, mech, inputs
+
+
+def cpu_reference(mech, cfg, inputs, sample: int):
+    """micm's own CPU solver (oracle/_ref) over a bounded sample of the workload."""
+    import oracle
+    if not oracle.reference_available():
+        return None
+    n = min(sample, len(inputs["temperature"]))
+    sub = {k: v[:n] for k, v in inputs.items()}
+    ref = oracle.Reference(mech, tableau=cfg["stages"])
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    ref.solve_per_cell(sub, cfg["dt"], threads=threads)
+    t = time.perf_counter() - t0
+    return {"value": n / t, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{n} cells of the workload, one 1-cell micm State per cell over {threads} host threads, "
+                      f"micm CpuSolverBuilderInPlace (vector ordering L=1, in-place Mozart LU), {t:.1f} s"}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cfg, mech, inputs = workload(min(args.cells, args.cpu_sample * max(1, args.steps + args.warmup)))
+    import oracle
+    if not oracle.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmicm_ref.so was not built"}))
+        return
+    ref = oracle.Reference(mech, tableau=cfg["stages"])
+    threads = os.cpu_count() or 1
+    n = args.cpu_sample
+    times = []
+    for i in range(args.warmup + args.steps):
+        sub = {k: v[(i * n) % len(v):(i * n) % len(v) + n] for k, v in inputs.items()}
+        t0 = time.perf_counter()
+        ref.solve_per_cell(sub, cfg["dt"], threads=threads)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    t = float(np.sum(times))
+    value = n * args.steps / t
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * t / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "impl": "reference",
+            "config": {"workload": f"{CONFIG_NAME}: 210 species, 440 reactions, 4-stage Rosenbrock, dt=600 s, "
+                                   f"per-cell step control; each step a {n}-cell sample",
+                       "cells_per_step": n},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": f"{n} cells per step, 1-cell micm States over {threads} threads"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from micm_b200 import Solver
+    from micm_b200 import solver as sv
+    from micm_b200.mechanism import to_vector_layout, padded_cells
+
+    cfg, mech, inputs = workload(args.cells, rank)
+    L = 128
+    solver = Solver(mech, cfg["stages"], vector_length=L)
+    state = solver.get_state(args.cells)
+    state.set_inputs(inputs)
+    state.sync_inputs_to_device()
+    solver.update_state_parameters(state)
+    S = mech.n_species
+    npad = padded_cells(args.cells, L)
+    y0_host = to_vector_layout(state.variables, L)
+    y_dev = torch.from_numpy(y0_host).cuda()
+    y_view = device_view(state, sv.BUF_VARIABLES)   # torch view of the state's own buffer
+    stream = torch.cuda.current_stream()
+    import ctypes
+    from micm_b200._native import check, lib
+    check(lib().micmb_state_set_stream(state.handle, ctypes.c_void_p(stream.cuda_stream)))
+
+    def restore_torch():
+        y_view.copy_(y_dev)
+
+    warm = args.warmup
+    # warmup
+    for _ in range(warm):
+        restore_torch()
+        res = solver.solve(cfg["dt"], state, method="fused", step_control="per_cell")
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        start.record(stream)
+        stats_sum = None
+        for _ in range(args.steps):
+            restore_torch()
+            res = solver.solve(cfg["dt"], state, method="fused", step_control="per_cell")
+            stats_sum = res.stats
+        end.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = args.cells * world * args.steps / (ms / 1000.0)
+    attempts_per_cell = stats_sum["number_of_steps"] / args.cells
+    accepted_per_cell = stats_sum["accepted"] / args.cells
+
+    # e2e: public API with host buffers every step
+    import torch as _t
+    h_vars = _t.from_numpy(y0_host).pin_memory().numpy()
+    cond = np.stack([state.temperature, state.pressure, state.air_density], axis=1)
+    h_cond = _t.from_numpy(to_vector_layout(cond, L)).pin_memory().numpy()
+    h_par = _t.from_numpy(to_vector_layout(state.custom_rate_parameters, L)).pin_memory().numpy()
+    h_out = _t.empty(h_vars.shape[0], dtype=_t.float64).pin_memory().numpy()
+    e2e_steps = max(1, min(args.steps, 2))
+    _t.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        state.upload(sv.BUF_VARIABLES, h_vars)
+        state.upload(sv.BUF_CONDITIONS, h_cond)
+        state.upload(sv.BUF_CUSTOM_PARAMS, h_par)
+        solver.update_state_parameters(state)
+        solver.solve(cfg["dt"], state, method="fused", step_control="per_cell")
+        check(lib().micmb_state_download(state.handle, sv.BUF_VARIABLES,
+                                         h_out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+    e2e_t = time.perf_counter() - t0
+    h2d = h_vars.nbytes + h_cond.nbytes + h_par.nbytes
+    d2h = h_out.nbytes
+
+    # plain method on a subset (per-stage kernels), for the fused-vs-plain ratio
+    plain = None
+    if args.plain_cells and rank == 0:
+        pc = min(args.plain_cells, args.cells)
+        _, _, pin = workload(pc, rank)
+        pstate = solver.get_state(pc)
+        pstate.set_inputs(pin)
+        pstate.sync_inputs_to_device()
+        solver.update_state_parameters(pstate)
+        _t.cuda.synchronize()
+        t0 = time.perf_counter()
+        pres = solver.solve(cfg["dt"], pstate, method="plain", step_control="per_cell")
+        _t.cuda.synchronize()
+        pt = time.perf_counter() - t0
+        plain = {"value": pc / pt, "unit": UNIT, "cells": pc, "ms": 1000 * pt,
+                 "attempts_per_cell": pres.stats["number_of_steps"] / pc}
+        del pstate
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_reference(mech, cfg, inputs, args.cpu_sample)
+
+    if rank == 0:
+        info = solver.compiled.info
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": f"{CONFIG_NAME}: 210 species, 440 reactions, {args.cells} cells per GPU, "
+                                   "half night, T~U(200,310) K, 4-stage Rosenbrock, dt=600 s, per-cell step control, "
+                                   "fused persistent kernel",
+                       "cells_per_gpu": args.cells, "vector_length": L, "l2": "inputs exceed L2 (5.5 GB)",
+                       "lu_nnz": info["jacobian_nnz"], "lu_updates": info["lu_updates"],
+                       "attempts_per_cell": attempts_per_cell, "accepted_per_cell": accepted_per_cell},
+            "clocks": clocks.summary(),
+            "e2e": {"value": args.cells * e2e_steps / e2e_t, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": args.steps,
+            "plain": plain,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+class _DeviceArray:
+    """__cuda_array_interface__ over a state buffer so torch can view it in place."""
+
+    def __init__(self, ptr: int, count: int):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": "<f8", "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+def device_view(state, buffer):
+    import torch
+    ptr, count = state.device_buffer(buffer)
+    return torch.as_tensor(_DeviceArray(ptr, count), device="cuda")
+
+
+if __name__ == "__main__":
+    main()

@@ -121,6 +121,38 @@ namespace micmb
       return o;
     }
 
+    struct WarpOffsets
+    {
+      size_t lcs, ch, it, tm, cf;
+      int32_t n_levels;
+      bool has_coef;
+    };
+
+    WarpOffsets AddWarp(Packer& pk, const WarpTable& w)
+    {
+      WarpOffsets o;
+      o.lcs = pk.add(w.level_chunk_start);
+      o.ch = pk.add(w.chunk);
+      o.it = pk.add(w.item);
+      o.tm = pk.add(w.term);
+      o.cf = pk.add(w.coef);
+      o.n_levels = w.n_levels;
+      o.has_coef = !w.coef.empty();
+      return o;
+    }
+
+    DevWarpTable ResolveWarp(const char* base, const WarpOffsets& o)
+    {
+      DevWarpTable d;
+      d.n_levels = o.n_levels;
+      d.level_chunk_start = reinterpret_cast<const int32_t*>(base + o.lcs);
+      d.chunk = reinterpret_cast<const int4*>(base + o.ch);
+      d.item = reinterpret_cast<const uint32_t*>(base + o.it);
+      d.term = reinterpret_cast<const uint32_t*>(base + o.tm);
+      d.coef = o.has_coef ? reinterpret_cast<const double*>(base + o.cf) : nullptr;
+      return d;
+    }
+
     DevSchedule Resolve(const char* base, const SchedOffsets& o)
     {
       DevSchedule d;
@@ -163,6 +195,17 @@ namespace micmb
       const size_t o_dp = pk.add(m.diag_pos), o_dro = pk.add(diag_row_of);
       const SchedOffsets lu = AddSchedule(pk, m.lu), fw = AddSchedule(pk, m.fwd), bw = AddSchedule(pk, m.bwd),
                          fwt = AddSchedule(pk, m.fwd_t), bwt = AddSchedule(pk, m.bwd_t);
+      WarpOffsets wl{}, wf{}, wb{}, wft{}, wbt{}, wfo{}, wj{};
+      if (m.has_warp_tables)
+      {
+        wl = AddWarp(pk, m.w_lu);
+        wf = AddWarp(pk, m.w_fwd);
+        wb = AddWarp(pk, m.w_bwd);
+        wft = AddWarp(pk, m.w_fwd_t);
+        wbt = AddWarp(pk, m.w_bwd_t);
+        wfo = AddWarp(pk, m.w_forcing);
+        wj = AddWarp(pk, m.w_jacobian);
+      }
       s.tables = DeviceMemory(pk.bytes.size());
       MICMB_CUDA(cudaMemcpy(s.tables.p, pk.bytes.data(), pk.bytes.size(), cudaMemcpyHostToDevice));
       std::vector<double> ones(std::max<int32_t>(m.R, 1), 1.0);
@@ -200,6 +243,18 @@ namespace micmb
       d.fwd_t = Resolve(b, fwt);
       d.bwd_t = Resolve(b, bwt);
       s.diag_row_of = d.diag_row_of;
+      d.has_warp = m.has_warp_tables ? 1 : 0;
+      d.scratch_zero = m.scratch_zero;
+      if (m.has_warp_tables)
+      {
+        d.w_lu = ResolveWarp(b, wl);
+        d.w_fwd = ResolveWarp(b, wf);
+        d.w_bwd = ResolveWarp(b, wb);
+        d.w_fwd_t = ResolveWarp(b, wft);
+        d.w_bwd_t = ResolveWarp(b, wbt);
+        d.w_forcing = ResolveWarp(b, wfo);
+        d.w_jacobian = ResolveWarp(b, wj);
+      }
     }
 
     template<class F>

@@ -33,6 +33,17 @@ namespace micmb
     const int32_t* tb;
   };
 
+  // lane-interleaved level schedule (mechanism.hpp WarpTable)
+  struct DevWarpTable
+  {
+    int32_t n_levels;
+    const int32_t* level_chunk_start;  // [n_levels + 1]
+    const int4* chunk;                 // term base, T, first item, n items
+    const uint32_t* item;
+    const uint32_t* term;
+    const double* coef;
+  };
+
   struct DevMech
   {
     int32_t S, R, P, nnz, n_info;
@@ -60,6 +71,10 @@ namespace micmb
     const int32_t* diag_pos;     // [S] storage position of a_ii
     const int32_t* diag_row_of;  // [nnz] row i if the position holds a_ii, else -1
     DevSchedule lu, fwd, bwd, fwd_t, bwd_t;
+    // warp-interleaved tables (fused kernel); dummy slots: LU[nnz], x[S], scratch[scratch_zero]
+    int32_t has_warp;
+    int32_t scratch_zero;
+    DevWarpTable w_lu, w_fwd, w_bwd, w_fwd_t, w_bwd_t, w_forcing, w_jacobian;
   };
 
   // Rosenbrock tableau in device-friendly form
@@ -291,6 +306,136 @@ namespace micmb
         x[i] = v / A[sch.aux[it]];
       }
       lane_sync<NL>();
+    }
+  }
+
+  // ---------------------------------------------------------------------
+  // warp-interleaved versions (32 lanes, one cell, shared-memory operands)
+  // ---------------------------------------------------------------------
+  __device__ __forceinline__ int4 load_chunk(const int4* p)
+  {
+    return __ldg(p);
+  }
+
+  // in-place LU; A[nnz] must be 0; inv[S] receives 1/a_ii
+  __device__ __forceinline__ void warp_lu(const DevWarpTable& W, double* A, double* inv, int lane)
+  {
+    for (int32_t l = 0; l < W.n_levels; ++l)
+    {
+      const int32_t c1 = __ldg(W.level_chunk_start + l + 1);
+      for (int32_t ch = __ldg(W.level_chunk_start + l); ch < c1; ++ch)
+      {
+        const int4 c = load_chunk(W.chunk + ch);
+        if (lane < c.w)
+        {
+          const uint32_t it = __ldg(W.item + c.z + lane);
+          const uint32_t e = it & 0xFFFFu, hi = it >> 16;
+          double v = A[e];
+          const uint32_t* tp = W.term + c.x + lane;
+          int32_t t = 0;
+          for (; t + 4 <= c.y; t += 4)
+          {
+            const uint32_t q0 = __ldg(tp + (t + 0) * 32), q1 = __ldg(tp + (t + 1) * 32);
+            const uint32_t q2 = __ldg(tp + (t + 2) * 32), q3 = __ldg(tp + (t + 3) * 32);
+            const double a0 = A[q0 & 0xFFFFu], b0 = A[q0 >> 16], a1 = A[q1 & 0xFFFFu], b1 = A[q1 >> 16];
+            const double a2 = A[q2 & 0xFFFFu], b2 = A[q2 >> 16], a3 = A[q3 & 0xFFFFu], b3 = A[q3 >> 16];
+            v -= a0 * b0;
+            v -= a1 * b1;
+            v -= a2 * b2;
+            v -= a3 * b3;
+          }
+          for (; t < c.y; ++t)
+          {
+            const uint32_t q = __ldg(tp + t * 32);
+            v -= A[q & 0xFFFFu] * A[q >> 16];
+          }
+          if (hi == 0xFFFFu)
+            A[e] = v;
+          else if (hi & 0x8000u)
+          {
+            A[e] = v;
+            inv[hi & 0x7FFFu] = 1.0 / v;
+          }
+          else
+            A[e] = v * inv[hi];
+        }
+      }
+      __syncwarp();
+    }
+  }
+
+  // x_i = (x_i - sum A[a] x[b]) [/ A[aux]]; x[S] and A[nnz] must be 0
+  __device__ __forceinline__ void warp_solve(const DevWarpTable& W, const double* A, double* x, int lane)
+  {
+    for (int32_t l = 0; l < W.n_levels; ++l)
+    {
+      const int32_t c1 = __ldg(W.level_chunk_start + l + 1);
+      for (int32_t ch = __ldg(W.level_chunk_start + l); ch < c1; ++ch)
+      {
+        const int4 c = load_chunk(W.chunk + ch);
+        if (lane < c.w)
+        {
+          const uint32_t it = __ldg(W.item + c.z + lane);
+          const uint32_t i = it & 0xFFFFu, hi = it >> 16;
+          double v = x[i];
+          const uint32_t* tp = W.term + c.x + lane;
+          int32_t t = 0;
+          for (; t + 4 <= c.y; t += 4)
+          {
+            const uint32_t q0 = __ldg(tp + (t + 0) * 32), q1 = __ldg(tp + (t + 1) * 32);
+            const uint32_t q2 = __ldg(tp + (t + 2) * 32), q3 = __ldg(tp + (t + 3) * 32);
+            const double a0 = A[q0 & 0xFFFFu], b0 = x[q0 >> 16], a1 = A[q1 & 0xFFFFu], b1 = x[q1 >> 16];
+            const double a2 = A[q2 & 0xFFFFu], b2 = x[q2 >> 16], a3 = A[q3 & 0xFFFFu], b3 = x[q3 >> 16];
+            v -= a0 * b0;
+            v -= a1 * b1;
+            v -= a2 * b2;
+            v -= a3 * b3;
+          }
+          for (; t < c.y; ++t)
+          {
+            const uint32_t q = __ldg(tp + t * 32);
+            v -= A[q & 0xFFFFu] * x[q >> 16];
+          }
+          x[i] = (hi == 0xFFFFu) ? v : v / A[hi];
+        }
+      }
+      __syncwarp();
+    }
+  }
+
+  // out[target] = sum coef * src[term] (+ alpha on flagged items); src[scratch_zero] must be 0
+  __device__ __forceinline__ void warp_gather(const DevWarpTable& W, const double* src, double* out, double alpha,
+                                              int lane)
+  {
+    const int32_t c1 = __ldg(W.level_chunk_start + 1);
+    for (int32_t ch = 0; ch < c1; ++ch)
+    {
+      const int4 c = load_chunk(W.chunk + ch);
+      if (lane < c.w)
+      {
+        const uint32_t it = __ldg(W.item + c.z + lane);
+        double acc = 0.0;
+        const uint32_t* tp = W.term + c.x + lane;
+        const double* cp = W.coef + c.x + lane;
+        int32_t t = 0;
+        for (; t + 4 <= c.y; t += 4)
+        {
+          const uint32_t q0 = __ldg(tp + (t + 0) * 32), q1 = __ldg(tp + (t + 1) * 32);
+          const uint32_t q2 = __ldg(tp + (t + 2) * 32), q3 = __ldg(tp + (t + 3) * 32);
+          const double f0 = __ldg(cp + (t + 0) * 32), f1 = __ldg(cp + (t + 1) * 32);
+          const double f2 = __ldg(cp + (t + 2) * 32), f3 = __ldg(cp + (t + 3) * 32);
+          const double s0 = src[q0], s1 = src[q1], s2 = src[q2], s3 = src[q3];
+          acc += f0 * s0;
+          acc += f1 * s1;
+          acc += f2 * s2;
+          acc += f3 * s3;
+        }
+        for (; t < c.y; ++t)
+          acc += __ldg(cp + t * 32) * src[__ldg(tp + t * 32)];
+        if ((it >> 16) != 0xFFFFu)
+          acc += alpha;
+        out[it & 0xFFFFu] = acc;
+      }
     }
   }
 

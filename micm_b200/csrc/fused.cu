@@ -21,10 +21,16 @@ namespace micmb
       return (size_t)(c / L) * (size_t)L * (size_t)ncol + (size_t)(c % L);
     }
 
+    // per-warp shared-memory layout (doubles); every vector has one extra zero
+    // slot (index S) that padded table terms read
     struct WarpLayout
     {
       int32_t S, R, stages, scratch_cols, nnz;
-      int32_t per_warp;  // doubles per warp in shared memory
+      int32_t VS;        // vector stride = S + 1 rounded to even
+      int32_t KS;        // rate-constant block
+      int32_t SC;        // scratch block = scratch_cols + 1 rounded to even
+      int32_t LUS;       // LU block = nnz + 1 rounded to even
+      int32_t per_warp;  // doubles per warp
     };
 
     __host__ __device__ inline int32_t RoundUp2(int32_t v)
@@ -41,7 +47,11 @@ namespace micmb
       w.stages = stages;
       w.scratch_cols = R > n_info ? R : n_info;
       w.nnz = nnz;
-      w.per_warp = RoundUp2(S * (5 + stages) + R + w.scratch_cols + (lu_shared ? nnz : 0));
+      w.VS = RoundUp2(S + 1);
+      w.KS = RoundUp2(R > 0 ? R : 1);
+      w.SC = RoundUp2(w.scratch_cols + 1);
+      w.LUS = RoundUp2(nnz + 1);
+      w.per_warp = w.VS * (5 + stages) + w.KS + w.SC + (lu_shared ? w.LUS : 0);
       return w;
     }
 
@@ -62,16 +72,28 @@ namespace micmb
       const int warps = blockDim.x >> 5;
       const int32_t S = M.S, R = M.R, L = A.L;
       double* base = smem + (size_t)warp * W.per_warp;
+      const int32_t VS = W.VS;
       double* Y = base;
-      double* Yn = Y + S;
-      double* F0 = Yn + S;
-      double* Fc = F0 + S;
-      double* inv = Fc + S;
-      double* K = inv + S;
-      double* kk = K + (size_t)P.stages * S;
-      double* scr = kk + R;
-      double* LU = LU_SHARED ? (scr + W.scratch_cols)
+      double* Yn = Y + VS;
+      double* F0 = Yn + VS;
+      double* Fc = F0 + VS;
+      double* inv = Fc + VS;
+      double* K = inv + VS;
+      double* kk = K + (size_t)P.stages * VS;
+      double* scr = kk + W.KS;
+      double* LU = LU_SHARED ? (scr + W.SC)
                              : A.lu_global + ((size_t)blockIdx.x * warps + warp) * (size_t)A.lu_slot_stride;
+      // zero slots read by padded table terms (never written afterwards)
+      if (lane == 0)
+      {
+        for (int32_t st = 0; st < P.stages; ++st)
+          K[(size_t)st * VS + S] = 0.0;
+        Y[S] = 0.0;
+        Yn[S] = 0.0;
+        scr[M.scratch_zero] = 0.0;
+        LU[M.nnz] = 0.0;
+      }
+      __syncwarp();
       long long acc[8] = { 0 };
 
       for (;;)
@@ -107,16 +129,16 @@ namespace micmb
           }
           reaction_rates<kWarp>(M, Unit{ kk }, Unit{ Y }, Unit{ scr }, lane);
           __syncwarp();
-          forcing_gather<kWarp>(M, Unit{ scr }, Unit{ F0 }, lane);
+          warp_gather(M.w_forcing, scr, F0, 0.0, lane);
           __syncwarp();
           for (;;)
           {
             const double alpha = 1.0 / (c.H * P.gamma0);
             jacobian_rates<kWarp>(M, Unit{ kk }, Unit{ Y }, Unit{ scr }, lane);
             __syncwarp();
-            jacobian_gather<kWarp>(M, Unit{ scr }, Unit{ LU }, alpha, true, lane);
+            warp_gather(M.w_jacobian, scr, LU, alpha, lane);
             __syncwarp();
-            lu_decompose<kWarp>(M.lu, M.diag_row_of, Unit{ LU }, Unit{ inv }, lane);
+            warp_lu(M.w_lu, LU, inv, lane);
             const double* Fsrc = F0;
             for (int32_t st = 0; st < P.stages; ++st)
             {
@@ -127,30 +149,30 @@ namespace micmb
                 {
                   double v = Y[i];
                   for (int32_t j = 0; j < st; ++j)
-                    v += P.a[sc + j] * K[(size_t)j * S + i];
+                    v += P.a[sc + j] * K[(size_t)j * VS + i];
                   Yn[i] = v;
                 }
                 __syncwarp();
                 reaction_rates<kWarp>(M, Unit{ kk }, Unit{ Yn }, Unit{ scr }, lane);
                 __syncwarp();
-                forcing_gather<kWarp>(M, Unit{ scr }, Unit{ Fc }, lane);
+                warp_gather(M.w_forcing, scr, Fc, 0.0, lane);
                 __syncwarp();
                 Fsrc = Fc;
               }
-              double* Ks = K + (size_t)st * S;
+              double* Ks = K + (size_t)st * VS;
               for (int32_t i = lane; i < S; i += kWarp)
               {
                 double v = Fsrc[i];
                 for (int32_t j = 0; j < st; ++j)
                 {
                   const double c_over_h = P.c[sc + j] / c.H;
-                  v += c_over_h * K[(size_t)j * S + i];
+                  v += c_over_h * K[(size_t)j * VS + i];
                 }
                 Ks[i] = v;
               }
               __syncwarp();
-              solve_lower<kWarp>(M.fwd, Unit{ LU }, Unit{ Ks }, lane);
-              solve_upper<kWarp>(M.bwd, Unit{ LU }, Unit{ Ks }, lane);
+              warp_solve(M.w_fwd, LU, Ks, lane);
+              warp_solve(M.w_bwd, LU, Ks, lane);
             }
             double part = 0.0;
             for (int32_t i = lane; i < S; i += kWarp)
@@ -159,7 +181,7 @@ namespace micmb
               double e = 0.0;
               for (int32_t st = 0; st < P.stages; ++st)
               {
-                const double kv = K[(size_t)st * S + i];
+                const double kv = K[(size_t)st * VS + i];
                 v += P.m[st] * kv;
                 e += P.e[st] * kv;
               }
@@ -251,6 +273,8 @@ namespace micmb
     const int warps = FusedWarpsPerCta(s, cfg);
     if (warps < 1)
       throw Error(MICMB_ERR_UNSUPPORTED, "mechanism too large for the fused kernel's shared-memory working set");
+    if (!s.dev.has_warp)
+      throw Error(MICMB_ERR_UNSUPPORTED, "mechanism exceeds the fused kernel's 16-bit table positions (nnz <= 65534)");
     const bool lu_shared = cfg.lu_in_shared != 0;
     WarpLayout W = MakeLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz, lu_shared);
     const size_t smem = (size_t)W.per_warp * sizeof(double) * warps;
@@ -294,7 +318,7 @@ namespace micmb
     if (!lu_shared)
     {
       const int64_t slots = grid * warps;
-      const int64_t stride = ((int64_t)m.nnz + 31) & ~31ll;
+      const int64_t stride = ((int64_t)m.nnz + 1 + 31) & ~31ll;
       if (st.lu_slot_count < slots || !st.lu_slots.p)
       {
         st.lu_slots = DeviceMemory(sizeof(double) * (size_t)(slots * stride));

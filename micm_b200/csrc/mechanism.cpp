@@ -81,6 +81,69 @@ namespace micmb
       return s;
     }
 
+    // Lane-interleave a level schedule (see WarpTable).  `meta(i)` packs item i,
+    // `pack(t)` packs term t, `coef` (optional) is per term; padding terms
+    // are `dummy` with coefficient 0.
+    template<class Meta, class Pack>
+    WarpTable BuildWarp(const LevelSchedule& s, Meta meta, Pack pack, uint32_t dummy, const std::vector<double>* coef)
+    {
+      WarpTable w;
+      w.n_levels = s.n_levels();
+      w.level_chunk_start.push_back(0);
+      for (int32_t l = 0; l < w.n_levels; ++l)
+      {
+        for (int32_t first = s.level_start[l]; first < s.level_start[l + 1]; first += 32)
+        {
+          const int32_t n = std::min<int32_t>(32, s.level_start[l + 1] - first);
+          int32_t T = 0;
+          for (int32_t i = first; i < first + n; ++i)
+            T = std::max(T, s.term_start[i + 1] - s.term_start[i]);
+          w.chunk.push_back((int32_t)w.term.size());
+          w.chunk.push_back(T);
+          w.chunk.push_back((int32_t)w.item.size());
+          w.chunk.push_back(n);
+          for (int32_t i = first; i < first + n; ++i)
+            w.item.push_back(meta(i));
+          const size_t base = w.term.size();
+          w.term.resize(base + (size_t)T * 32, dummy);
+          if (coef)
+            w.coef.resize(base + (size_t)T * 32, 0.0);
+          for (int32_t i = first; i < first + n; ++i)
+            for (int32_t t = s.term_start[i]; t < s.term_start[i + 1]; ++t)
+            {
+              const size_t at = base + (size_t)(t - s.term_start[i]) * 32 + (size_t)(i - first);
+              w.term[at] = pack(t);
+              if (coef)
+                w.coef[at] = (*coef)[t];
+            }
+        }
+        w.level_chunk_start.push_back((int32_t)(w.chunk.size() / 4));
+      }
+      return w;
+    }
+
+    // one-level schedule of independent gather items (forcing / -J)
+    LevelSchedule GatherSchedule(const std::vector<int32_t>& start, const std::vector<int32_t>& idx,
+                                 const std::vector<double>& cf, std::vector<double>& coef_out)
+    {
+      std::vector<RawItem> items;
+      const int32_t n = (int32_t)start.size() - 1;
+      for (int32_t i = 0; i < n; ++i)
+      {
+        RawItem it;
+        it.target = i;
+        it.aux = -1;
+        for (int32_t t = start[i]; t < start[i + 1]; ++t)
+          it.terms.push_back({ idx[t], t });  // term_b carries the coefficient index
+        items.push_back(std::move(it));
+      }
+      LevelSchedule s = Schedule(items);
+      coef_out.resize(s.term_b.size());
+      for (size_t t = 0; t < s.term_b.size(); ++t)
+        coef_out[t] = cf[s.term_b[t]];
+      return s;
+    }
+
     uint64_t Fnv(uint64_t h, const void* data, size_t bytes)
     {
       const unsigned char* p = static_cast<const unsigned char*>(data);
@@ -532,7 +595,54 @@ namespace micmb
       m.bwd_t = Schedule(bt);
     }
 
-    // 10. hash of everything the device sees
+    // 10. warp-interleaved tables for the fused kernel (16-bit operand positions)
+    const int32_t scratch_cols = std::max<int32_t>(R, (int32_t)m.info_rxn.size());
+    m.scratch_zero = scratch_cols;
+    if (m.nnz + 1 <= 0xFFFF && S + 1 < 0x7FFF && scratch_cols + 1 <= 0xFFFF)
+    {
+      const uint32_t NZ = (uint32_t)m.nnz, SV = (uint32_t)S;
+      auto pack2 = [](uint32_t a, uint32_t b) { return a | (b << 16); };
+      m.w_lu = BuildWarp(
+          m.lu,
+          [&](int32_t i) {
+            const int32_t e = m.lu.item_target[i];
+            const int32_t j = m.nz_row[e], k = m.nz_col[e];
+            const uint32_t hi = (j < k) ? 0xFFFFu : (j == k ? (0x8000u | (uint32_t)j) : (uint32_t)k);
+            return (uint32_t)e | (hi << 16);
+          },
+          [&](int32_t t) { return pack2((uint32_t)m.lu.term_a[t], (uint32_t)m.lu.term_b[t]); }, pack2(NZ, NZ),
+          nullptr);
+      auto solve_table = [&](const LevelSchedule& s) {
+        return BuildWarp(
+            s,
+            [&](int32_t i) {
+              const uint32_t hi = s.item_aux[i] < 0 ? 0xFFFFu : (uint32_t)s.item_aux[i];
+              return (uint32_t)s.item_target[i] | (hi << 16);
+            },
+            [&](int32_t t) { return pack2((uint32_t)s.term_a[t], (uint32_t)s.term_b[t]); }, pack2(NZ, SV), nullptr);
+      };
+      m.w_fwd = solve_table(m.fwd);
+      m.w_bwd = solve_table(m.bwd);
+      m.w_fwd_t = solve_table(m.fwd_t);
+      m.w_bwd_t = solve_table(m.bwd_t);
+      std::vector<double> fco, jco;
+      const LevelSchedule fs = GatherSchedule(m.f_start, m.f_rxn, m.f_coef, fco);
+      m.w_forcing = BuildWarp(
+          fs, [&](int32_t i) { return (uint32_t)fs.item_target[i] | (0xFFFFu << 16); },
+          [&](int32_t t) { return (uint32_t)fs.term_a[t]; }, (uint32_t)m.scratch_zero, &fco);
+      const LevelSchedule js = GatherSchedule(m.j_start, m.j_info, m.j_coef, jco);
+      m.w_jacobian = BuildWarp(
+          js,
+          [&](int32_t i) {
+            const int32_t e = js.item_target[i];
+            const uint32_t hi = (m.nz_row[e] == m.nz_col[e]) ? (0x8000u | (uint32_t)m.nz_row[e]) : 0xFFFFu;
+            return (uint32_t)e | (hi << 16);
+          },
+          [&](int32_t t) { return (uint32_t)js.term_a[t]; }, (uint32_t)m.scratch_zero, &jco);
+      m.has_warp_tables = true;
+    }
+
+    // 11. hash of everything the device sees
     uint64_t h = 1469598103934665603ull;
     h = Fnv(h, &m.S, sizeof(m.S));
     h = Fnv(h, &m.R, sizeof(m.R));

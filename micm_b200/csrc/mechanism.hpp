@@ -44,6 +44,22 @@ namespace micmb
     }
   };
 
+  // A level schedule re-laid out for a 32-lane warp: the items of a level are
+  // cut into chunks of 32 consecutive items (one per lane); the terms of a
+  // chunk are stored lane-interleaved, term t of lane l at base + 32 t + l,
+  // padded to the chunk's longest item with terms that read zero slots, so
+  // one 128-byte line feeds a whole warp step.  Operands are 16-bit
+  // positions packed in one 32-bit word.
+  struct WarpTable
+  {
+    int32_t n_levels = 0;
+    std::vector<int32_t> level_chunk_start;  // [n_levels + 1]
+    std::vector<int32_t> chunk;              // [n_chunks * 4]: term base, T, first item, n items
+    std::vector<uint32_t> item;              // packed item metadata
+    std::vector<uint32_t> term;              // packed operand pair (a | b << 16)
+    std::vector<double> coef;                // per-term coefficient (gathers with weights)
+  };
+
   struct RateDef
   {
     int32_t kind = 0;
@@ -92,6 +108,13 @@ namespace micmb
     LevelSchedule bwd;     // U x = y: target row i, aux = U_ii pos, terms (U_ij pos, j)
     LevelSchedule fwd_t;   // U^T w = g: target i, aux = U_ii pos, terms (U_ji pos, j)
     LevelSchedule bwd_t;   // L^T z = w: target i, terms (L_ji pos, j)
+
+    // warp-interleaved forms for the fused kernel (empty when the mechanism
+    // exceeds 16-bit positions); dummy operands: LU slot nnz, vector slot S,
+    // scratch slot `scratch_zero`, all holding 0.0
+    bool has_warp_tables = false;
+    int32_t scratch_zero = 0;
+    WarpTable w_lu, w_fwd, w_bwd, w_fwd_t, w_bwd_t, w_forcing, w_jacobian;
 
     int32_t lu_updates = 0;
     int32_t lu_lower = 0;

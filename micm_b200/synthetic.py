@@ -51,7 +51,7 @@ def abc_mechanism(rate1=None, rate2=None) -> Mechanism:
 
 def synthetic_mechanism(n_species: int, n_reactions: int, seed: int,
                         atol: float = 1e-12, hub_fraction: float = 0.07,
-                        window: int = 12) -> Mechanism:
+                        window: int = 12, hub_skew: float = 1.0) -> Mechanism:
     """Seeded gas-phase mechanism (see module docstring)."""
     rng = np.random.default_rng(seed)
     S, R = int(n_species), int(n_reactions)
@@ -76,6 +76,14 @@ def synthetic_mechanism(n_species: int, n_reactions: int, seed: int,
         if j < len(loss_capable):
             primary[loss_capable[j]] = int(o)
 
+    # hub partners follow a Zipf law (weight 1/(rank+1)^hub_skew): as in real
+    # mechanisms, a few oxidants (OH, O3, NO3, ...) take most of the reactions
+    hub_w = 1.0 / np.arange(1, H + 1) ** hub_skew
+    hub_w /= hub_w.sum()
+
+    def hub() -> int:
+        return int(rng.choice(H, p=hub_w))
+
     def downstream(x: int) -> int:
         lo = x + 1
         hi = min(S - 1, x + window)
@@ -90,7 +98,7 @@ def synthetic_mechanism(n_species: int, n_reactions: int, seed: int,
         used_hub = False
         for _ in range(n_prod):
             if (not used_hub) and (rng.random() < 0.3 or not orgs and rng.random() < 0.5):
-                h = int(rng.integers(0, H))
+                h = hub()
                 used_hub = True
                 prods.append(h)
             elif orgs:
@@ -108,11 +116,11 @@ def synthetic_mechanism(n_species: int, n_reactions: int, seed: int,
     for i, kind in enumerate(kinds):
         if kind == "bi":
             if i in primary:
-                reactants = [primary[i], int(rng.integers(0, H))]
+                reactants = [primary[i], hub()]
             elif rng.random() < 0.85:
-                reactants = [int(rng.choice(organics)), int(rng.integers(0, H))]
+                reactants = [int(rng.choice(organics)), hub()]
             else:
-                reactants = [int(rng.integers(0, H)), int(rng.integers(0, H))]
+                reactants = [hub(), hub()]
             A = 10.0 ** rng.uniform(-16, -10) * CM3_MOLEC
             C = rng.uniform(-2000.0, 500.0)
             rate = arrhenius(A=A, C=C)
@@ -122,15 +130,15 @@ def synthetic_mechanism(n_species: int, n_reactions: int, seed: int,
             elif rng.random() < 0.9:
                 reactants = [int(rng.choice(organics))]
             else:
-                reactants = [int(rng.integers(0, H))]
+                reactants = [hub()]
             A = 10.0 ** rng.uniform(-6, -1)
             C = rng.uniform(-2000.0, 500.0)
             rate = arrhenius(A=A, C=C)
         elif kind == "troe":
             if rng.random() < 0.5:
-                reactants = [int(rng.integers(0, H)), int(rng.integers(0, H))]
+                reactants = [hub(), hub()]
             else:
-                reactants = [int(rng.choice(organics)), int(rng.integers(0, H))]
+                reactants = [int(rng.choice(organics)), hub()]
             k0 = 10.0 ** rng.uniform(-33, -29) * CM6_MOLEC2
             kinf = 10.0 ** rng.uniform(-12, -10) * CM3_MOLEC
             rate = troe(k0_A=k0, k0_B=float(rng.uniform(-4.0, 0.0)), kinf_A=kinf,
@@ -141,7 +149,7 @@ def synthetic_mechanism(n_species: int, n_reactions: int, seed: int,
             elif rng.random() < 0.7:
                 reactants = [int(rng.choice(organics))]
             else:
-                reactants = [int(rng.integers(0, H))]
+                reactants = [hub()]
             rate = user_defined(f"PHOTO.j{photo_i:03d}", 1.0)
             photo_i += 1
         m.add(rate, reactants, products_for(reactants))

@@ -198,3 +198,115 @@ class Reference:
             self.handle, n, float(dt), int(n_solves), _p(inputs["temperature"]), _p(inputs["pressure"]),
             _p(inputs["air_density"]), _p(params), _p(y), _p(stats, C.c_int64), int(threads)))
         return self.y_from_columns(y), stats
+
+
+_om = None
+
+
+def _load_oracle():
+    global _om
+    if _om is None:
+        lib = C.CDLL(ORACLE_LIB)
+        lib.om_create.restype = C.c_void_p
+        lib.om_create.argtypes = [C.c_void_p]
+        lib.om_destroy.argtypes = [C.c_void_p]
+        lib.om_last_error.restype = C.c_char_p
+        lib.om_n_params.argtypes = [C.c_void_p]
+        lib.om_nnz.argtypes = [C.c_void_p]
+        lib.om_species_columns.argtypes = [C.c_void_p, _i32p]
+        lib.om_reaction_columns.argtypes = [C.c_void_p, _i32p]
+        lib.om_jacobian_pattern.argtypes = [C.c_void_p, _i32p, _i32p]
+        lib.om_rate_constants.argtypes = [C.c_void_p, C.c_int, _f64p, _f64p, _f64p, _f64p, _f64p]
+        lib.om_solve_per_cell.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, _f64p, _f64p, C.c_double,
+                                          _f64p, _i64p, C.c_int]
+        lib.om_adjoint_per_cell.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, _f64p, _f64p,
+                                            C.c_double, _f64p, _f64p, _f64p, _f64p, _f64p, C.c_int, C.c_int]
+        _om = lib
+    return _om
+
+
+def restatement_available() -> bool:
+    return os.path.exists(ORACLE_LIB)
+
+
+def tableau(kind: int):
+    """micm's tableau in micmb_rosenbrock_params form, restated from
+    rosenbrock_solver_parameters.hpp:152-434 through the reference bridge-free
+    path: the values are the published coefficients (tests check they equal
+    the library's own defaults)."""
+    from micm_b200.solver import RosenbrockSolverParameters
+    return RosenbrockSolverParameters.from_stages(kind)
+
+
+class Restatement:
+    """oracle.c: plain-C restatement of micm's Rosenbrock path + discrete adjoint."""
+
+    def __init__(self, mech: Mechanism, tableau_kind: int = 3, params=None):
+        self.lib = _load_oracle()
+        self.mech = mech
+        self._desc = DescHolder(mech.flat())
+        self.handle = self.lib.om_create(C.byref(self._desc.desc))
+        if not self.handle:
+            raise RuntimeError("om_create: " + self.lib.om_last_error().decode())
+        self.S, self.R = mech.n_species, mech.n_reactions
+        self.params = params if params is not None else tableau(tableau_kind)
+        self.species_columns = np.zeros(self.S, np.int32)
+        self.lib.om_species_columns(self.handle, _p(self.species_columns, C.c_int32))
+        self.reaction_columns = np.zeros(max(self.R, 1), np.int32)
+        self.lib.om_reaction_columns(self.handle, _p(self.reaction_columns, C.c_int32))
+        self.reaction_columns = self.reaction_columns[: self.R]
+        self.nnz = self.lib.om_nnz(self.handle)
+        self.n_params = self.lib.om_n_params(self.handle)
+        self.rows = np.zeros(self.nnz, np.int32)
+        self.cols = np.zeros(self.nnz, np.int32)
+        self.lib.om_jacobian_pattern(self.handle, _p(self.rows, C.c_int32), _p(self.cols, C.c_int32))
+        self.atol_columns = np.zeros(self.S)
+        self.atol_columns[self.species_columns] = mech.atol()
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            self.lib.om_destroy(self.handle)
+            self.handle = None
+
+    def rate_constants(self, T, P, rho, params):
+        n = len(T)
+        k = np.zeros((n, max(self.R, 1)))
+        params = np.ascontiguousarray(params if params.size else np.zeros((n, 1)))
+        self.lib.om_rate_constants(self.handle, n, _p(np.ascontiguousarray(T)), _p(np.ascontiguousarray(P)),
+                                   _p(np.ascontiguousarray(rho)), _p(params), _p(k))
+        return k[:, : self.R]
+
+    def _k(self, inputs):
+        return np.ascontiguousarray(self.rate_constants(inputs["temperature"], inputs["pressure"],
+                                                        inputs["air_density"], inputs["custom_params"]))
+
+    def solve_per_cell(self, inputs, dt, threads=0, k=None):
+        y = np.zeros_like(inputs["concentrations"])
+        y[:, self.species_columns] = inputs["concentrations"]
+        n = len(y)
+        k = self._k(inputs) if k is None else np.ascontiguousarray(k)
+        stats = np.zeros((n, 10), np.int64)
+        rc = self.lib.om_solve_per_cell(self.handle, C.byref(self.params), n, float(dt), _p(k),
+                                        _p(self.atol_columns), self.mech.relative_tolerance, _p(y),
+                                        _p(stats, C.c_int64), int(threads or os.cpu_count() or 1))
+        if rc:
+            raise RuntimeError(self.lib.om_last_error().decode())
+        return np.ascontiguousarray(y[:, self.species_columns]), stats
+
+    def adjoint_per_cell(self, inputs, dt, ybar_final_sys, threads=0, max_steps=512, k=None):
+        """Returns (y_final, dL/dy0, dL/dlogk [n, R input order]) in system order."""
+        n, S = len(inputs["temperature"]), self.S
+        y0 = np.zeros((n, S))
+        y0[:, self.species_columns] = inputs["concentrations"]
+        yb = np.zeros((n, S))
+        yb[:, self.species_columns] = ybar_final_sys
+        k = self._k(inputs) if k is None else np.ascontiguousarray(k)
+        yf = np.zeros((n, S)); yb0 = np.zeros((n, S)); kb = np.zeros((n, max(self.R, 1)))
+        rc = self.lib.om_adjoint_per_cell(self.handle, C.byref(self.params), n, float(dt), _p(k),
+                                          _p(self.atol_columns), self.mech.relative_tolerance, _p(y0), _p(yb),
+                                          _p(yf), _p(yb0), _p(kb), int(max_steps),
+                                          int(threads or os.cpu_count() or 1))
+        if rc:
+            raise RuntimeError(self.lib.om_last_error().decode())
+        return (yf[:, self.species_columns], yb0[:, self.species_columns],
+                kb[:, : self.R][:, self.reaction_columns])

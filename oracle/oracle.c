@@ -1,0 +1,1048 @@
+/*
+ * oracle.c -- TEST INFRASTRUCTURE ONLY: plain-C restatement of micm's
+ * Rosenbrock path and its discrete adjoint.  See oracle.h for the reference
+ * locations each part restates.  Dense n x n maps are used for the symbolic
+ * steps (fine for the test sizes, n <= a few thousand).
+ */
+#define _GNU_SOURCE
+#include "oracle.h"
+
+#include <math.h>
+#include <pthread.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+static __thread char g_err[256];
+
+const char* om_last_error(void)
+{
+  return g_err;
+}
+
+struct om_mech
+{
+  int S, R, P, nnz, n_info;
+  int* species_col;  /* [S] system species -> column */
+  int* reaction_col; /* [R] input reaction -> rate column */
+  int* kind;         /* by rate column */
+  double* rp;        /* [R][MICMB_RATE_PARAM_STRIDE] */
+  int* pcol;
+  int* nmult;
+  double* mult; /* [R][4][4] */
+  int *rs, *rid;  /* reactants by rate column (state columns) */
+  int *ps, *pid;  /* products */
+  double* py;
+  int *info_ind, *info_rxn, *info_ds, *info_dep;
+  int* pos; /* [S*S] storage position or -1 */
+  int *nz_row, *nz_col;
+};
+
+#define NA 6.02214076e23
+#define KB 1.380649e-23
+#define RGAS (KB * NA)
+#define PI 3.14159265358979323846
+
+static void* xcalloc(size_t n, size_t s)
+{
+  void* p = calloc(n ? n : 1, s ? s : 1);
+  if (!p)
+  {
+    fprintf(stderr, "oracle: out of memory\n");
+    abort();
+  }
+  return p;
+}
+
+void om_destroy(om_mech* m)
+{
+  if (!m)
+    return;
+  free(m->species_col);
+  free(m->reaction_col);
+  free(m->kind);
+  free(m->rp);
+  free(m->pcol);
+  free(m->nmult);
+  free(m->mult);
+  free(m->rs);
+  free(m->rid);
+  free(m->ps);
+  free(m->pid);
+  free(m->py);
+  free(m->info_ind);
+  free(m->info_rxn);
+  free(m->info_ds);
+  free(m->info_dep);
+  free(m->pos);
+  free(m->nz_row);
+  free(m->nz_col);
+  free(m);
+}
+
+/* Markowitz (linear_solver.inl:30-124) on a dense 0/1 pattern; perm[new] = old. */
+static void markowitz(int n, unsigned char* M, int* perm)
+{
+  uint64_t* rd = xcalloc(n, sizeof(uint64_t));
+  uint64_t* cd = xcalloc(n, sizeof(uint64_t));
+  unsigned char* alive = xcalloc(n, 1);
+  int* cols = xcalloc(n, sizeof(int));
+  int* ins = xcalloc(n, sizeof(int));
+  for (int i = 0; i < n; ++i)
+  {
+    alive[i] = 1;
+    for (int j = 0; j < n; ++j)
+      if (M[(size_t)i * n + j])
+      {
+        rd[i]++;
+        cd[j]++;
+      }
+  }
+  for (int step = 0; step < n; ++step)
+  {
+    int pivot = n;
+    uint64_t best = UINT64_MAX;
+    for (int v = 0; v < n; ++v)
+    {
+      if (!alive[v])
+        continue;
+      uint64_t cost = (rd[v] - 1u) * (cd[v] - 1u);
+      if (pivot == n || cost < best)
+      {
+        best = cost;
+        pivot = v;
+      }
+    }
+    perm[step] = pivot;
+    alive[pivot] = 0;
+    int nc = 0, ni = 0;
+    for (int c = 0; c < n; ++c)
+      if (c != pivot && alive[c] && M[(size_t)pivot * n + c])
+        cols[nc++] = c;
+    for (int i = 0; i < n; ++i)
+      if (i != pivot && alive[i] && M[(size_t)i * n + pivot])
+        ins[ni++] = i;
+    for (int a = 0; a < ni; ++a)
+      for (int b = 0; b < nc; ++b)
+        if (!M[(size_t)ins[a] * n + cols[b]])
+        {
+          M[(size_t)ins[a] * n + cols[b]] = 1;
+          rd[ins[a]]++;
+          cd[cols[b]]++;
+        }
+    for (int b = 0; b < nc; ++b)
+    {
+      M[(size_t)pivot * n + cols[b]] = 0;
+      cd[cols[b]]--;
+    }
+    for (int a = 0; a < ni; ++a)
+    {
+      M[(size_t)ins[a] * n + pivot] = 0;
+      rd[ins[a]]--;
+    }
+  }
+  free(rd);
+  free(cd);
+  free(alive);
+  free(cols);
+  free(ins);
+}
+
+om_mech* om_create(const micmb_mechanism_desc* d)
+{
+  const int S = d->n_species, R = d->n_reactions;
+  if (S <= 0 || R < 0)
+  {
+    snprintf(g_err, sizeof g_err, "bad sizes");
+    return NULL;
+  }
+  om_mech* m = xcalloc(1, sizeof(om_mech));
+  m->S = S;
+  m->R = R;
+  /* 1. stable counting sort by kind (solver_builder.inl:274-329) */
+  int* order = xcalloc(R, sizeof(int));
+  {
+    int k = 0;
+    for (int kind = 0; kind <= MICMB_RATE_SURFACE; ++kind)
+      for (int r = 0; r < R; ++r)
+        if (d->rate_type[r] == kind)
+          order[k++] = r;
+    if (k != R)
+    {
+      snprintf(g_err, sizeof g_err, "unsupported rate kind");
+      free(order);
+      om_destroy(m);
+      return NULL;
+    }
+  }
+  m->reaction_col = xcalloc(R, sizeof(int));
+  for (int i = 0; i < R; ++i)
+    m->reaction_col[order[i]] = i;
+  /* 2. species columns */
+  m->species_col = xcalloc(S, sizeof(int));
+  unsigned char* M = xcalloc((size_t)S * S, 1);
+  for (int r = 0; r < R; ++r)
+    for (int i = d->reactant_start[r]; i < d->reactant_start[r + 1]; ++i)
+    {
+      int ind = d->reactant_species[i];
+      if (ind < 0)
+        continue;
+      for (int j = d->reactant_start[r]; j < d->reactant_start[r + 1]; ++j)
+        if (d->reactant_species[j] >= 0)
+          M[(size_t)d->reactant_species[j] * S + ind] = 1;
+      for (int j = d->product_start[r]; j < d->product_start[r + 1]; ++j)
+        M[(size_t)d->product_species[j] * S + ind] = 1;
+    }
+  if (d->reorder_state)
+  {
+    int* perm = xcalloc(S, sizeof(int));
+    markowitz(S, M, perm);
+    for (int i = 0; i < S; ++i)
+      m->species_col[perm[i]] = i;
+    free(perm);
+  }
+  else
+    for (int i = 0; i < S; ++i)
+      m->species_col[i] = i;
+  /* 3. tables by rate column */
+  m->kind = xcalloc(R, sizeof(int));
+  m->rp = xcalloc((size_t)R * MICMB_RATE_PARAM_STRIDE, sizeof(double));
+  m->pcol = xcalloc(R, sizeof(int));
+  m->nmult = xcalloc(R, sizeof(int));
+  m->mult = xcalloc((size_t)R * 16, sizeof(double));
+  m->rs = xcalloc(R + 1, sizeof(int));
+  m->ps = xcalloc(R + 1, sizeof(int));
+  const int nre = d->reactant_start[R], npr = d->product_start[R];
+  m->rid = xcalloc(nre, sizeof(int));
+  m->pid = xcalloc(npr, sizeof(int));
+  m->py = xcalloc(npr, sizeof(double));
+  int next_param = 0, nr = 0, np = 0;
+  for (int rc = 0; rc < R; ++rc)
+  {
+    const int r = order[rc];
+    const double* p = d->rate_params + (size_t)r * MICMB_RATE_PARAM_STRIDE;
+    double* q = m->rp + (size_t)rc * MICMB_RATE_PARAM_STRIDE;
+    memcpy(q, p, sizeof(double) * MICMB_RATE_PARAM_STRIDE);
+    m->kind[rc] = d->rate_type[r];
+    m->pcol[rc] = -1;
+    if (m->kind[rc] == MICMB_RATE_BRANCHED)
+    {
+      /* reaction_rate_store.hpp:268-281 */
+      double n = floor(p[4]);
+      double k0 = 2.0e-22 * NA * 1.0e-6 * exp(n);
+      double air_ref = 2.45e19 / NA * 1.0e6;
+      double a = k0 * air_ref;
+      double b = 0.43 * pow(293.0 / 298.0, -8.0);
+      double A_val = a / (1.0 + a / b) * pow(0.41, 1.0 / (1.0 + pow(log10(a / b), 2.0)));
+      q[5] = k0;
+      q[6] = A_val * (1.0 - p[3]) / p[3];
+    }
+    else if (m->kind[rc] == MICMB_RATE_USER_DEFINED)
+    {
+      m->pcol[rc] = next_param;
+      next_param += 1;
+    }
+    else if (m->kind[rc] == MICMB_RATE_SURFACE)
+    {
+      q[1] = 8.0 * RGAS / (PI * p[1]);
+      m->pcol[rc] = next_param;
+      next_param += 2;
+    }
+    for (int i = d->reactant_start[r]; i < d->reactant_start[r + 1]; ++i)
+    {
+      int s = d->reactant_species[i];
+      if (s >= 0)
+        m->rid[nr++] = m->species_col[s];
+      else
+      {
+        const double* c = d->parameterized_coef + 4 * (size_t)(-s - 1);
+        memcpy(m->mult + ((size_t)rc * 4 + m->nmult[rc]) * 4, c, 4 * sizeof(double));
+        m->nmult[rc]++;
+      }
+    }
+    m->rs[rc + 1] = nr;
+    for (int i = d->product_start[r]; i < d->product_start[r + 1]; ++i)
+    {
+      m->pid[np] = m->species_col[d->product_species[i]];
+      m->py[np] = d->product_yield[i];
+      np++;
+    }
+    m->ps[rc + 1] = np;
+  }
+  m->P = next_param;
+  /* 4. jacobian infos (process_set.hpp:329-391): stable by independent column */
+  m->info_ind = xcalloc(nr, sizeof(int));
+  m->info_rxn = xcalloc(nr, sizeof(int));
+  m->info_ds = xcalloc(nr + 1, sizeof(int));
+  m->info_dep = xcalloc(nr * 3 + 1, sizeof(int));
+  {
+    int ni = 0, nd = 0;
+    for (int ind = 0; ind < S; ++ind)
+      for (int rc = 0; rc < R; ++rc)
+        for (int i = m->rs[rc]; i < m->rs[rc + 1]; ++i)
+          if (m->rid[i] == ind)
+          {
+            m->info_ind[ni] = ind;
+            m->info_rxn[ni] = rc;
+            int found = 0;
+            for (int j = m->rs[rc]; j < m->rs[rc + 1]; ++j)
+            {
+              if (m->rid[j] == ind && !found)
+              {
+                found = 1;
+                continue;
+              }
+              m->info_dep[nd++] = m->rid[j];
+            }
+            ni++;
+            m->info_ds[ni] = nd;
+          }
+    m->n_info = ni;
+  }
+  /* 5. sparsity + diagonal, LU fill, storage positions */
+  memset(M, 0, (size_t)S * S);
+  for (int rc = 0; rc < R; ++rc)
+    for (int i = m->rs[rc]; i < m->rs[rc + 1]; ++i)
+    {
+      int ind = m->rid[i];
+      for (int j = m->rs[rc]; j < m->rs[rc + 1]; ++j)
+        M[(size_t)m->rid[j] * S + ind] = 1;
+      for (int j = m->ps[rc]; j < m->ps[rc + 1]; ++j)
+        M[(size_t)m->pid[j] * S + ind] = 1;
+    }
+  for (int i = 0; i < S; ++i)
+    M[(size_t)i * S + i] = 1;
+  for (int i = 0; i < S; ++i)
+    for (int k = i + 1; k < S; ++k)
+      if (M[(size_t)i * S + k])
+        for (int j = i + 1; j < S; ++j)
+          if (M[(size_t)j * S + i])
+            M[(size_t)j * S + k] = 1;
+  m->pos = xcalloc((size_t)S * S, sizeof(int));
+  int nnz = 0;
+  for (size_t i = 0; i < (size_t)S * S; ++i)
+    nnz += M[i];
+  m->nz_row = xcalloc(nnz, sizeof(int));
+  m->nz_col = xcalloc(nnz, sizeof(int));
+  nnz = 0;
+  for (int i = 0; i < S; ++i)
+    for (int j = 0; j < S; ++j)
+    {
+      if (M[(size_t)i * S + j])
+      {
+        m->pos[(size_t)i * S + j] = nnz;
+        m->nz_row[nnz] = i;
+        m->nz_col[nnz] = j;
+        nnz++;
+      }
+      else
+        m->pos[(size_t)i * S + j] = -1;
+    }
+  m->nnz = nnz;
+  free(M);
+  free(order);
+  return m;
+}
+
+int om_n_params(const om_mech* m)
+{
+  return m->P;
+}
+int om_nnz(const om_mech* m)
+{
+  return m->nnz;
+}
+void om_species_columns(const om_mech* m, int32_t* out)
+{
+  for (int i = 0; i < m->S; ++i)
+    out[i] = m->species_col[i];
+}
+void om_reaction_columns(const om_mech* m, int32_t* out)
+{
+  for (int i = 0; i < m->R; ++i)
+    out[i] = m->reaction_col[i];
+}
+void om_jacobian_pattern(const om_mech* m, int32_t* rows, int32_t* cols)
+{
+  for (int e = 0; e < m->nnz; ++e)
+  {
+    rows[e] = m->nz_row[e];
+    cols[e] = m->nz_col[e];
+  }
+}
+
+/* ---------------------------------------------------------------- */
+/* rate constants (rate_constant_functions.hpp:52-136)               */
+/* ---------------------------------------------------------------- */
+static double falloff(const double* p, double T, double rho, double scale)
+{
+  double k0 = p[0] * exp(p[2] / T) * pow(T / 300.0, p[1]);
+  double kinf = p[3] * exp(p[5] / T) * pow(T / 300.0, p[4]);
+  double ratio = k0 * rho / kinf;
+  return k0 * scale / (1.0 + ratio) * pow(p[6], p[7] / (p[7] + pow(log10(ratio), 2.0)));
+}
+
+static double rate_constant(const om_mech* m, int r, double T, double Pr, double rho, const double* prm)
+{
+  const double* p = m->rp + (size_t)r * MICMB_RATE_PARAM_STRIDE;
+  double k = 0.0;
+  switch (m->kind[r])
+  {
+    case MICMB_RATE_ARRHENIUS: k = p[0] * exp(p[2] / T) * pow(T / p[3], p[1]) * (1.0 + p[4] * Pr); break;
+    case MICMB_RATE_TROE: k = falloff(p, T, rho, rho); break;
+    case MICMB_RATE_TERNARY_CHEMICAL_ACTIVATION: k = falloff(p, T, rho, 1.0); break;
+    case MICMB_RATE_BRANCHED:
+    {
+      double a = p[5] * rho;
+      double b = 0.43 * pow(T / 298.0, -8.0);
+      double A_val = a / (1.0 + a / b) * pow(0.41, 1.0 / (1.0 + pow(log10(a / b), 2.0)));
+      double pre = p[1] * exp(-p[2] / T);
+      k = (p[0] == 0.0) ? pre * (p[6] / (p[6] + A_val)) : pre * (A_val / (A_val + p[6]));
+      break;
+    }
+    case MICMB_RATE_TUNNELING: k = p[0] * exp(-p[1] / T + p[2] / (T * T * T)); break;
+    case MICMB_RATE_TAYLOR_SERIES:
+    {
+      double poly = 0.0, tp = 1.0;
+      int n = (int)p[5];
+      for (int j = 0; j < n; ++j, tp *= T)
+        poly += p[6 + j] * tp;
+      k = poly * p[0] * exp(p[2] / T) * pow(T / p[3], p[1]) * (1.0 + p[4] * Pr);
+      break;
+    }
+    case MICMB_RATE_REVERSIBLE: k = p[0] * exp(p[1] / T) * p[2]; break;
+    case MICMB_RATE_USER_DEFINED: k = prm[m->pcol[r]] * p[0]; break;
+    case MICMB_RATE_SURFACE:
+    {
+      double radius = prm[m->pcol[r]], num = prm[m->pcol[r] + 1];
+      double mfs = sqrt(p[1] * T);
+      k = 4.0 * num * PI * radius * radius / (radius / p[0] + 4.0 / (mfs * p[2]));
+      break;
+    }
+  }
+  if (m->nmult[r] > 0)
+  {
+    double v = 1.0;
+    for (int i = 0; i < m->nmult[r]; ++i)
+    {
+      const double* c = m->mult + ((size_t)r * 4 + i) * 4;
+      v *= c[0] + c[1] * T + c[2] * Pr + c[3] * rho;
+    }
+    k *= v;
+  }
+  return k;
+}
+
+void om_rate_constants(const om_mech* m, int n, const double* T, const double* P, const double* rho,
+                       const double* params, double* k_out)
+{
+  for (int c = 0; c < n; ++c)
+    for (int r = 0; r < m->R; ++r)
+      k_out[(size_t)c * m->R + r] = rate_constant(m, r, T[c], P[c], rho[c], params + (size_t)c * m->P);
+}
+
+/* ---------------------------------------------------------------- */
+/* per-cell numerics in micm's scatter order                         */
+/* ---------------------------------------------------------------- */
+static void forcing(const om_mech* m, const double* k, const double* y, double* f)
+{
+  for (int s = 0; s < m->S; ++s)
+    f[s] = 0.0;
+  for (int r = 0; r < m->R; ++r)
+  {
+    double rate = k[r];
+    for (int i = m->rs[r]; i < m->rs[r + 1]; ++i)
+      rate *= y[m->rid[i]];
+    for (int i = m->rs[r]; i < m->rs[r + 1]; ++i)
+      f[m->rid[i]] -= rate;
+    for (int i = m->ps[r]; i < m->ps[r + 1]; ++i)
+      f[m->pid[i]] += m->py[i] * rate;
+  }
+}
+
+/* jac = -J (process_set.hpp:594-670) */
+static void neg_jacobian(const om_mech* m, const double* k, const double* y, double* jac)
+{
+  const int S = m->S;
+  for (int e = 0; e < m->nnz; ++e)
+    jac[e] = 0.0;
+  for (int q = 0; q < m->n_info; ++q)
+  {
+    int rc = m->info_rxn[q], ind = m->info_ind[q];
+    double d = k[rc];
+    for (int i = m->info_ds[q]; i < m->info_ds[q + 1]; ++i)
+      d *= y[m->info_dep[i]];
+    for (int i = m->info_ds[q]; i < m->info_ds[q + 1]; ++i)
+      jac[m->pos[(size_t)m->info_dep[i] * S + ind]] += d;
+    jac[m->pos[(size_t)ind * S + ind]] += d;
+    for (int i = m->ps[rc]; i < m->ps[rc + 1]; ++i)
+      jac[m->pos[(size_t)m->pid[i] * S + ind]] -= m->py[i] * d;
+  }
+}
+
+static void decompose(const om_mech* m, double* A)
+{
+  const int S = m->S;
+  for (int i = 0; i < S; ++i)
+  {
+    double inv = 1.0 / A[m->pos[(size_t)i * S + i]];
+    for (int j = i + 1; j < S; ++j)
+    {
+      int pji = m->pos[(size_t)j * S + i];
+      if (pji >= 0)
+        A[pji] *= inv;
+    }
+    for (int k = i + 1; k < S; ++k)
+    {
+      int pik = m->pos[(size_t)i * S + k];
+      if (pik < 0)
+        continue;
+      for (int j = i + 1; j < S; ++j)
+      {
+        int pji = m->pos[(size_t)j * S + i];
+        if (pji < 0)
+          continue;
+        A[m->pos[(size_t)j * S + k]] -= A[pji] * A[pik];
+      }
+    }
+  }
+}
+
+static void lu_solve(const om_mech* m, const double* A, double* x)
+{
+  const int S = m->S;
+  for (int i = 0; i < S; ++i)
+    for (int j = 0; j < i; ++j)
+    {
+      int p = m->pos[(size_t)i * S + j];
+      if (p >= 0)
+        x[i] -= A[p] * x[j];
+    }
+  for (int i = S - 1; i >= 0; --i)
+  {
+    for (int j = i + 1; j < S; ++j)
+    {
+      int p = m->pos[(size_t)i * S + j];
+      if (p >= 0)
+        x[i] -= A[p] * x[j];
+    }
+    x[i] /= A[m->pos[(size_t)i * S + i]];
+  }
+}
+
+/* (LU)^T z = g : U^T w = g, then L^T z = w */
+static void lu_solve_transposed(const om_mech* m, const double* A, double* x)
+{
+  const int S = m->S;
+  for (int i = 0; i < S; ++i)
+  {
+    for (int j = 0; j < i; ++j)
+    {
+      int p = m->pos[(size_t)j * S + i];
+      if (p >= 0)
+        x[i] -= A[p] * x[j];
+    }
+    x[i] /= A[m->pos[(size_t)i * S + i]];
+  }
+  for (int i = S - 1; i >= 0; --i)
+    for (int j = i + 1; j < S; ++j)
+    {
+      int p = m->pos[(size_t)j * S + i];
+      if (p >= 0)
+        x[i] -= A[p] * x[j];
+    }
+}
+
+/* ---------------------------------------------------------------- */
+/* Rosenbrock (rosenbrock.inl:12-402) for one cell                   */
+/* ---------------------------------------------------------------- */
+typedef struct
+{
+  double* Y;
+  double* Ynew;
+  double* F0;
+  double* K;
+  double* Yerr;
+  double* J;
+  double* scratch; /* adjoint workspace */
+} work_t;
+
+static void work_alloc(work_t* w, const om_mech* m, int stages)
+{
+  const int S = m->S;
+  w->Y = xcalloc(S, sizeof(double));
+  w->Ynew = xcalloc(S, sizeof(double));
+  w->F0 = xcalloc(S, sizeof(double));
+  w->K = xcalloc((size_t)stages * S, sizeof(double));
+  w->Yerr = xcalloc(S, sizeof(double));
+  w->J = xcalloc(m->nnz, sizeof(double));
+  w->scratch = xcalloc((size_t)(4 * stages + 8) * S + m->R, sizeof(double));
+}
+
+static void work_free(work_t* w)
+{
+  free(w->Y);
+  free(w->Ynew);
+  free(w->F0);
+  free(w->K);
+  free(w->Yerr);
+  free(w->J);
+  free(w->scratch);
+}
+
+static double dmin(double a, double b)
+{
+  return (b < a) ? b : a; /* std::min */
+}
+static double dmax(double a, double b)
+{
+  return (a < b) ? b : a; /* std::max */
+}
+
+/* returns state; stats[0..6]; optionally records accepted (y_n, H_n) */
+static int rosenbrock_cell(const om_mech* m, const micmb_rosenbrock_params* p, double dt, const double* k,
+                           const double* atol, double rtol, work_t* w, int64_t* stats, double* ck_y, double* ck_h,
+                           int max_ck, int* n_ck)
+{
+  const int S = m->S, ns = p->stages;
+  double* Y = w->Y;
+  const double h_min = p->h_min == 0.0 ? 1.0e-15 * dt : p->h_min;
+  const double h_max = p->h_max == 0.0 ? dt : dmin(dt, p->h_max);
+  const double h_start = p->h_start == 0.0 ? 1.0e-6 * dt : dmin(h_max, p->h_start);
+  double H = dmin(dmax(h_min, fabs(h_start)), fabs(h_max));
+  double t = 0.0;
+  int reject_last = 0, reject_more = 0, state = MICMB_SOLVER_RUNNING;
+  int64_t fc = 0, ju = 0, nst = 0, acc = 0, rej = 0, dec = 0, sol = 0;
+  if (n_ck)
+    *n_ck = 0;
+  while ((t - dt + p->round_off) <= 0 && state == MICMB_SOLVER_RUNNING)
+  {
+    if (nst > p->max_number_of_steps)
+    {
+      state = MICMB_SOLVER_CONVERGENCE_EXCEEDED_MAX_STEPS;
+      break;
+    }
+    if (((t + 0.1 * H) == t) || (H <= p->round_off))
+    {
+      state = MICMB_SOLVER_STEP_SIZE_TOO_SMALL;
+      break;
+    }
+    H = dmin(H, fabs(dt - t));
+    forcing(m, k, Y, w->F0);
+    fc++;
+    neg_jacobian(m, k, Y, w->J);
+    ju++;
+    int accepted = 0;
+    while (!accepted)
+    {
+      double alpha = 1.0 / (H * p->gamma[0]);
+      for (int i = 0; i < S; ++i)
+        w->J[m->pos[(size_t)i * S + i]] += alpha;
+      decompose(m, w->J);
+      dec++;
+      for (int s = 0; s < ns; ++s)
+      {
+        const int sc = s * (s - 1) / 2;
+        double* Ks = w->K + (size_t)s * S;
+        if (s == 0)
+          memcpy(Ks, w->F0, sizeof(double) * S);
+        else if (p->new_function_evaluation[s])
+        {
+          memcpy(w->Ynew, Y, sizeof(double) * S);
+          for (int j = 0; j < s; ++j)
+            for (int i = 0; i < S; ++i)
+              w->Ynew[i] += p->a[sc + j] * w->K[(size_t)j * S + i];
+          forcing(m, k, w->Ynew, Ks);
+          fc++;
+        }
+        if (s + 1 < ns && !p->new_function_evaluation[s + 1])
+          memcpy(w->K + (size_t)(s + 1) * S, Ks, sizeof(double) * S);
+        for (int j = 0; j < s; ++j)
+        {
+          double coh = p->c[sc + j] / H;
+          for (int i = 0; i < S; ++i)
+            Ks[i] += coh * w->K[(size_t)j * S + i];
+        }
+        lu_solve(m, w->J, Ks);
+        sol++;
+      }
+      memcpy(w->Ynew, Y, sizeof(double) * S);
+      for (int s = 0; s < ns; ++s)
+        for (int i = 0; i < S; ++i)
+          w->Ynew[i] += p->m[s] * w->K[(size_t)s * S + i];
+      for (int i = 0; i < S; ++i)
+        w->Yerr[i] = 0.0;
+      for (int s = 0; s < ns; ++s)
+        for (int i = 0; i < S; ++i)
+          w->Yerr[i] += p->e[s] * w->K[(size_t)s * S + i];
+      double sum = 0.0;
+      for (int i = 0; i < S; ++i)
+      {
+        double ay = fabs(Y[i]), an = fabs(w->Ynew[i]);
+        double ymax = ay > an ? ay : an;
+        double q = w->Yerr[i] / (atol[i] + rtol * ymax);
+        sum += q * q;
+      }
+      double error = dmax(sqrt(sum / (double)(S > 0 ? S : 1)), 1.0e-10);
+      double fac = dmin(p->factor_max,
+                        dmax(p->factor_min, p->safety_factor / pow(error, 1 / p->estimator_of_local_order)));
+      double Hnew = H * fac;
+      nst++;
+      if (isnan(error))
+      {
+        state = MICMB_SOLVER_NAN_DETECTED;
+        break;
+      }
+      if (isinf(error))
+      {
+        state = MICMB_SOLVER_INF_DETECTED;
+        break;
+      }
+      if ((error < 1) || (H < h_min))
+      {
+        acc++;
+        if (ck_y && n_ck)
+        {
+          if (*n_ck >= max_ck)
+          {
+            state = MICMB_SOLVER_CONVERGENCE_EXCEEDED_MAX_STEPS;
+            break;
+          }
+          memcpy(ck_y + (size_t)(*n_ck) * S, Y, sizeof(double) * S);
+          ck_h[*n_ck] = H;
+          (*n_ck)++;
+        }
+        t = t + H;
+        memcpy(Y, w->Ynew, sizeof(double) * S);
+        Hnew = dmax(h_min, dmin(Hnew, h_max));
+        if (reject_last)
+          Hnew = dmin(Hnew, H);
+        reject_last = 0;
+        reject_more = 0;
+        H = Hnew;
+        accepted = 1;
+      }
+      else
+      {
+        if (reject_more)
+          Hnew = H * p->rejection_factor_decrease;
+        reject_more = reject_last;
+        reject_last = 1;
+        H = Hnew;
+        if (acc >= 1)
+          rej++;
+        neg_jacobian(m, k, Y, w->J);
+        ju++;
+      }
+    }
+  }
+  if (state == MICMB_SOLVER_RUNNING)
+    state = MICMB_SOLVER_CONVERGED;
+  if (stats)
+  {
+    stats[0] = fc;
+    stats[1] = ju;
+    stats[2] = nst;
+    stats[3] = acc;
+    stats[4] = rej;
+    stats[5] = dec;
+    stats[6] = sol;
+    stats[7] = state;
+    memcpy(&stats[8], &t, sizeof(double));
+    stats[9] = 0;
+  }
+  return state;
+}
+
+/* ---------------------------------------------------------------- */
+/* adjoint building blocks: f = sum_r nu_r w_r(y), w_r = k_r prod y  */
+/* ---------------------------------------------------------------- */
+static double nu_dot(const om_mech* m, int r, const double* v)
+{
+  double s = 0.0;
+  for (int i = m->ps[r]; i < m->ps[r + 1]; ++i)
+    s += m->py[i] * v[m->pid[i]];
+  for (int i = m->rs[r]; i < m->rs[r + 1]; ++i)
+    s -= v[m->rid[i]];
+  return s;
+}
+
+/* product of reactant concentrations skipping occurrences a and b (-1 = none) */
+static double prod_except(const om_mech* m, int r, const double* y, int a, int b)
+{
+  double v = 1.0;
+  for (int i = m->rs[r]; i < m->rs[r + 1]; ++i)
+    if (i != a && i != b)
+      v *= y[m->rid[i]];
+  return v;
+}
+
+/* ybar += J(y)^T g ; kbar[r] += (nu_r . g) w_r(y) */
+static void vjp_f(const om_mech* m, const double* k, const double* y, const double* g, double* ybar, double* kbar)
+{
+  for (int r = 0; r < m->R; ++r)
+  {
+    double c = nu_dot(m, r, g);
+    if (c == 0.0)
+      continue;
+    kbar[r] += c * k[r] * prod_except(m, r, y, -1, -1);
+    for (int i = m->rs[r]; i < m->rs[r + 1]; ++i)
+      ybar[m->rid[i]] += c * k[r] * prod_except(m, r, y, i, -1);
+  }
+}
+
+/* second-order term of the Jacobian: for rho = nu_r . Rbar and direction K,
+ * ybar += rho * H_r K ; kbar[r] += rho * (grad w_r . K) */
+static void jacobian_term(const om_mech* m, const double* k, const double* y, const double* Rbar, const double* K,
+                          double* ybar, double* kbar)
+{
+  for (int r = 0; r < m->R; ++r)
+  {
+    double rho = nu_dot(m, r, Rbar);
+    if (rho == 0.0)
+      continue;
+    double gk = 0.0;
+    for (int i = m->rs[r]; i < m->rs[r + 1]; ++i)
+      gk += k[r] * prod_except(m, r, y, i, -1) * K[m->rid[i]];
+    kbar[r] += rho * gk;
+    for (int i = m->rs[r]; i < m->rs[r + 1]; ++i)
+      for (int j = m->rs[r]; j < m->rs[r + 1]; ++j)
+        if (i != j)
+          ybar[m->rid[j]] += rho * k[r] * prod_except(m, r, y, i, j) * K[m->rid[i]];
+  }
+}
+
+static void adjoint_cell(const om_mech* m, const micmb_rosenbrock_params* p, const double* k, const double* ck_y,
+                         const double* ck_h, int n_ck, double* ybar, double* kbar, work_t* w)
+{
+  const int S = m->S, ns = p->stages;
+  double* Ys = w->scratch;                      /* [ns][S] stage inputs */
+  double* Kb = Ys + (size_t)ns * S;             /* [ns][S] */
+  double* Gb = Kb + (size_t)ns * S;             /* [ns][S] */
+  double* Rb = Gb + (size_t)ns * S;             /* [ns][S] */
+  double* yb = Rb + (size_t)ns * S;             /* [S] */
+  double* tmp = yb + S;                         /* [S] */
+  for (int n = n_ck - 1; n >= 0; --n)
+  {
+    const double* y = ck_y + (size_t)n * S;
+    const double H = ck_h[n];
+    /* recompute the accepted step */
+    forcing(m, k, y, w->F0);
+    neg_jacobian(m, k, y, w->J);
+    const double alpha = 1.0 / (H * p->gamma[0]);
+    for (int i = 0; i < S; ++i)
+      w->J[m->pos[(size_t)i * S + i]] += alpha;
+    decompose(m, w->J);
+    for (int s = 0; s < ns; ++s)
+    {
+      const int sc = s * (s - 1) / 2;
+      double* Ks = w->K + (size_t)s * S;
+      memcpy(Ys + (size_t)s * S, y, sizeof(double) * S);
+      if (s == 0)
+        memcpy(Ks, w->F0, sizeof(double) * S);
+      else if (p->new_function_evaluation[s])
+      {
+        for (int j = 0; j < s; ++j)
+          for (int i = 0; i < S; ++i)
+            Ys[(size_t)s * S + i] += p->a[sc + j] * w->K[(size_t)j * S + i];
+        forcing(m, k, Ys + (size_t)s * S, Ks);
+      }
+      if (s + 1 < ns && !p->new_function_evaluation[s + 1])
+        memcpy(w->K + (size_t)(s + 1) * S, Ks, sizeof(double) * S);
+      for (int j = 0; j < s; ++j)
+      {
+        double coh = p->c[sc + j] / H;
+        for (int i = 0; i < S; ++i)
+          Ks[i] += coh * w->K[(size_t)j * S + i];
+      }
+      lu_solve(m, w->J, Ks);
+    }
+    /* reverse sweep */
+    memcpy(yb, ybar, sizeof(double) * S);
+    for (int s = 0; s < ns; ++s)
+      for (int i = 0; i < S; ++i)
+      {
+        Kb[(size_t)s * S + i] = p->m[s] * ybar[i];
+        Gb[(size_t)s * S + i] = 0.0;
+      }
+    for (int s = ns - 1; s >= 0; --s)
+    {
+      const int sc = s * (s - 1) / 2;
+      double* rb = Rb + (size_t)s * S;
+      memcpy(rb, Kb + (size_t)s * S, sizeof(double) * S);
+      lu_solve_transposed(m, w->J, rb);
+      for (int i = 0; i < S; ++i)
+        Gb[(size_t)s * S + i] += rb[i];
+      for (int j = 0; j < s; ++j)
+      {
+        double coh = p->c[sc + j] / H;
+        for (int i = 0; i < S; ++i)
+          Kb[(size_t)j * S + i] += coh * rb[i];
+      }
+      if (s == 0)
+        continue;
+      if (p->new_function_evaluation[s])
+      {
+        for (int i = 0; i < S; ++i)
+          tmp[i] = 0.0;
+        vjp_f(m, k, Ys + (size_t)s * S, Gb + (size_t)s * S, tmp, kbar);
+        for (int i = 0; i < S; ++i)
+          yb[i] += tmp[i];
+        for (int j = 0; j < s; ++j)
+          for (int i = 0; i < S; ++i)
+            Kb[(size_t)j * S + i] += p->a[sc + j] * tmp[i];
+      }
+      else
+        for (int i = 0; i < S; ++i)
+          Gb[(size_t)(s - 1) * S + i] += Gb[(size_t)s * S + i];
+    }
+    vjp_f(m, k, y, Gb, yb, kbar);
+    for (int s = 0; s < ns; ++s)
+      jacobian_term(m, k, y, Rb + (size_t)s * S, w->K + (size_t)s * S, yb, kbar);
+    memcpy(ybar, yb, sizeof(double) * S);
+  }
+}
+
+/* ---------------------------------------------------------------- */
+/* threaded drivers                                                  */
+/* ---------------------------------------------------------------- */
+typedef struct
+{
+  const om_mech* m;
+  const micmb_rosenbrock_params* p;
+  int n;
+  double dt;
+  const double *k, *atol;
+  double rtol;
+  double* y;
+  int64_t* stats;
+  const double *y0, *ybar_final;
+  double *y_final, *ybar0, *kbar;
+  int max_ck;
+  int next;
+  pthread_mutex_t lock;
+  int adjoint;
+  int failed;
+} job_t;
+
+static int take(job_t* j)
+{
+  pthread_mutex_lock(&j->lock);
+  int c = j->next++;
+  pthread_mutex_unlock(&j->lock);
+  return c;
+}
+
+static void* worker(void* arg)
+{
+  job_t* j = arg;
+  const om_mech* m = j->m;
+  const int S = m->S;
+  work_t w;
+  work_alloc(&w, m, j->p->stages);
+  double* ck_y = NULL;
+  double* ck_h = NULL;
+  if (j->adjoint)
+  {
+    ck_y = xcalloc((size_t)j->max_ck * S, sizeof(double));
+    ck_h = xcalloc(j->max_ck, sizeof(double));
+  }
+  for (;;)
+  {
+    int c = take(j);
+    if (c >= j->n)
+      break;
+    const double* k = j->k + (size_t)c * m->R;
+    if (!j->adjoint)
+    {
+      memcpy(w.Y, j->y + (size_t)c * S, sizeof(double) * S);
+      rosenbrock_cell(m, j->p, j->dt, k, j->atol, j->rtol, &w, j->stats ? j->stats + (size_t)c * 10 : NULL, NULL,
+                      NULL, 0, NULL);
+      for (int i = 0; i < S; ++i)
+        j->y[(size_t)c * S + i] = w.Y[i] < 0.0 ? 0.0 : w.Y[i];
+    }
+    else
+    {
+      int n_ck = 0;
+      memcpy(w.Y, j->y0 + (size_t)c * S, sizeof(double) * S);
+      int st = rosenbrock_cell(m, j->p, j->dt, k, j->atol, j->rtol, &w, NULL, ck_y, ck_h, j->max_ck, &n_ck);
+      if (st != MICMB_SOLVER_CONVERGED)
+        j->failed = 1;
+      double* yb = j->ybar0 + (size_t)c * S;
+      for (int i = 0; i < S; ++i)
+      {
+        double v = w.Y[i];
+        j->y_final[(size_t)c * S + i] = v < 0.0 ? 0.0 : v;
+        yb[i] = v < 0.0 ? 0.0 : j->ybar_final[(size_t)c * S + i]; /* d max(y,0)/dy */
+      }
+      double* kb = j->kbar + (size_t)c * m->R;
+      for (int r = 0; r < m->R; ++r)
+        kb[r] = 0.0;
+      adjoint_cell(m, j->p, k, ck_y, ck_h, n_ck, yb, kb, &w);
+    }
+  }
+  free(ck_y);
+  free(ck_h);
+  work_free(&w);
+  return NULL;
+}
+
+static int run(job_t* j, int n_threads)
+{
+  if (n_threads < 1)
+    n_threads = 1;
+  pthread_mutex_init(&j->lock, NULL);
+  pthread_t* th = xcalloc(n_threads, sizeof(pthread_t));
+  for (int t = 1; t < n_threads; ++t)
+    pthread_create(&th[t], NULL, worker, j);
+  worker(j);
+  for (int t = 1; t < n_threads; ++t)
+    pthread_join(th[t], NULL);
+  free(th);
+  pthread_mutex_destroy(&j->lock);
+  return j->failed ? -1 : 0;
+}
+
+int om_solve_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n, double dt, const double* k,
+                      const double* atol, double rtol, double* y, int64_t* stats_out, int n_threads)
+{
+  job_t j;
+  memset(&j, 0, sizeof j);
+  j.m = m;
+  j.p = p;
+  j.n = n;
+  j.dt = dt;
+  j.k = k;
+  j.atol = atol;
+  j.rtol = rtol;
+  j.y = y;
+  j.stats = stats_out;
+  return run(&j, n_threads);
+}
+
+int om_adjoint_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n, double dt, const double* k,
+                        const double* atol, double rtol, const double* y0, const double* ybar_final,
+                        double* y_final, double* ybar0, double* kbar, int max_steps_stored, int n_threads)
+{
+  job_t j;
+  memset(&j, 0, sizeof j);
+  j.m = m;
+  j.p = p;
+  j.n = n;
+  j.dt = dt;
+  j.k = k;
+  j.atol = atol;
+  j.rtol = rtol;
+  j.y0 = y0;
+  j.ybar_final = ybar_final;
+  j.y_final = y_final;
+  j.ybar0 = ybar0;
+  j.kbar = kbar;
+  j.max_ck = max_steps_stored;
+  j.adjoint = 1;
+  int rc = run(&j, n_threads);
+  if (rc)
+    snprintf(g_err, sizeof g_err, "a cell did not converge (or exceeded the checkpoint capacity)");
+  return rc;
+}

@@ -1,0 +1,63 @@
+/*
+ * oracle.h -- TEST INFRASTRUCTURE ONLY (never linked by the product).
+ *
+ * A plain-C restatement of micm's Rosenbrock path (NCAR/micm 3.13.0) for
+ * checking the B200 kernels, plus the FP64 discrete adjoint micm does not
+ * have.  Everything is restated from the reference's algorithm, with the
+ * scatter loops in micm's own order:
+ *   reaction sort           include/micm/solver/solver_builder.inl:274-329
+ *   Markowitz reordering    include/micm/solver/linear_solver.inl:30-124
+ *   Jacobian sparsity       include/micm/process/process_set.hpp:425-457, util/jacobian.hpp:15-32
+ *   LU fill / Decompose     include/micm/solver/lu_decomposition_mozart_in_place.inl:121-210
+ *   forcing / -J            include/micm/process/process_set.hpp:256-422, 524-670
+ *   linear solve            include/micm/solver/linear_solver_in_place.inl:113-167
+ *   rate constants          include/micm/process/rate_constant/rate_constant_functions.hpp:52-136
+ *   Rosenbrock + control    include/micm/solver/rosenbrock.inl:12-402
+ * Arrays are row-major [cell][column] in state columns.
+ */
+#ifndef MICMB_ORACLE_H
+#define MICMB_ORACLE_H
+
+#include "../include/micmb.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct om_mech om_mech;
+
+om_mech* om_create(const micmb_mechanism_desc* desc);
+void om_destroy(om_mech* m);
+const char* om_last_error(void);
+int om_n_params(const om_mech* m);
+int om_nnz(const om_mech* m);
+void om_species_columns(const om_mech* m, int32_t* out);
+void om_reaction_columns(const om_mech* m, int32_t* out);
+void om_jacobian_pattern(const om_mech* m, int32_t* rows, int32_t* cols);
+
+/* rate constants of n cells: params [cell][P], k_out [cell][R] */
+void om_rate_constants(const om_mech* m, int n, const double* T, const double* P, const double* rho,
+                       const double* params, double* k_out);
+
+/* Per-cell Rosenbrock over n cells (one independent solve per cell, n_threads
+ * host threads).  y [cell][S] in/out (clamped at zero on exit); stats_out
+ * [cell][10] = function_calls, jacobian_updates, number_of_steps, accepted,
+ * rejected, decompositions, solves, state, (final time bits), 0. */
+int om_solve_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n, double dt, const double* k,
+                      const double* atol, double rtol, double* y, int64_t* stats_out, int n_threads);
+
+/* Discrete adjoint of the accepted steps (step sizes frozen) of a per-cell
+ * solve.  Runs the forward solve from y0, then sweeps back.
+ *   ybar_final [cell][S]: dL/d(final clamped y)
+ *   y_final    [cell][S]: out, final clamped y
+ *   ybar0      [cell][S]: out, dL/dy0
+ *   kbar       [cell][R]: out, dL/d log k_r (rate columns) */
+int om_adjoint_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n, double dt, const double* k,
+                        const double* atol, double rtol, const double* y0, const double* ybar_final,
+                        double* y_final, double* ybar0, double* kbar, int max_steps_stored, int n_threads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
