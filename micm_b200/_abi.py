@@ -80,7 +80,7 @@ class MechanismInfo(C.Structure):
 
 class FusedConfig(C.Structure):
     _fields_ = [("cells_per_cta", C.c_int32), ("lu_in_shared", C.c_int32),
-                ("ctas_per_sm", C.c_int32)]
+                ("ctas_per_sm", C.c_int32), ("ring_slots", C.c_int32), ("variant", C.c_int32)]
 
 
 def ptr(a: np.ndarray, ctype):

@@ -206,6 +206,15 @@ namespace micmb
         wfo = AddWarp(pk, m.w_forcing);
         wj = AddWarp(pk, m.w_jacobian);
       }
+      if (m.has_warp_tables && !m.stream.block_bytes.empty())
+      {
+        s.stream_blocks = DeviceMemory(m.stream.bytes.size());
+        MICMB_CUDA(cudaMemcpy(s.stream_blocks.p, m.stream.bytes.data(), m.stream.bytes.size(),
+                              cudaMemcpyHostToDevice));
+        s.stream_block_bytes = DeviceMemory(m.stream.block_bytes.size() * sizeof(int32_t));
+        MICMB_CUDA(cudaMemcpy(s.stream_block_bytes.p, m.stream.block_bytes.data(),
+                              m.stream.block_bytes.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+      }
       s.tables = DeviceMemory(pk.bytes.size());
       MICMB_CUDA(cudaMemcpy(s.tables.p, pk.bytes.data(), pk.bytes.size(), cudaMemcpyHostToDevice));
       std::vector<double> ones(std::max<int32_t>(m.R, 1), 1.0);
@@ -640,6 +649,8 @@ extern "C"
     return Guard([&] {
       Need(solver && config, "null argument");
       Need(config->cells_per_cta >= 0 && config->cells_per_cta <= 8, "cells_per_cta must be 0..8");
+      Need(config->ring_slots >= 0 && config->ring_slots <= 8, "ring_slots must be 0..8");
+      Need(config->variant == 0 || config->variant == 1, "variant must be 0 (streamed) or 1 (direct)");
       solver->fused = *config;
     });
   }

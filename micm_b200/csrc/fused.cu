@@ -330,9 +330,15 @@ namespace micmb
     MICMB_CUDA(cudaMemsetAsync(cbase, 0, 128, st.stream));
     if (n > 0)
     {
-      const StepBounds B = step_bounds(s.params, dt);
-      kernel<<<(unsigned)grid, threads, smem, st.stream>>>(s.dev, s.params, B, A, W);
-      MICMB_CUDA(cudaGetLastError());
+      bool done = false;
+      if (s.fused.variant == 0)
+        done = SolveFusedStream(s, st, dt, A);
+      if (!done)
+      {
+        const StepBounds B = step_bounds(s.params, dt);
+        kernel<<<(unsigned)grid, threads, smem, st.stream>>>(s.dev, s.params, B, A, W);
+        MICMB_CUDA(cudaGetLastError());
+      }
     }
     if (stats || per_cell_status || per_cell_accepted)
     {
@@ -345,6 +351,10 @@ namespace micmb
         MICMB_CUDA(cudaMemcpyAsync(per_cell_accepted, A.cell_accepted, sizeof(int32_t) * n, cudaMemcpyDeviceToHost,
                                    st.stream));
       MICMB_CUDA(cudaStreamSynchronize(st.stream));
+      int32_t err_flag = 0;
+      MICMB_CUDA(cudaMemcpy(&err_flag, cbase + 16, sizeof(int32_t), cudaMemcpyDeviceToHost));
+      if (err_flag)
+        throw Error(MICMB_ERR_TIMEOUT, "fused kernel: a pipeline wait timed out");
       if (stats)
       {
         stats->function_calls = (int64_t)hs[0];

@@ -2,6 +2,7 @@
 #include "mechanism.hpp"
 
 #include <algorithm>
+#include <cstring>
 #include <cmath>
 #include <numeric>
 #include <set>
@@ -142,6 +143,96 @@ namespace micmb
       for (size_t t = 0; t < s.term_b.size(); ++t)
         coef_out[t] = cf[s.term_b[t]];
       return s;
+    }
+
+    inline int32_t Pad16(int32_t b)
+    {
+      return (b + 15) & ~15;
+    }
+
+    // Re-cut one warp table into stream blocks (see StreamProgram).
+    void AppendStreamPhase(StreamProgram& P, const WarpTable& w, StreamPhase& ph)
+    {
+      const bool has_coef = !w.coef.empty();
+      const int32_t B = kStreamBlockBytes;
+      int32_t n_blocks = (int32_t)P.block_bytes.size();
+      ph.first_block = n_blocks;
+      int32_t used = 16;  // header
+      int32_t n_segs = 0;
+      auto block_ptr = [&]() { return P.bytes.data() + (size_t)n_blocks * B; };
+      auto open_block = [&]() {
+        P.bytes.resize((size_t)(n_blocks + 1) * B, 0);
+        used = 16;
+        n_segs = 0;
+      };
+      auto close_block = [&]() {
+        std::memcpy(block_ptr(), &n_segs, sizeof(int32_t));
+        P.block_bytes.push_back(used);
+        ++n_blocks;
+      };
+      open_block();
+      for (int32_t l = 0; l < w.n_levels; ++l)
+      {
+        for (int32_t ch = w.level_chunk_start[l]; ch < w.level_chunk_start[l + 1]; ++ch)
+        {
+          const int32_t base = w.chunk[4 * ch + 0], T = w.chunk[4 * ch + 1], first = w.chunk[4 * ch + 2],
+                        n = w.chunk[4 * ch + 3];
+          const bool last_in_level = (ch + 1 == w.level_chunk_start[l + 1]);
+          const int32_t fixed = 16 + Pad16(4 * n);
+          int32_t t0 = 0;
+          bool first_seg = true;
+          for (;;)
+          {
+            const int32_t avail = B - used;
+            int32_t tseg = 0;
+            // largest tseg with fixed + Pad16(4 n tseg) + coef bytes <= avail
+            const int32_t per_t = 4 * n + (has_coef ? 8 * n : 0);
+            if (avail >= fixed + 32)
+              tseg = std::min(T - t0, (avail - fixed - 32) / per_t);  // 32: padding of both arrays
+            tseg = std::max(tseg, 0);
+            const bool fits = avail >= fixed && (tseg > 0 || T == t0);
+            if (!fits)
+            {
+              if (n_segs == 0)
+                throw std::runtime_error("stream block too small for one table segment");
+              close_block();
+              open_block();
+              continue;
+            }
+            const int32_t term_bytes = Pad16(4 * n * tseg);
+            const int32_t seg_bytes = Pad16(fixed + term_bytes + (has_coef ? 8 * n * tseg : 0));
+            uint8_t* seg = block_ptr() + used;
+            int32_t flags = first_seg ? kSegFirst : 0;
+            const bool last_seg = (t0 + tseg == T);
+            if (last_seg)
+              flags |= kSegLast;
+            if (last_seg && last_in_level)
+              flags |= kSegLevelEnd;
+            const int32_t desc[4] = { tseg, n | (flags << 8), seg_bytes, 0 };
+            std::memcpy(seg, desc, 16);
+            std::memcpy(seg + 16, w.item.data() + first, 4 * (size_t)n);
+            uint32_t* terms = reinterpret_cast<uint32_t*>(seg + fixed);
+            for (int32_t t = 0; t < tseg; ++t)
+              for (int32_t lane = 0; lane < n; ++lane)
+                terms[t * n + lane] = w.term[(size_t)base + (size_t)(t0 + t) * 32 + lane];
+            if (has_coef)
+            {
+              double* cf = reinterpret_cast<double*>(seg + fixed + term_bytes);
+              for (int32_t t = 0; t < tseg; ++t)
+                for (int32_t lane = 0; lane < n; ++lane)
+                  cf[t * n + lane] = w.coef[(size_t)base + (size_t)(t0 + t) * 32 + lane];
+            }
+            used += seg_bytes;
+            ++n_segs;
+            t0 += tseg;
+            first_seg = false;
+            if (last_seg)
+              break;
+          }
+        }
+      }
+      close_block();
+      ph.n_blocks = n_blocks - ph.first_block;
     }
 
     uint64_t Fnv(uint64_t h, const void* data, size_t bytes)
@@ -640,6 +731,13 @@ namespace micmb
           },
           [&](int32_t t) { return (uint32_t)js.term_a[t]; }, (uint32_t)m.scratch_zero, &jco);
       m.has_warp_tables = true;
+      AppendStreamPhase(m.stream, m.w_forcing, m.stream.forcing);
+      AppendStreamPhase(m.stream, m.w_jacobian, m.stream.jacobian);
+      AppendStreamPhase(m.stream, m.w_lu, m.stream.lu);
+      AppendStreamPhase(m.stream, m.w_fwd, m.stream.fwd);
+      AppendStreamPhase(m.stream, m.w_bwd, m.stream.bwd);
+      AppendStreamPhase(m.stream, m.w_fwd_t, m.stream.fwd_t);
+      AppendStreamPhase(m.stream, m.w_bwd_t, m.stream.bwd_t);
     }
 
     // 11. hash of everything the device sees

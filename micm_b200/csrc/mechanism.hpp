@@ -60,6 +60,32 @@ namespace micmb
     std::vector<double> coef;                // per-term coefficient (gathers with weights)
   };
 
+  // The warp tables re-cut into fixed-size blocks for bulk (TMA) streaming
+  // into a shared-memory ring.  A block holds a 16-byte header (segment count)
+  // followed by segments laid end to end:
+  //   int4 {T, n | flags << 8, segment bytes, 0}
+  //   uint32 items[n]            (padded to 16 bytes)
+  //   uint32 terms[T][n]         (lane l's term t at t*n + l, padded to 16 bytes)
+  //   double coef[T][n]          (weighted gathers only)
+  // A chunk whose terms do not fit in the rest of a block continues in the
+  // next block (FIRST/LAST flags); LEVEL_END marks the end of a dependency
+  // level (the warp synchronises there).
+  constexpr int32_t kStreamBlockBytes = 8192;
+  constexpr int32_t kSegFirst = 1, kSegLast = 2, kSegLevelEnd = 4;
+
+  struct StreamPhase
+  {
+    int32_t first_block = 0;
+    int32_t n_blocks = 0;
+  };
+
+  struct StreamProgram
+  {
+    std::vector<uint8_t> bytes;          // all blocks, each kStreamBlockBytes apart
+    std::vector<int32_t> block_bytes;    // used bytes per block (multiple of 16)
+    StreamPhase forcing, jacobian, lu, fwd, bwd, fwd_t, bwd_t;
+  };
+
   struct RateDef
   {
     int32_t kind = 0;
@@ -115,6 +141,7 @@ namespace micmb
     bool has_warp_tables = false;
     int32_t scratch_zero = 0;
     WarpTable w_lu, w_fwd, w_bwd, w_fwd_t, w_bwd_t, w_forcing, w_jacobian;
+    StreamProgram stream;
 
     int32_t lu_updates = 0;
     int32_t lu_lower = 0;

@@ -94,7 +94,9 @@ struct micmb_solver
   const int32_t* diag_row_of = nullptr;  // [nnz]: row if diagonal, else -1
   micmb_rosenbrock_params host_params{};
   micmb::DevParams params{};
-  micmb_fused_config fused{ 0, 1, 0 };
+  micmb_fused_config fused{ 0, 1, 0, 0, 0 };
+  micmb::DeviceMemory stream_blocks;       // StreamProgram bytes
+  micmb::DeviceMemory stream_block_bytes;  // [n_blocks]
 };
 
 struct micmb_state
@@ -117,6 +119,8 @@ struct micmb_state
   // fused path
   micmb::DeviceMemory lu_slots;
   int64_t lu_slot_count = 0;
+  micmb::DeviceMemory attempt_order;  // streamed kernel: block order of one attempt
+  double dt_for_launch = 0.0;
 
   size_t dense_bytes(int32_t ncols) const
   {
@@ -141,5 +145,8 @@ namespace micmb
   void LaunchLinearSolve(micmb_solver& s, micmb_state& st);
   void NormalizedError(micmb_solver& s, micmb_state& st, double* global_out, double* per_cell_out);
   size_t FusedSharedBytes(const micmb_solver& s, bool lu_in_shared);
+  // streamed warp-specialised variant; returns false when it does not apply
+  bool SolveFusedStream(micmb_solver& s, micmb_state& st, double dt, const FusedArgs& A);
+  int StreamWarpsPerCta(const micmb_solver& s, int slots, int cap);
   int FusedWarpsPerCta(const micmb_solver& s, const micmb_fused_config& cfg);
 }  // namespace micmb

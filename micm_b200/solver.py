@@ -151,15 +151,16 @@ class Solver:
         assert scale.shape == (self.mech.n_reactions,)
         check(lib().micmb_solver_set_rate_scale(self.handle, _f64(scale)))
 
-    def set_fused_config(self, cells_per_cta=0, lu_in_shared=1, ctas_per_sm=0):
-        cfg = FusedConfig(int(cells_per_cta), int(lu_in_shared), int(ctas_per_sm))
+    def set_fused_config(self, cells_per_cta=0, lu_in_shared=1, ctas_per_sm=0, ring_slots=0, variant=0):
+        """variant 0: TMA-streamed warp-specialised kernel; 1: direct kernel."""
+        cfg = FusedConfig(int(cells_per_cta), int(lu_in_shared), int(ctas_per_sm), int(ring_slots), int(variant))
         check(lib().micmb_solver_set_fused_config(self.handle, C.byref(cfg)))
 
     def get_fused_config(self) -> Dict[str, int]:
         cfg = FusedConfig()
         check(lib().micmb_solver_get_fused_config(self.handle, C.byref(cfg)))
         return dict(cells_per_cta=cfg.cells_per_cta, lu_in_shared=cfg.lu_in_shared,
-                    ctas_per_sm=cfg.ctas_per_sm)
+                    ctas_per_sm=cfg.ctas_per_sm, ring_slots=cfg.ring_slots, variant=cfg.variant)
 
     def get_state(self, n_cells: int = 1, vector_length: Optional[int] = None) -> "State":
         return State(self, n_cells, vector_length or self.vector_length)

@@ -1,0 +1,50 @@
+"""micm's CUDA-path C++ API (include/micm_b200/micm.hpp) over the C ABI."""
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_DIR = os.path.join(ROOT, "micm_b200")
+
+README_TABLE = [
+    "0,   1.18e+01,   5.90e+00,   1.91e+00", "500,   6.79e+00,   9.05e+00,   3.32e+00",
+    "1000,   3.83e+00,   1.07e+01,   4.21e+00", "1500,   2.14e+00,   1.17e+01,   4.74e+00",
+    "2000,   1.19e+00,   1.22e+01,   5.04e+00", "2500,   6.58e-01,   1.24e+01,   5.21e+00",
+    "3000,   3.64e-01,   1.26e+01,   5.31e+00", "3500,   2.01e-01,   1.27e+01,   5.36e+00",
+    "4000,   1.11e-01,   1.27e+01,   5.39e+00", "4500,   6.13e-02,   1.28e+01,   5.41e+00",
+]
+
+
+@pytest.fixture(scope="module")
+def readme_binary(tmp_path_factory):
+    out = str(tmp_path_factory.mktemp("cpp") / "readme_example")
+    subprocess.run(["g++", "-std=c++20", "-O2", "-I" + os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "readme_example.cpp"), "-o", out, "-L" + LIB_DIR,
+                    "-lmicmb", "-Wl,-rpath," + LIB_DIR], check=True)
+    return out
+
+
+def _has_gpu():
+    import torch
+    return torch.cuda.is_available()
+
+
+def test_cpp_api_compiles_and_reports_missing_device(readme_binary):
+    if _has_gpu():
+        pytest.skip("a GPU is present; covered by the gpu test")
+    r = subprocess.run([readme_binary], capture_output=True, text=True)
+    assert r.returncode == 3 and "no CUDA device" in r.stderr
+
+
+def _rows(stdout):
+    return [re.sub(r"\s+", " ", l.strip()) for l in stdout.strip().splitlines()[1:]]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method", ["plain", "fused"])
+def test_cpp_readme_example_on_gpu(cuda_device, readme_binary, method):
+    r = subprocess.run([readme_binary, method], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert _rows(r.stdout) == [re.sub(r"\s+", " ", l) for l in README_TABLE]

@@ -104,5 +104,30 @@ def test_fused_lu_in_global_memory(cuda_device):
     inp = synthetic.cell_inputs(m, 150, seed=32)
     y_s, _ = solve_gpu(m, inp, 600.0, 4, "fused", "per_cell", L=32)
     y_g, _ = solve_gpu(m, inp, 600.0, 4, "fused", "per_cell", L=32,
-                       fused_config=dict(cells_per_cta=4, lu_in_shared=0))
+                       fused_config=dict(cells_per_cta=4, lu_in_shared=0, variant=1))
     np.testing.assert_array_equal(y_s, y_g)
+
+
+@pytest.mark.parametrize("config", [dict(variant=1), dict(variant=0, ring_slots=2), dict(variant=0, ring_slots=6),
+                                    dict(variant=0, cells_per_cta=1), dict(variant=0, ctas_per_sm=2)])
+def test_fused_variants_bitwise(cuda_device, config):
+    """Every fused configuration computes exactly what the plain kernels compute."""
+    m = synthetic.synthetic_mechanism(210, 440, seed=2101)
+    inp = synthetic.cell_inputs(m, 333, seed=33, t_range=(200.0, 310.0), night_fraction=0.5)
+    y_p, r_p = solve_gpu(m, inp, 600.0, 4, "plain", "per_cell", L=32)
+    y_f, r_f = solve_gpu(m, inp, 600.0, 4, "fused", "per_cell", L=32, fused_config=config)
+    np.testing.assert_array_equal(y_f, y_p)
+    np.testing.assert_array_equal(r_f[0].per_cell_accepted, r_p[0].per_cell_accepted)
+    assert r_f[0].stats["number_of_steps"] == r_p[0].stats["number_of_steps"]
+
+
+def test_fused_tiny_and_ragged(cuda_device):
+    """Fewer cells than warps, and a cell count that is no multiple of anything."""
+    m = synthetic.synthetic_mechanism(60, 120, seed=601)
+    for n in (1, 3, 37):
+        inp = synthetic.cell_inputs(m, n, seed=40 + n)
+        ref = oracle.Reference(m, tableau=4)
+        y_ref, st_ref = ref.solve_per_cell(inp, 3600.0)
+        y, res = solve_gpu(m, inp, 3600.0, 4, "fused", "per_cell", L=8)
+        _close(y, y_ref)
+        np.testing.assert_array_equal(res[0].per_cell_accepted, st_ref[:, 3])
