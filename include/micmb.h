@@ -197,6 +197,12 @@ int micmb_mechanism_custom_param_columns(const micmb_mechanism* mech, int32_t* o
 int micmb_mechanism_jacobian_pattern(const micmb_mechanism* mech, int32_t* rows, int32_t* cols);
 /* the unfilled Jacobian sparsity (ProcessSet::NonZeroJacobianElements + diagonal) */
 int micmb_mechanism_jacobian_pattern_unfilled(const micmb_mechanism* mech, int32_t* rows, int32_t* cols);
+/* Shape of the fused kernel's streamed schedule, per phase (forcing, -J,
+ * LU, forward, backward, forward-transposed, backward-transposed):
+ * out[p*4 + 0] blocks, [1] segments, [2] lane steps (sum of segment lengths),
+ * [3] terms (nonzero work).  Returns MICMB_ERR_UNSUPPORTED when the
+ * mechanism has no streamed schedule. */
+int micmb_mechanism_stream_stats(const micmb_mechanism* mech, int64_t* out /*[28]*/);
 /* 64-bit FNV-1a hash of the compiled tables (autotuner cache key) */
 uint64_t micmb_mechanism_hash(const micmb_mechanism* mech);
 

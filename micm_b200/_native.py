@@ -42,6 +42,7 @@ def lib():
             "micmb_mechanism_jacobian_pattern": [vp, i32p, i32p],
             "micmb_mechanism_jacobian_pattern_unfilled": [vp, i32p, i32p],
             "micmb_rosenbrock_params_default": [C.c_int32, C.POINTER(RosenbrockParams)],
+            "micmb_mechanism_stream_stats": [vp, C.POINTER(C.c_int64)],
             "micmb_solver_create": [vp, C.POINTER(RosenbrockParams), C.POINTER(vp)],
             "micmb_solver_set_params": [vp, C.POINTER(RosenbrockParams)],
             "micmb_solver_set_rate_scale": [vp, f64p],

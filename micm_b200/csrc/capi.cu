@@ -417,6 +417,43 @@ extern "C"
     });
   }
 
+  int micmb_mechanism_stream_stats(const micmb_mechanism* mech, int64_t* out)
+  {
+    return Guard([&] {
+      Need(mech && out, "null argument");
+      const auto& m = mech->m;
+      if (!m.has_warp_tables)
+        throw Error(MICMB_ERR_UNSUPPORTED, "no streamed schedule for this mechanism");
+      const StreamPhase* ph[7] = { &m.stream.forcing, &m.stream.jacobian, &m.stream.lu, &m.stream.fwd,
+                                   &m.stream.bwd,     &m.stream.fwd_t,    &m.stream.bwd_t };
+      const LevelSchedule* sch[7] = { nullptr, nullptr, &m.lu, &m.fwd, &m.bwd, &m.fwd_t, &m.bwd_t };
+      for (int p = 0; p < 7; ++p)
+      {
+        int64_t segs = 0, steps = 0;
+        for (int32_t b = ph[p]->first_block; b < ph[p]->first_block + ph[p]->n_blocks; ++b)
+        {
+          const uint8_t* blk = m.stream.bytes.data() + (size_t)b * kStreamBlockBytes;
+          int32_t nseg = 0;
+          std::memcpy(&nseg, blk, 4);
+          const uint8_t* q = blk + 16;
+          for (int32_t g = 0; g < nseg; ++g)
+          {
+            int32_t d[4];
+            std::memcpy(d, q, 16);
+            steps += d[0];
+            q += d[2];
+          }
+          segs += nseg;
+        }
+        out[p * 4 + 0] = ph[p]->n_blocks;
+        out[p * 4 + 1] = segs;
+        out[p * 4 + 2] = steps;
+        out[p * 4 + 3] = sch[p] ? (int64_t)sch[p]->term_a.size()
+                                : (int64_t)(p == 0 ? m.f_rxn.size() : m.j_info.size());
+      }
+    });
+  }
+
   uint64_t micmb_mechanism_hash(const micmb_mechanism* mech)
   {
     return mech ? mech->m.hash : 0;

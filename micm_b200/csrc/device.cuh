@@ -259,12 +259,12 @@ namespace micmb
         double v = A[e];
         for (int32_t t = sch.term_start[it]; t < sch.term_start[it + 1]; ++t)
           v -= A[sch.ta[t]] * A[sch.tb[t]];
-        const int32_t aux = sch.aux[it];
+        const int32_t aux = sch.aux[it];  // -2: partial sum (stored, finalised by a later unit)
         if (aux >= 0)
           v *= inv[diag_row[aux]];
         A[e] = v;
         const int32_t dr = diag_row[e];
-        if (dr >= 0)
+        if (aux != -2 && dr >= 0)
           inv[dr] = 1.0 / v;
       }
       lane_sync<NL>();
@@ -303,7 +303,8 @@ namespace micmb
         double v = x[i];
         for (int32_t t = sch.term_start[it]; t < sch.term_start[it + 1]; ++t)
           v -= A[sch.ta[t]] * x[sch.tb[t]];
-        x[i] = v / A[sch.aux[it]];
+        const int32_t aux = sch.aux[it];  // -2: partial sum
+        x[i] = aux >= 0 ? v / A[aux] : v;
       }
       lane_sync<NL>();
     }
@@ -349,7 +350,7 @@ namespace micmb
             const uint32_t q = __ldg(tp + t * 32);
             v -= A[q & 0xFFFFu] * A[q >> 16];
           }
-          if (hi == 0xFFFFu)
+          if (hi >= 0xFFFEu)  // U entry, or a partial sum
             A[e] = v;
           else if (hi & 0x8000u)
           {
@@ -396,7 +397,7 @@ namespace micmb
             const uint32_t q = __ldg(tp + t * 32);
             v -= A[q & 0xFFFFu] * x[q >> 16];
           }
-          x[i] = (hi == 0xFFFFu) ? v : v / A[hi];
+          x[i] = (hi >= 0xFFFEu) ? v : v / A[hi];
         }
       }
       __syncwarp();

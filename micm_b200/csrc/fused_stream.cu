@@ -210,7 +210,7 @@ namespace micmb
           }
           if (s.flags & kSegLast)
           {
-            if (hi == 0xFFFFu)
+            if (hi >= 0xFFFEu)  // U entry, or a partial sum
               A[e] = acc;
             else if (hi & 0x8000u)
             {
@@ -260,7 +260,7 @@ namespace micmb
             acc -= A[q & 0xFFFFu] * x[q >> 16];
           }
           if (s.flags & kSegLast)
-            x[i] = (hi == 0xFFFFu) ? acc : acc / A[hi];
+            x[i] = (hi >= 0xFFFEu) ? acc : acc / A[hi];
         }
         if (s.flags & kSegLevelEnd)
           __syncwarp();

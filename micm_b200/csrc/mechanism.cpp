@@ -23,62 +23,113 @@ namespace micmb
         throw std::runtime_error(what);
     }
 
-    // Longest-path levels for a DAG whose items are visited in a dependency-
-    // respecting order; returns the schedule with items grouped by level.
+    // One output value (LU entry, solution component, forcing, -J entry) with
+    // its ordered terms.  term_dep[t] lists the items whose final values term
+    // t reads; final_dep lists the items the finalisation reads (the pivot
+    // 1/a_kk of an L entry).
     struct RawItem
     {
       int32_t target;
       int32_t aux;
       std::vector<std::pair<int32_t, int32_t>> terms;
-      std::vector<int32_t> deps;  // item indices (in visit order) this item reads
+      std::vector<std::vector<int32_t>> term_dep;
+      std::vector<int32_t> final_dep;
     };
 
+    // "As soon as possible" level schedule that keeps every item's terms in
+    // their original order.  Term t of an item can be applied once its
+    // operands are final (and after the item's earlier terms), so an item is
+    // cut into work units, one per level in which it gains terms; each unit
+    // reloads the partial sum from memory and stores it back (an exact round
+    // trip), and only the last unit finalises (pivot scaling, reciprocal,
+    // division).  Long dot products then overlap the levels that produce
+    // their operands instead of running after all of them.  Items must be
+    // visited in a dependency-respecting order.
     LevelSchedule Schedule(const std::vector<RawItem>& items)
     {
       const int32_t n = (int32_t)items.size();
-      std::vector<int32_t> level(n, 0);
-      int32_t max_level = -1;
+      std::vector<int32_t> final_level(n, 0);
+      struct Unit
+      {
+        int32_t level, item, t0, t1;
+        bool final;
+      };
+      std::vector<Unit> units;
+      int32_t max_level = 0;
       for (int32_t i = 0; i < n; ++i)
       {
-        int32_t l = 0;
-        for (int32_t d : items[i].deps)
+        const RawItem& it = items[i];
+        const int32_t m = (int32_t)it.terms.size();
+        int32_t unit_start = 0, unit_level = -1, prefix = 0;
+        for (int32_t t = 0; t < m; ++t)
         {
-          if (d >= i)
-            throw std::runtime_error("schedule: dependency visited after its user");
-          l = std::max(l, level[d] + 1);
+          int32_t d = 0;
+          for (int32_t dep : it.term_dep[t])
+          {
+            if (dep >= i)
+              throw std::runtime_error("schedule: dependency visited after its user");
+            d = std::max(d, final_level[dep] + 1);
+          }
+          prefix = std::max(prefix, d);
+          if (t == 0)
+            unit_level = prefix;
+          else if (prefix > unit_level)
+          {
+            units.push_back({ unit_level, i, unit_start, t, false });
+            unit_start = t;
+            unit_level = prefix;
+          }
         }
-        level[i] = l;
-        max_level = std::max(max_level, l);
+        int32_t fin = 0;
+        for (int32_t dep : it.final_dep)
+        {
+          if (dep >= i)
+            throw std::runtime_error("schedule: dependency visited after its user");
+          fin = std::max(fin, final_level[dep] + 1);
+        }
+        if (m == 0)
+        {
+          units.push_back({ fin, i, 0, 0, true });
+          final_level[i] = fin;
+        }
+        else if (fin <= unit_level)
+        {
+          units.push_back({ unit_level, i, unit_start, m, true });
+          final_level[i] = unit_level;
+        }
+        else
+        {
+          units.push_back({ unit_level, i, unit_start, m, false });
+          units.push_back({ fin, i, m, m, true });
+          final_level[i] = fin;
+        }
+        max_level = std::max(max_level, final_level[i]);
       }
-      std::vector<int32_t> order(n);
-      std::iota(order.begin(), order.end(), 0);
       // by level, then longer term lists first so lanes finish together
-      std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
-        if (level[a] != level[b])
-          return level[a] < level[b];
-        return items[a].terms.size() > items[b].terms.size();
+      std::stable_sort(units.begin(), units.end(), [](const Unit& a, const Unit& b) {
+        if (a.level != b.level)
+          return a.level < b.level;
+        return (a.t1 - a.t0) > (b.t1 - b.t0);
       });
       LevelSchedule s;
-      s.level_start.assign(max_level + 2, 0);
-      for (int32_t i = 0; i < n; ++i)
-        s.level_start[level[i] + 1]++;
-      for (int32_t l = 0; l <= max_level; ++l)
+      s.level_start.assign(n ? max_level + 2 : 1, 0);
+      for (const Unit& u : units)
+        s.level_start[u.level + 1]++;
+      for (int32_t l = 0; l + 1 < (int32_t)s.level_start.size(); ++l)
         s.level_start[l + 1] += s.level_start[l];
       s.term_start.push_back(0);
-      for (int32_t idx : order)
+      for (const Unit& u : units)
       {
-        const auto& it = items[idx];
+        const RawItem& it = items[u.item];
         s.item_target.push_back(it.target);
-        s.item_aux.push_back(it.aux);
-        for (const auto& t : it.terms)
+        s.item_aux.push_back(u.final ? it.aux : -2);  // -2: partial sum, no finalisation
+        for (int32_t t = u.t0; t < u.t1; ++t)
         {
-          s.term_a.push_back(t.first);
-          s.term_b.push_back(t.second);
+          s.term_a.push_back(it.terms[t].first);
+          s.term_b.push_back(it.terms[t].second);
         }
         s.term_start.push_back((int32_t)s.term_a.size());
       }
-      if (n == 0)
-        s.level_start.assign(1, 0);
       return s;
     }
 
@@ -135,7 +186,10 @@ namespace micmb
         it.target = i;
         it.aux = -1;
         for (int32_t t = start[i]; t < start[i + 1]; ++t)
+        {
           it.terms.push_back({ idx[t], t });  // term_b carries the coefficient index
+          it.term_dep.emplace_back();
+        }
         items.push_back(std::move(it));
       }
       LevelSchedule s = Schedule(items);
@@ -597,12 +651,11 @@ namespace micmb
             if (f == m.position.end())
               continue;
             it.terms.push_back({ pos(j, i), f->second });
-            it.deps.push_back(item_of_pos.at(pos(j, i)));
-            it.deps.push_back(item_of_pos.at(f->second));
+            it.term_dep.push_back({ item_of_pos.at(pos(j, i)), item_of_pos.at(f->second) });
           }
           if (j > k)
           {
-            it.deps.push_back(item_of_pos.at(pos(k, k)));
+            it.final_dep.push_back(item_of_pos.at(pos(k, k)));
             m.lu_lower++;
           }
           m.lu_updates += (int32_t)it.terms.size();
@@ -633,7 +686,7 @@ namespace micmb
           if (j >= i)
             break;
           it.terms.push_back({ pos(i, j), j });
-          it.deps.push_back(j);
+          it.term_dep.push_back({ j });
         }
         f.push_back(std::move(it));
       }
@@ -649,7 +702,7 @@ namespace micmb
           if (j > i)
           {
             it.terms.push_back({ pos(i, j), j });
-            it.deps.push_back(S - 1 - j);
+            it.term_dep.push_back({ S - 1 - j });
           }
         b.push_back(std::move(it));
       }
@@ -664,7 +717,7 @@ namespace micmb
           if (j >= i)
             break;
           it.terms.push_back({ pos(j, i), j });
-          it.deps.push_back(j);
+          it.term_dep.push_back({ j });
         }
         ft.push_back(std::move(it));
       }
@@ -679,7 +732,7 @@ namespace micmb
           if (j > i)
           {
             it.terms.push_back({ pos(j, i), j });
-            it.deps.push_back(S - 1 - j);
+            it.term_dep.push_back({ S - 1 - j });
           }
         bt.push_back(std::move(it));
       }
@@ -698,7 +751,9 @@ namespace micmb
           [&](int32_t i) {
             const int32_t e = m.lu.item_target[i];
             const int32_t j = m.nz_row[e], k = m.nz_col[e];
-            const uint32_t hi = (j < k) ? 0xFFFFu : (j == k ? (0x8000u | (uint32_t)j) : (uint32_t)k);
+            uint32_t hi = (j < k) ? 0xFFFFu : (j == k ? (0x8000u | (uint32_t)j) : (uint32_t)k);
+            if (m.lu.item_aux[i] == -2)
+              hi = 0xFFFEu;  // partial sum
             return (uint32_t)e | (hi << 16);
           },
           [&](int32_t t) { return pack2((uint32_t)m.lu.term_a[t], (uint32_t)m.lu.term_b[t]); }, pack2(NZ, NZ),
@@ -707,7 +762,7 @@ namespace micmb
         return BuildWarp(
             s,
             [&](int32_t i) {
-              const uint32_t hi = s.item_aux[i] < 0 ? 0xFFFFu : (uint32_t)s.item_aux[i];
+              const uint32_t hi = s.item_aux[i] == -2 ? 0xFFFEu : (s.item_aux[i] < 0 ? 0xFFFFu : (uint32_t)s.item_aux[i]);
               return (uint32_t)s.item_target[i] | (hi << 16);
             },
             [&](int32_t t) { return pack2((uint32_t)s.term_a[t], (uint32_t)s.term_b[t]); }, pack2(NZ, SV), nullptr);

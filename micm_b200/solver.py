@@ -105,6 +105,14 @@ class CompiledMechanism:
                                                               _i32(self.cols_unfilled)))
         self.hash = int(lib().micmb_mechanism_hash(self.handle))
 
+    def stream_stats(self) -> Dict[str, Dict[str, int]]:
+        """Blocks, segments, lane steps and terms of each streamed phase."""
+        out = np.zeros(28, np.int64)
+        check(lib().micmb_mechanism_stream_stats(self.handle, out.ctypes.data_as(C.POINTER(C.c_int64))))
+        names = ["forcing", "jacobian", "lu", "forward", "backward", "forward_t", "backward_t"]
+        return {n: dict(blocks=int(out[4 * i]), segments=int(out[4 * i + 1]), steps=int(out[4 * i + 2]),
+                        terms=int(out[4 * i + 3])) for i, n in enumerate(names)}
+
     def __del__(self):
         h = getattr(self, "handle", None)
         if h and h.value and _native._lib is not None:
