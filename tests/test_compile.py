@@ -38,7 +38,8 @@ def test_numbering_without_reorder():
 
 
 def test_large_mechanism_numbering():
-    m = synthetic.synthetic_mechanism(600, 1500, seed=6001)
+    # a denser hub structure than the default, so the LU fill outgrows shared memory
+    m = synthetic.synthetic_mechanism(600, 1500, seed=6001, hub_fraction=0.07, window=12, hub_skew=1.0)
     cm = CompiledMechanism(m)
     ref = oracle.Reference(m, tableau=4)
     np.testing.assert_array_equal(cm.species_columns, ref.species_columns)
