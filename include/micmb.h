@@ -280,8 +280,8 @@ int micmb_solve(micmb_solver* solver, micmb_state* state, double dt, int32_t met
 
 /* Fused-kernel launch configuration (autotuner knobs). */
 typedef struct micmb_fused_config {
-  int32_t cells_per_cta;   /* consumer warps (one cell each) per CTA, 0 = as many as fit */
-  int32_t lu_in_shared;    /* direct variant: 1 LU in shared memory, 0 LU in global memory */
+  int32_t cells_per_cta;   /* consumer warps (one cell each) per CTA, 0..12, 0 = as many as fit */
+  int32_t lu_in_shared;    /* 1 LU factor in shared memory, 0 in a per-warp global (L2) slot */
   int32_t ctas_per_sm;     /* persistent grid = ctas_per_sm * SM count (0 = occupancy) */
   int32_t ring_slots;      /* streamed variant: shared-memory slots for table blocks (0 = 4) */
   int32_t variant;         /* 0 streamed (TMA-fed, warp-specialised), 1 direct */

@@ -195,6 +195,7 @@ namespace micmb
       const size_t o_dp = pk.add(m.diag_pos), o_dro = pk.add(diag_row_of);
       const SchedOffsets lu = AddSchedule(pk, m.lu), fw = AddSchedule(pk, m.fwd), bw = AddSchedule(pk, m.bwd),
                          fwt = AddSchedule(pk, m.fwd_t), bwt = AddSchedule(pk, m.bwd_t);
+      const size_t o_rd = pk.add(m.rate_desc), o_drd = pk.add(m.drate_desc);
       WarpOffsets wl{}, wf{}, wb{}, wft{}, wbt{}, wfo{}, wj{};
       if (m.has_warp_tables)
       {
@@ -214,6 +215,10 @@ namespace micmb
         s.stream_block_bytes = DeviceMemory(m.stream.block_bytes.size() * sizeof(int32_t));
         MICMB_CUDA(cudaMemcpy(s.stream_block_bytes.p, m.stream.block_bytes.data(),
                               m.stream.block_bytes.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+        s.n_stream_coef = (int32_t)m.stream.coef_table.size();
+        s.stream_coef = DeviceMemory(m.stream.coef_table.size() * sizeof(double));
+        MICMB_CUDA(cudaMemcpy(s.stream_coef.p, m.stream.coef_table.data(),
+                              m.stream.coef_table.size() * sizeof(double), cudaMemcpyHostToDevice));
       }
       s.tables = DeviceMemory(pk.bytes.size());
       MICMB_CUDA(cudaMemcpy(s.tables.p, pk.bytes.data(), pk.bytes.size(), cudaMemcpyHostToDevice));
@@ -264,6 +269,8 @@ namespace micmb
         d.w_forcing = ResolveWarp(b, wfo);
         d.w_jacobian = ResolveWarp(b, wj);
       }
+      d.rate_desc = m.rate_desc.empty() ? nullptr : reinterpret_cast<const int4*>(b + o_rd);
+      d.drate_desc = m.drate_desc.empty() ? nullptr : reinterpret_cast<const int4*>(b + o_drd);
     }
 
     template<class F>
@@ -685,7 +692,7 @@ extern "C"
   {
     return Guard([&] {
       Need(solver && config, "null argument");
-      Need(config->cells_per_cta >= 0 && config->cells_per_cta <= 8, "cells_per_cta must be 0..8");
+      Need(config->cells_per_cta >= 0 && config->cells_per_cta <= 12, "cells_per_cta must be 0..12");
       Need(config->ring_slots >= 0 && config->ring_slots <= 8, "ring_slots must be 0..8");
       Need(config->variant == 0 || config->variant == 1, "variant must be 0 (streamed) or 1 (direct)");
       solver->fused = *config;

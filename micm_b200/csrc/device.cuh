@@ -75,6 +75,9 @@ namespace micmb
     int32_t has_warp;
     int32_t scratch_zero;
     DevWarpTable w_lu, w_fwd, w_bwd, w_fwd_t, w_bwd_t, w_forcing, w_jacobian;
+    // fixed-width product lists (nullptr when a reaction has more than three reactants)
+    const int4* rate_desc;   // [R]
+    const int4* drate_desc;  // [n_info]
   };
 
   // Rosenbrock tableau in device-friendly form
@@ -197,6 +200,38 @@ namespace micmb
       for (int32_t i = M.react_start[r]; i < M.react_start[r + 1]; ++i)
         v *= y[M.react_ids[i]];
       rate[r] = v;
+    }
+  }
+
+  // reaction_rates / jacobian_rates over fixed-width product lists; y[S + 1]
+  // must hold 1.0.  Same products in the same order as the loops above.
+  template<int NL, class KV, class YV, class RV>
+  __device__ __forceinline__ void reaction_rates_narrow(const DevMech& M, KV k, YV y, RV rate, int lane)
+  {
+#pragma unroll 4
+    for (int32_t r = lane; r < M.R; r += NL)
+    {
+      const int4 d = M.rate_desc[r];
+      double v = k[r];
+      v *= y[d.x];
+      v *= y[d.y];
+      v *= y[d.z];
+      rate[r] = v;
+    }
+  }
+
+  template<int NL, class KV, class YV, class DV>
+  __device__ __forceinline__ void jacobian_rates_narrow(const DevMech& M, KV k, YV y, DV drate, int lane)
+  {
+#pragma unroll 4
+    for (int32_t i = lane; i < M.n_info; i += NL)
+    {
+      const int4 d = M.drate_desc[i];
+      double v = k[d.x];
+      v *= y[d.y];
+      v *= y[d.z];
+      v *= y[d.w];
+      drate[i] = v;
     }
   }
 

@@ -319,10 +319,10 @@ namespace micmb
     {
       const int64_t slots = grid * warps;
       const int64_t stride = ((int64_t)m.nnz + 1 + 31) & ~31ll;
-      if (st.lu_slot_count < slots || !st.lu_slots.p)
+      if (st.lu_slot_count < slots * stride || !st.lu_slots.p)
       {
         st.lu_slots = DeviceMemory(sizeof(double) * (size_t)(slots * stride));
-        st.lu_slot_count = slots;
+        st.lu_slot_count = slots * stride;
       }
       A.lu_global = st.lu_slots.as<double>();
       A.lu_slot_stride = stride;

@@ -14,6 +14,7 @@
 // the CTA runs while any of its warps has a cell.
 #include "pipeline.cuh"
 #include "runtime.hpp"
+#include "stream_engine.cuh"
 
 #include <algorithm>
 
@@ -21,8 +22,10 @@ namespace micmb
 {
   namespace
   {
+    using namespace stream;
     constexpr int kWarp = 32;
     constexpr int kMaxSlots = 8;
+    constexpr int kMaxConsumers = 12;  // consumer warps per CTA (register file: 13 warps x 32 x 157)
     constexpr int kBlockBytes = kStreamBlockBytes;
 
     __device__ __forceinline__ size_t cell_base(int64_t c, int32_t L, int32_t ncol)
@@ -35,10 +38,6 @@ namespace micmb
       return (v + 1) & ~1;
     }
 
-    __host__ __device__ inline int32_t Pad16(int32_t v)
-    {
-      return (v + 15) & ~15;
-    }
 
     struct StreamArgs
     {
@@ -49,28 +48,32 @@ namespace micmb
       int32_t n_slots;
       int32_t f_n, j_n, lu_n, fw_n, bw_n;  // blocks per phase
       int32_t* error_flag;
+      const double* coef;                  // negated gather coefficients
+      int32_t n_coef;
     };
 
     struct Layout
     {
-      int32_t VS, KS, SC, LUS, per_warp;  // doubles
-      int32_t ring_offset;                // bytes from smem start
+      int32_t VS, KS, SC, LUS, per_warp;  // doubles (LUS = 0: the LU lives in a global slot)
+      int32_t coef_offset;                // bytes from smem start: coefficient table (CTA-wide)
+      int32_t ring_offset;
       int32_t bar_offset;
       int32_t flag_offset;
       int32_t total_bytes;
     };
 
     __host__ __device__ inline Layout MakeLayout(int32_t S, int32_t R, int32_t stages, int32_t n_info, int32_t nnz,
-                                                 int32_t warps, int32_t slots)
+                                                 int32_t n_coef, int32_t warps, int32_t slots, bool lu_shared)
     {
       Layout l;
       const int32_t scratch_cols = R > n_info ? R : n_info;
-      l.VS = RoundUp2(S + 1);
+      l.VS = RoundUp2(S + 2);  // slot S holds 0, slot S + 1 holds 1
       l.KS = RoundUp2(R > 0 ? R : 1);
       l.SC = RoundUp2(scratch_cols + 1);
-      l.LUS = RoundUp2(nnz + 1);
+      l.LUS = lu_shared ? RoundUp2(nnz + 1) : 0;
       l.per_warp = l.VS * (4 + stages) + l.KS + l.SC + l.LUS;  // 1/a_ii shares Fc's slot
-      l.ring_offset = Pad16(l.per_warp * 8 * warps);
+      l.coef_offset = Pad16(l.per_warp * 8 * warps);
+      l.ring_offset = Pad16(l.coef_offset + 8 * n_coef);
       l.bar_offset = l.ring_offset + slots * kBlockBytes;
       l.flag_offset = l.bar_offset + 2 * slots * 8;
       l.total_bytes = l.flag_offset + 2 * 16 * 4 + 16;
@@ -110,188 +113,16 @@ namespace micmb
       }
     };
 
-    struct Seg
-    {
-      int32_t T, n, flags, bytes;
-      const uint32_t* items;
-      const uint32_t* terms;
-      const double* coef;
-    };
-
-    __device__ __forceinline__ Seg read_seg(const uint8_t* p)
-    {
-      const int4 d = *reinterpret_cast<const int4*>(p);
-      Seg s;
-      s.T = d.x;
-      s.n = d.y & 0xFF;
-      s.flags = d.y >> 8;
-      s.bytes = d.z;
-      s.items = reinterpret_cast<const uint32_t*>(p + 16);
-      const int32_t ib = Pad16(4 * s.n);
-      s.terms = reinterpret_cast<const uint32_t*>(p + 16 + ib);
-      s.coef = reinterpret_cast<const double*>(p + 16 + ib + Pad16(4 * s.n * s.T));
-      return s;
-    }
-
-    // out[target] = sum coef * src[idx] (+ alpha on flagged items)
-    __device__ void blk_gather(const uint8_t* blk, const double* src, double* out, double alpha, double& acc, int lane)
-    {
-      const int32_t nseg = *reinterpret_cast<const int32_t*>(blk);
-      const uint8_t* p = blk + 16;
-      for (int32_t g = 0; g < nseg; ++g)
-      {
-        const Seg s = read_seg(p);
-        if (lane < s.n)
-        {
-          if (s.flags & kSegFirst)
-            acc = 0.0;
-          const uint32_t* tp = s.terms + lane;
-          const double* cp = s.coef + lane;
-          const int32_t n = s.n;
-          int32_t t = 0;
-          for (; t + 4 <= s.T; t += 4)
-          {
-            const uint32_t q0 = tp[(t + 0) * n], q1 = tp[(t + 1) * n], q2 = tp[(t + 2) * n], q3 = tp[(t + 3) * n];
-            const double f0 = cp[(t + 0) * n], f1 = cp[(t + 1) * n], f2 = cp[(t + 2) * n], f3 = cp[(t + 3) * n];
-            const double s0 = src[q0], s1 = src[q1], s2 = src[q2], s3 = src[q3];
-            acc += f0 * s0;
-            acc += f1 * s1;
-            acc += f2 * s2;
-            acc += f3 * s3;
-          }
-          for (; t < s.T; ++t)
-            acc += cp[t * n] * src[tp[t * n]];
-          if (s.flags & kSegLast)
-          {
-            const uint32_t it = s.items[lane];
-            double v = acc;
-            if ((it >> 16) != 0xFFFFu)
-              v += alpha;
-            out[it & 0xFFFFu] = v;
-          }
-        }
-        if (s.flags & kSegLevelEnd)
-          __syncwarp();
-        p += s.bytes;
-      }
-    }
-
-    // in-place LU block (item flags as in warp_lu)
-    __device__ void blk_lu(const uint8_t* blk, double* A, double* inv, double& acc, int lane)
-    {
-      const int32_t nseg = *reinterpret_cast<const int32_t*>(blk);
-      const uint8_t* p = blk + 16;
-      for (int32_t g = 0; g < nseg; ++g)
-      {
-        const Seg s = read_seg(p);
-        if (lane < s.n)
-        {
-          const uint32_t it = s.items[lane];
-          const uint32_t e = it & 0xFFFFu, hi = it >> 16;
-          if (s.flags & kSegFirst)
-            acc = A[e];
-          const uint32_t* tp = s.terms + lane;
-          const int32_t n = s.n;
-          int32_t t = 0;
-          for (; t + 4 <= s.T; t += 4)
-          {
-            const uint32_t q0 = tp[(t + 0) * n], q1 = tp[(t + 1) * n], q2 = tp[(t + 2) * n], q3 = tp[(t + 3) * n];
-            const double a0 = A[q0 & 0xFFFFu], b0 = A[q0 >> 16], a1 = A[q1 & 0xFFFFu], b1 = A[q1 >> 16];
-            const double a2 = A[q2 & 0xFFFFu], b2 = A[q2 >> 16], a3 = A[q3 & 0xFFFFu], b3 = A[q3 >> 16];
-            acc -= a0 * b0;
-            acc -= a1 * b1;
-            acc -= a2 * b2;
-            acc -= a3 * b3;
-          }
-          for (; t < s.T; ++t)
-          {
-            const uint32_t q = tp[t * n];
-            acc -= A[q & 0xFFFFu] * A[q >> 16];
-          }
-          if (s.flags & kSegLast)
-          {
-            if (hi >= 0xFFFEu)  // U entry, or a partial sum
-              A[e] = acc;
-            else if (hi & 0x8000u)
-            {
-              A[e] = acc;
-              inv[hi & 0x7FFFu] = 1.0 / acc;
-            }
-            else
-              A[e] = acc * inv[hi];
-          }
-        }
-        if (s.flags & kSegLevelEnd)
-          __syncwarp();
-        p += s.bytes;
-      }
-    }
-
-    // triangular-solve block: x_i = (x_i - sum A[a] x[b]) [/ A[aux]]
-    __device__ void blk_solve(const uint8_t* blk, const double* A, double* x, double& acc, int lane)
-    {
-      const int32_t nseg = *reinterpret_cast<const int32_t*>(blk);
-      const uint8_t* p = blk + 16;
-      for (int32_t g = 0; g < nseg; ++g)
-      {
-        const Seg s = read_seg(p);
-        if (lane < s.n)
-        {
-          const uint32_t it = s.items[lane];
-          const uint32_t i = it & 0xFFFFu, hi = it >> 16;
-          if (s.flags & kSegFirst)
-            acc = x[i];
-          const uint32_t* tp = s.terms + lane;
-          const int32_t n = s.n;
-          int32_t t = 0;
-          for (; t + 4 <= s.T; t += 4)
-          {
-            const uint32_t q0 = tp[(t + 0) * n], q1 = tp[(t + 1) * n], q2 = tp[(t + 2) * n], q3 = tp[(t + 3) * n];
-            const double a0 = A[q0 & 0xFFFFu], b0 = x[q0 >> 16], a1 = A[q1 & 0xFFFFu], b1 = x[q1 >> 16];
-            const double a2 = A[q2 & 0xFFFFu], b2 = x[q2 >> 16], a3 = A[q3 & 0xFFFFu], b3 = x[q3 >> 16];
-            acc -= a0 * b0;
-            acc -= a1 * b1;
-            acc -= a2 * b2;
-            acc -= a3 * b3;
-          }
-          for (; t < s.T; ++t)
-          {
-            const uint32_t q = tp[t * n];
-            acc -= A[q & 0xFFFFu] * x[q >> 16];
-          }
-          if (s.flags & kSegLast)
-            x[i] = (hi >= 0xFFFEu) ? acc : acc / A[hi];
-        }
-        if (s.flags & kSegLevelEnd)
-          __syncwarp();
-        p += s.bytes;
-      }
-    }
-
-    enum
-    {
-      kGather = 0,
-      kLU = 1,
-      kSolve = 2
-    };
-
     template<int KIND>
-    __device__ __forceinline__ void consume(Ring& ring, int32_t n_blocks, bool active, const double* src, double* A,
-                                            double* x, double alpha, int lane)
+    __device__ __forceinline__ void consume(Ring& ring, int32_t n_blocks, bool active, const double* X,
+                                            const double* Yv, double* out, double* inv, double alpha, int lane)
     {
-      double acc = 0.0;
+      double acc[4] = { 0.0, 0.0, 0.0, 0.0 };
       for (int32_t b = 0; b < n_blocks; ++b)
       {
         const uint8_t* blk = ring.acquire();
         if (blk && active)
-        {
-          if constexpr (KIND == kGather)
-            blk_gather(blk, src, A, alpha, acc, lane);
-          else if constexpr (KIND == kLU)
-            blk_lu(blk, A, x, acc, lane);
-          else
-            blk_solve(blk, A, x, acc, lane);
-        }
+          blk_run<KIND>(blk, X, Yv, out, inv, alpha, acc, lane);
         ring.release(lane);
       }
     }
@@ -341,6 +172,9 @@ namespace micmb
         *abort_flag = 0;
         fence_barrier_init();
       }
+      double* coefs = reinterpret_cast<double*>(sm + LY.coef_offset);
+      for (int32_t i = threadIdx.x; i < SA.n_coef; i += blockDim.x)
+        coefs[i] = SA.coef[i];
       __syncthreads();
 
       if (warp == W)
@@ -403,13 +237,16 @@ namespace micmb
       double* K = Fc + VS;
       double* kk = K + (size_t)P.stages * VS;
       double* scr = kk + LY.KS;
-      double* LU = scr + LY.SC;
+      double* LU = LY.LUS ? scr + LY.SC
+                          : A.lu_global + ((size_t)blockIdx.x * W + warp) * (size_t)A.lu_slot_stride;
       if (lane == 0)
       {
         for (int32_t st = 0; st < P.stages; ++st)
           K[(size_t)st * VS + S] = 0.0;
         Y[S] = 0.0;
         Yn[S] = 0.0;
+        Y[S + 1] = 1.0;
+        Yn[S + 1] = 1.0;
         scr[M.scratch_zero] = 0.0;
         LU[M.nnz] = 0.0;
       }
@@ -503,22 +340,28 @@ namespace micmb
         const bool do_f0 = act && wc.need_f0;
         if (do_f0)
         {
-          reaction_rates<kWarp>(M, Unit{ kk }, Unit{ Y }, Unit{ scr }, lane);
+          if (M.rate_desc)
+            reaction_rates_narrow<kWarp>(M, Unit{ kk }, Unit{ Y }, Unit{ scr }, lane);
+          else
+            reaction_rates<kWarp>(M, Unit{ kk }, Unit{ Y }, Unit{ scr }, lane);
           __syncwarp();
         }
-        consume<kGather>(ring, SA.f_n, do_f0, scr, F0, nullptr, 0.0, lane);
+        consume<kGather>(ring, SA.f_n, do_f0, scr, coefs, F0, nullptr, 0.0, lane);
         __syncwarp();
         // alpha I - J at Y, then LU
         const double H = wc.c.H;
         const double alpha = 1.0 / (H * P.gamma0);
         if (act)
         {
-          jacobian_rates<kWarp>(M, Unit{ kk }, Unit{ Y }, Unit{ scr }, lane);
+          if (M.drate_desc)
+            jacobian_rates_narrow<kWarp>(M, Unit{ kk }, Unit{ Y }, Unit{ scr }, lane);
+          else
+            jacobian_rates<kWarp>(M, Unit{ kk }, Unit{ Y }, Unit{ scr }, lane);
           __syncwarp();
         }
-        consume<kGather>(ring, SA.j_n, act, scr, LU, nullptr, alpha, lane);
+        consume<kGather>(ring, SA.j_n, act, scr, coefs, LU, nullptr, alpha, lane);
         __syncwarp();
-        consume<kLU>(ring, SA.lu_n, act, nullptr, LU, inv, 0.0, lane);
+        consume<kLU>(ring, SA.lu_n, act, LU, LU, LU, inv, 0.0, lane);
         __syncwarp();
         const double* Fsrc = F0;
         for (int32_t st = 0; st < P.stages; ++st)
@@ -536,31 +379,34 @@ namespace micmb
                 Yn[i] = v;
               }
               __syncwarp();
-              reaction_rates<kWarp>(M, Unit{ kk }, Unit{ Yn }, Unit{ scr }, lane);
+              if (M.rate_desc)
+                reaction_rates_narrow<kWarp>(M, Unit{ kk }, Unit{ Yn }, Unit{ scr }, lane);
+              else
+                reaction_rates<kWarp>(M, Unit{ kk }, Unit{ Yn }, Unit{ scr }, lane);
               __syncwarp();
             }
-            consume<kGather>(ring, SA.f_n, act, scr, Fc, nullptr, 0.0, lane);
+            consume<kGather>(ring, SA.f_n, act, scr, coefs, Fc, nullptr, 0.0, lane);
             __syncwarp();
             Fsrc = Fc;
           }
           double* Ks = K + (size_t)st * VS;
           if (act)
           {
+            double coh[6];
+            for (int32_t j = 0; j < st; ++j)
+              coh[j] = P.c[sc + j] / H;
             for (int32_t i = lane; i < S; i += kWarp)
             {
               double v = Fsrc[i];
               for (int32_t j = 0; j < st; ++j)
-              {
-                const double c_over_h = P.c[sc + j] / H;
-                v += c_over_h * K[(size_t)j * VS + i];
-              }
+                v += coh[j] * K[(size_t)j * VS + i];
               Ks[i] = v;
             }
           }
           __syncwarp();
-          consume<kSolve>(ring, SA.fw_n, act, nullptr, LU, Ks, 0.0, lane);
+          consume<kSolve>(ring, SA.fw_n, act, LU, Ks, Ks, nullptr, 0.0, lane);
           __syncwarp();
-          consume<kSolve>(ring, SA.bw_n, act, nullptr, LU, Ks, 0.0, lane);
+          consume<kSolveDiv>(ring, SA.bw_n, act, LU, Ks, Ks, nullptr, 0.0, lane);
           __syncwarp();
         }
         if (act && !*abort_flag)
@@ -642,13 +488,13 @@ namespace micmb
     }
   }  // namespace
 
-  int StreamWarpsPerCta(const micmb_solver& s, int slots, int cap)
+  int StreamWarpsPerCta(const micmb_solver& s, int slots, int cap, bool lu_shared)
   {
     const auto& m = *s.mech;
-    for (int w = std::min(cap > 0 ? cap : 8, 8); w >= 1; --w)
+    for (int w = std::min(cap > 0 ? cap : kMaxConsumers, kMaxConsumers); w >= 1; --w)
     {
-      const Layout l =
-          MakeLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz, w, slots);
+      const Layout l = MakeLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz, s.n_stream_coef, w,
+                                  slots, lu_shared);
       if ((size_t)l.total_bytes <= s.smem_optin)
         return w;
     }
@@ -661,10 +507,12 @@ namespace micmb
     if (!s.dev.has_warp || !s.stream_blocks.p)
       return false;
     const int slots = std::max(2, std::min(kMaxSlots, s.fused.ring_slots > 0 ? s.fused.ring_slots : 4));
-    const int W = StreamWarpsPerCta(s, slots, s.fused.cells_per_cta);
+    const bool lu_shared = s.fused.lu_in_shared != 0;
+    const int W = StreamWarpsPerCta(s, slots, s.fused.cells_per_cta, lu_shared);
     if (W < 1)
       return false;
-    const Layout LY = MakeLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz, W, slots);
+    const Layout LY =
+        MakeLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz, s.n_stream_coef, W, slots, lu_shared);
     // per-attempt block order: F0 forcing, -J, LU, then per stage [forcing], forward, backward
     std::vector<int32_t> order;
     auto add = [&](const StreamPhase& ph) {
@@ -697,19 +545,38 @@ namespace micmb
     SA.fw_n = m.stream.fwd.n_blocks;
     SA.bw_n = m.stream.bwd.n_blocks;
     SA.error_flag = reinterpret_cast<int32_t*>(st.counters.as<char>() + 16);
+    SA.coef = s.stream_coef.as<const double>();
+    SA.n_coef = s.n_stream_coef;
     int64_t grid = (int64_t)s.sm_count * (s.fused.ctas_per_sm > 0 ? s.fused.ctas_per_sm : 1);
     grid = std::max<int64_t>(1, std::min<int64_t>(grid, (st.n_cells + W - 1) / W));
+    FusedArgs A = A_in;
+    if (!lu_shared)
+    {
+      const int64_t slots_needed = grid * W;
+      const int64_t stride = ((int64_t)m.nnz + 2 + 31) & ~31ll;
+      if (st.lu_slot_count < slots_needed * stride || !st.lu_slots.p)
+      {
+        st.lu_slots = DeviceMemory(sizeof(double) * (size_t)(slots_needed * stride));
+        st.lu_slot_count = slots_needed * stride;
+      }
+      A.lu_global = st.lu_slots.as<double>();
+      A.lu_slot_stride = stride;
+    }
     st.dt_for_launch = dt;
     switch (W)
     {
-      case 1: Launch<1>(s, st, A_in, SA, LY, grid); break;
-      case 2: Launch<2>(s, st, A_in, SA, LY, grid); break;
-      case 3: Launch<3>(s, st, A_in, SA, LY, grid); break;
-      case 4: Launch<4>(s, st, A_in, SA, LY, grid); break;
-      case 5: Launch<5>(s, st, A_in, SA, LY, grid); break;
-      case 6: Launch<6>(s, st, A_in, SA, LY, grid); break;
-      case 7: Launch<7>(s, st, A_in, SA, LY, grid); break;
-      default: Launch<8>(s, st, A_in, SA, LY, grid); break;
+      case 1: Launch<1>(s, st, A, SA, LY, grid); break;
+      case 2: Launch<2>(s, st, A, SA, LY, grid); break;
+      case 3: Launch<3>(s, st, A, SA, LY, grid); break;
+      case 4: Launch<4>(s, st, A, SA, LY, grid); break;
+      case 5: Launch<5>(s, st, A, SA, LY, grid); break;
+      case 6: Launch<6>(s, st, A, SA, LY, grid); break;
+      case 7: Launch<7>(s, st, A, SA, LY, grid); break;
+      case 8: Launch<8>(s, st, A, SA, LY, grid); break;
+      case 9: Launch<9>(s, st, A, SA, LY, grid); break;
+      case 10: Launch<10>(s, st, A, SA, LY, grid); break;
+      case 11: Launch<11>(s, st, A, SA, LY, grid); break;
+      default: Launch<kMaxConsumers>(s, st, A, SA, LY, grid); break;
     }
     return true;
   }

@@ -135,39 +135,56 @@ namespace micmb
 
     // Lane-interleave a level schedule (see WarpTable).  `meta(i)` packs item i,
     // `pack(t)` packs term t, `coef` (optional) is per term; padding terms
-    // are `dummy` with coefficient 0.
-    template<class Meta, class Pack>
-    WarpTable BuildWarp(const LevelSchedule& s, Meta meta, Pack pack, uint32_t dummy, const std::vector<double>* coef)
+    // are `dummy` with coefficient 0.  `cls(i)` (0 or kSegRecip) keeps items
+    // that finalise differently in separate chunks; chunk_flags records it.
+    template<class Meta, class Pack, class Cls>
+    WarpTable BuildWarp(const LevelSchedule& s, Meta meta, Pack pack, uint32_t dummy, const std::vector<double>* coef,
+                        Cls cls)
     {
       WarpTable w;
+      w.dummy = dummy;
       w.n_levels = s.n_levels();
       w.level_chunk_start.push_back(0);
       for (int32_t l = 0; l < w.n_levels; ++l)
       {
-        for (int32_t first = s.level_start[l]; first < s.level_start[l + 1]; first += 32)
+        // items of the level, class by class, each class longest first (the schedule's order)
+        std::vector<int32_t> order;
+        for (int32_t i = s.level_start[l]; i < s.level_start[l + 1]; ++i)
+          order.push_back(i);
+        std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return cls(a) < cls(b); });
+        for (size_t first = 0; first < order.size();)
         {
-          const int32_t n = std::min<int32_t>(32, s.level_start[l + 1] - first);
+          const int32_t c = cls(order[first]);
+          size_t last = first;
+          while (last < order.size() && last - first < 32 && cls(order[last]) == c)
+            ++last;
+          const int32_t n = (int32_t)(last - first);
           int32_t T = 0;
-          for (int32_t i = first; i < first + n; ++i)
-            T = std::max(T, s.term_start[i + 1] - s.term_start[i]);
+          for (size_t q = first; q < last; ++q)
+            T = std::max(T, s.term_start[order[q] + 1] - s.term_start[order[q]]);
           w.chunk.push_back((int32_t)w.term.size());
           w.chunk.push_back(T);
           w.chunk.push_back((int32_t)w.item.size());
           w.chunk.push_back(n);
-          for (int32_t i = first; i < first + n; ++i)
-            w.item.push_back(meta(i));
+          w.chunk_flags.push_back(c);
+          for (size_t q = first; q < last; ++q)
+            w.item.push_back(meta(order[q]));
           const size_t base = w.term.size();
           w.term.resize(base + (size_t)T * 32, dummy);
           if (coef)
             w.coef.resize(base + (size_t)T * 32, 0.0);
-          for (int32_t i = first; i < first + n; ++i)
+          for (size_t q = first; q < last; ++q)
+          {
+            const int32_t i = order[q];
             for (int32_t t = s.term_start[i]; t < s.term_start[i + 1]; ++t)
             {
-              const size_t at = base + (size_t)(t - s.term_start[i]) * 32 + (size_t)(i - first);
+              const size_t at = base + (size_t)(t - s.term_start[i]) * 32 + (q - first);
               w.term[at] = pack(t);
               if (coef)
                 w.coef[at] = (*coef)[t];
             }
+          }
+          first = last;
         }
         w.level_chunk_start.push_back((int32_t)(w.chunk.size() / 4));
       }
@@ -204,10 +221,39 @@ namespace micmb
       return (b + 15) & ~15;
     }
 
-    // Re-cut one warp table into stream blocks (see StreamProgram).
-    void AppendStreamPhase(StreamProgram& P, const WarpTable& w, StreamPhase& ph)
+    // index of -c in the stream's coefficient table (entry 0 stays +0 for padding)
+    uint32_t InternCoef(StreamProgram& P, std::map<uint64_t, uint32_t>& seen, double c)
+    {
+      if (P.coef_table.empty())
+        P.coef_table.push_back(0.0);
+      const double v = -c;
+      uint64_t bits;
+      std::memcpy(&bits, &v, sizeof(bits));
+      auto it = seen.find(bits);
+      if (it != seen.end())
+        return it->second;
+      const uint32_t idx = (uint32_t)P.coef_table.size();
+      if (idx > 0xFFFFu)
+        throw std::runtime_error("too many distinct coefficients for the streamed schedule");
+      P.coef_table.push_back(v);
+      seen.emplace(bits, idx);
+      return idx;
+    }
+
+    // operand pair of 16-bit element indices -> pair of 16-bit byte offsets
+    inline uint32_t ToBytes(uint32_t v)
+    {
+      return (((v & 0xFFFFu) * 8u) & 0xFFFFu) | ((((v >> 16) * 8u) & 0xFFFFu) << 16);
+    }
+
+    // Re-cut one warp table into stream blocks (see StreamProgram).  Weighted
+    // gathers (w.coef non-empty) get their coefficients interned in the table.
+    void AppendStreamPhase(StreamProgram& P, std::map<uint64_t, uint32_t>& seen, const WarpTable& w,
+                           StreamPhase& ph)
     {
       const bool has_coef = !w.coef.empty();
+      if (P.coef_table.empty())
+        P.coef_table.push_back(0.0);
       const int32_t B = kStreamBlockBytes;
       int32_t n_blocks = (int32_t)P.block_bytes.size();
       ph.first_block = n_blocks;
@@ -225,25 +271,54 @@ namespace micmb
         ++n_blocks;
       };
       open_block();
+      auto packed = [&](size_t at) -> uint32_t {
+        if (!has_coef)
+          return w.term[at];
+        const double c = w.coef[at];
+        uint64_t bits;
+        std::memcpy(&bits, &c, sizeof(bits));
+        const uint32_t cidx = bits == 0 ? 0u : InternCoef(P, seen, c);
+        return (w.term[at] & 0xFFFFu) | (cidx << 16);
+      };
+      const uint32_t pad_term = has_coef ? (w.dummy & 0xFFFFu) : w.dummy;  // coefficient entry 0 is +0
+      // term t of lane `lane` in chunk ch (padding past the chunk's own length)
+      auto term_of = [&](int32_t ch, int32_t lane, int32_t t) -> uint32_t {
+        const int32_t base = w.chunk[4 * ch + 0], T = w.chunk[4 * ch + 1], n = w.chunk[4 * ch + 3];
+        return (t < T && lane < n) ? packed((size_t)base + (size_t)t * 32 + lane) : pad_term;
+      };
       for (int32_t l = 0; l < w.n_levels; ++l)
       {
-        for (int32_t ch = w.level_chunk_start[l]; ch < w.level_chunk_start[l + 1]; ++ch)
+        const int32_t c_end = w.level_chunk_start[l + 1];
+        for (int32_t ch = w.level_chunk_start[l]; ch < c_end;)
         {
-          const int32_t base = w.chunk[4 * ch + 0], T = w.chunk[4 * ch + 1], first = w.chunk[4 * ch + 2],
-                        n = w.chunk[4 * ch + 3];
-          const bool last_in_level = (ch + 1 == w.level_chunk_start[l + 1]);
-          const int32_t fixed = 16 + Pad16(4 * n);
+          // Up to four chunks of similar length run side by side (U = 4: one
+          // accumulator per chunk in every lane); a chunk much longer than the
+          // next one runs alone, four terms per step (U = 1).
+          const int32_t T0 = w.chunk[4 * ch + 1];
+          const int32_t cflags = w.chunk_flags[ch];
+          auto joins = [&](int32_t c) {
+            return c < c_end && w.chunk_flags[c] == cflags && T0 <= 2 * w.chunk[4 * c + 1] + 2;
+          };
+          int32_t U = 1, width = 1;
+          if (T0 <= kWideMaxSteps && joins(ch + 1))
+          {
+            U = 4;
+            while (width < 4 && joins(ch + width))
+              ++width;
+          }
+          const int32_t T = T0, n = w.chunk[4 * ch + 3];
+          const bool last_in_level = (ch + width == c_end);
+          const int32_t fixed = 16 + Pad16(4 * n * U);
+          const int32_t per_group = 16 * n;
+          const int32_t step_quantum = (U == 1) ? 4 : 1;  // terms per uint4 and lane
           int32_t t0 = 0;
           bool first_seg = true;
           for (;;)
           {
             const int32_t avail = B - used;
             int32_t tseg = 0;
-            // largest tseg with fixed + Pad16(4 n tseg) + coef bytes <= avail
-            const int32_t per_t = 4 * n + (has_coef ? 8 * n : 0);
-            if (avail >= fixed + 32)
-              tseg = std::min(T - t0, (avail - fixed - 32) / per_t);  // 32: padding of both arrays
-            tseg = std::max(tseg, 0);
+            if (avail >= fixed)
+              tseg = std::min(T - t0, step_quantum * ((avail - fixed) / per_group));
             const bool fits = avail >= fixed && (tseg > 0 || T == t0);
             if (!fits)
             {
@@ -253,29 +328,47 @@ namespace micmb
               open_block();
               continue;
             }
-            const int32_t term_bytes = Pad16(4 * n * tseg);
-            const int32_t seg_bytes = Pad16(fixed + term_bytes + (has_coef ? 8 * n * tseg : 0));
+            const int32_t groups = (tseg + step_quantum - 1) / step_quantum;
+            const int32_t seg_bytes = fixed + per_group * groups;
             uint8_t* seg = block_ptr() + used;
-            int32_t flags = first_seg ? kSegFirst : 0;
+            int32_t flags = (first_seg ? kSegFirst : 0) | cflags;
             const bool last_seg = (t0 + tseg == T);
             if (last_seg)
               flags |= kSegLast;
             if (last_seg && last_in_level)
               flags |= kSegLevelEnd;
-            const int32_t desc[4] = { tseg, n | (flags << 8), seg_bytes, 0 };
+            const int32_t desc[4] = { tseg, n | (flags << 8) | (U << 16), seg_bytes, 0 };
             std::memcpy(seg, desc, 16);
-            std::memcpy(seg + 16, w.item.data() + first, 4 * (size_t)n);
-            uint32_t* terms = reinterpret_cast<uint32_t*>(seg + fixed);
-            for (int32_t t = 0; t < tseg; ++t)
+            uint32_t* items = reinterpret_cast<uint32_t*>(seg + 16);
+            for (int32_t u = 0; u < U; ++u)
               for (int32_t lane = 0; lane < n; ++lane)
-                terms[t * n + lane] = w.term[(size_t)base + (size_t)(t0 + t) * 32 + lane];
-            if (has_coef)
-            {
-              double* cf = reinterpret_cast<double*>(seg + fixed + term_bytes);
-              for (int32_t t = 0; t < tseg; ++t)
-                for (int32_t lane = 0; lane < n; ++lane)
-                  cf[t * n + lane] = w.coef[(size_t)base + (size_t)(t0 + t) * 32 + lane];
-            }
+              {
+                const int32_t c = ch + u;
+                const bool real = u < width && lane < w.chunk[4 * c + 3];
+                uint32_t it = kNoItem;
+                if (real)
+                {
+                  it = w.item[(size_t)w.chunk[4 * c + 2] + lane];
+                  it = (it & 0xFFFF0000u) | (((it & 0xFFFFu) * 8u) & 0xFFFFu);
+                }
+                items[u * n + lane] = it;
+              }
+            uint32_t* terms = reinterpret_cast<uint32_t*>(seg + fixed);
+            for (int32_t g = 0; g < groups; ++g)
+              for (int32_t lane = 0; lane < n; ++lane)
+                for (int32_t k = 0; k < 4; ++k)
+                {
+                  uint32_t v = pad_term;
+                  if (U == 1)
+                  {
+                    const int32_t t = t0 + 4 * g + k;
+                    if (t < T)
+                      v = term_of(ch, lane, t);
+                  }
+                  else if (k < width)
+                    v = term_of(ch + k, lane, t0 + g);
+                  terms[(g * n + lane) * 4 + k] = ToBytes(v);
+                }
             used += seg_bytes;
             ++n_segs;
             t0 += tseg;
@@ -283,6 +376,7 @@ namespace micmb
             if (last_seg)
               break;
           }
+          ch += width;
         }
       }
       close_block();
@@ -757,7 +851,10 @@ namespace micmb
             return (uint32_t)e | (hi << 16);
           },
           [&](int32_t t) { return pack2((uint32_t)m.lu.term_a[t], (uint32_t)m.lu.term_b[t]); }, pack2(NZ, NZ),
-          nullptr);
+          nullptr, [&](int32_t i) {
+            const int32_t e = m.lu.item_target[i];
+            return (m.lu.item_aux[i] != -2 && m.nz_row[e] == m.nz_col[e]) ? kSegRecip : 0;
+          });
       auto solve_table = [&](const LevelSchedule& s) {
         return BuildWarp(
             s,
@@ -765,7 +862,8 @@ namespace micmb
               const uint32_t hi = s.item_aux[i] == -2 ? 0xFFFEu : (s.item_aux[i] < 0 ? 0xFFFFu : (uint32_t)s.item_aux[i]);
               return (uint32_t)s.item_target[i] | (hi << 16);
             },
-            [&](int32_t t) { return pack2((uint32_t)s.term_a[t], (uint32_t)s.term_b[t]); }, pack2(NZ, SV), nullptr);
+            [&](int32_t t) { return pack2((uint32_t)s.term_a[t], (uint32_t)s.term_b[t]); }, pack2(NZ, SV), nullptr,
+            [](int32_t) { return 0; });
       };
       m.w_fwd = solve_table(m.fwd);
       m.w_bwd = solve_table(m.bwd);
@@ -775,7 +873,8 @@ namespace micmb
       const LevelSchedule fs = GatherSchedule(m.f_start, m.f_rxn, m.f_coef, fco);
       m.w_forcing = BuildWarp(
           fs, [&](int32_t i) { return (uint32_t)fs.item_target[i] | (0xFFFFu << 16); },
-          [&](int32_t t) { return (uint32_t)fs.term_a[t]; }, (uint32_t)m.scratch_zero, &fco);
+          [&](int32_t t) { return (uint32_t)fs.term_a[t]; }, (uint32_t)m.scratch_zero, &fco,
+          [](int32_t) { return 0; });
       const LevelSchedule js = GatherSchedule(m.j_start, m.j_info, m.j_coef, jco);
       m.w_jacobian = BuildWarp(
           js,
@@ -784,15 +883,42 @@ namespace micmb
             const uint32_t hi = (m.nz_row[e] == m.nz_col[e]) ? (0x8000u | (uint32_t)m.nz_row[e]) : 0xFFFFu;
             return (uint32_t)e | (hi << 16);
           },
-          [&](int32_t t) { return (uint32_t)js.term_a[t]; }, (uint32_t)m.scratch_zero, &jco);
+          [&](int32_t t) { return (uint32_t)js.term_a[t]; }, (uint32_t)m.scratch_zero, &jco,
+          [](int32_t) { return 0; });
       m.has_warp_tables = true;
-      AppendStreamPhase(m.stream, m.w_forcing, m.stream.forcing);
-      AppendStreamPhase(m.stream, m.w_jacobian, m.stream.jacobian);
-      AppendStreamPhase(m.stream, m.w_lu, m.stream.lu);
-      AppendStreamPhase(m.stream, m.w_fwd, m.stream.fwd);
-      AppendStreamPhase(m.stream, m.w_bwd, m.stream.bwd);
-      AppendStreamPhase(m.stream, m.w_fwd_t, m.stream.fwd_t);
-      AppendStreamPhase(m.stream, m.w_bwd_t, m.stream.bwd_t);
+      bool narrow = true;
+      for (int32_t r = 0; r < R; ++r)
+        narrow &= (m.react_start[r + 1] - m.react_start[r]) <= 3;
+      if (narrow)
+      {
+        const int32_t one = S + 1;
+        m.rate_desc.assign((size_t)4 * R, one);
+        for (int32_t r = 0; r < R; ++r)
+          for (int32_t i = m.react_start[r]; i < m.react_start[r + 1]; ++i)
+            m.rate_desc[(size_t)4 * r + (i - m.react_start[r])] = m.react_ids[i];
+        const int32_t ni = (int32_t)m.info_rxn.size();
+        m.drate_desc.assign((size_t)4 * ni, one);
+        for (int32_t i = 0; i < ni; ++i)
+        {
+          m.drate_desc[(size_t)4 * i] = m.info_rxn[i];
+          for (int32_t d = m.info_dep_start[i]; d < m.info_dep_start[i + 1]; ++d)
+            m.drate_desc[(size_t)4 * i + 1 + (d - m.info_dep_start[i])] = m.info_dep_ids[d];
+        }
+      }
+      std::map<uint64_t, uint32_t> seen;
+      m.stream = StreamProgram{};
+      AppendStreamPhase(m.stream, seen, m.w_forcing, m.stream.forcing);
+      AppendStreamPhase(m.stream, seen, m.w_jacobian, m.stream.jacobian);
+      AppendStreamPhase(m.stream, seen, m.w_lu, m.stream.lu);
+      AppendStreamPhase(m.stream, seen, m.w_fwd, m.stream.fwd);
+      AppendStreamPhase(m.stream, seen, m.w_bwd, m.stream.bwd);
+      AppendStreamPhase(m.stream, seen, m.w_fwd_t, m.stream.fwd_t);
+      AppendStreamPhase(m.stream, seen, m.w_bwd_t, m.stream.bwd_t);
+      // operands are addressed by 16-bit byte offsets from their array
+      const int64_t limit = 0xFFFF / 8;
+      if (m.nnz + 1 >= limit || S + 2 >= limit || scratch_cols + 1 >= limit ||
+          (int64_t)m.stream.coef_table.size() >= limit)
+        m.stream = StreamProgram{};
     }
 
     // 11. hash of everything the device sees

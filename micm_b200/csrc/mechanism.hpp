@@ -58,20 +58,34 @@ namespace micmb
     std::vector<uint32_t> item;              // packed item metadata
     std::vector<uint32_t> term;              // packed operand pair (a | b << 16)
     std::vector<double> coef;                // per-term coefficient (gathers with weights)
+    uint32_t dummy = 0;                      // padding term (operands that hold 0)
+    std::vector<int32_t> chunk_flags;        // [n_chunks]: extra segment flags (kSegRecip)
   };
 
   // The warp tables re-cut into fixed-size blocks for bulk (TMA) streaming
-  // into a shared-memory ring.  A block holds a 16-byte header (segment count)
-  // followed by segments laid end to end:
-  //   int4 {T, n | flags << 8, segment bytes, 0}
-  //   uint32 items[n]            (padded to 16 bytes)
-  //   uint32 terms[T][n]         (lane l's term t at t*n + l, padded to 16 bytes)
-  //   double coef[T][n]          (weighted gathers only)
-  // A chunk whose terms do not fit in the rest of a block continues in the
-  // next block (FIRST/LAST flags); LEVEL_END marks the end of a dependency
-  // level (the warp synchronises there).
+  // into a shared-memory ring.  Every term of every phase has one form,
+  //   acc = acc - X[a] * Y[b],   packed as a | b << 16,
+  // with X, Y chosen by the phase: LU (X = Y = factor), triangular solves
+  // (X = factor, Y = vector), weighted gathers (X = rates, Y = the table of
+  // negated coefficients `coef_table`; acc + c*w and acc - (-c)*w round
+  // identically).  A block holds a 16-byte header (segment count) followed by
+  // segments laid end to end:
+  //   int4 {T, n | flags << 8 | U << 16, segment bytes, 0}
+  //   uint32 items[U][n]           (padded to 16 bytes; kNoItem = empty slot)
+  //   U = 1: uint4 terms[ceil(T/4)][n]  (lane l's terms 4g..4g+3 at g*n + l)
+  //   U = 4: uint4 terms[T][n]          (term t of lane l's four items at t*n + l)
+  // With U = 4 every lane carries four independent sums.  Lanes with fewer
+  // than T terms are padded with products that are exactly +0 (operands
+  // that hold 0), which leave every sum bit-identical.  A chunk whose terms
+  // do not fit in the rest of a block continues in the next block
+  // (FIRST/LAST flags; U = 1 splits fall on 4-term boundaries); LEVEL_END
+  // marks the end of a dependency level (the warp synchronises there).
   constexpr int32_t kStreamBlockBytes = 8192;
-  constexpr int32_t kSegFirst = 1, kSegLast = 2, kSegLevelEnd = 4;
+  // kSegRecip: every item of the segment is a diagonal LU entry (store the
+  // pivot and its reciprocal); all other LU items store sum * (1/a_kk or 1).
+  constexpr int32_t kSegFirst = 1, kSegLast = 2, kSegLevelEnd = 4, kSegRecip = 8;
+  constexpr uint32_t kNoItem = 0xFFFFFFFFu;
+  constexpr int32_t kWideMaxSteps = 48;  // longest chunk run four-wide
 
   struct StreamPhase
   {
@@ -83,6 +97,7 @@ namespace micmb
   {
     std::vector<uint8_t> bytes;          // all blocks, each kStreamBlockBytes apart
     std::vector<int32_t> block_bytes;    // used bytes per block (multiple of 16)
+    std::vector<double> coef_table;      // negated gather coefficients; entry 0 is +0
     StreamPhase forcing, jacobian, lu, fwd, bwd, fwd_t, bwd_t;
   };
 
@@ -140,6 +155,12 @@ namespace micmb
     // scratch slot `scratch_zero`, all holding 0.0
     bool has_warp_tables = false;
     int32_t scratch_zero = 0;
+    // Fixed-width product lists for the fused kernels: rate_desc[4r..4r+2] are
+    // the reactant columns of reaction r, drate_desc[4i] the rate column and
+    // [4i+1..4i+3] the dependent columns of info i, padded with column S + 1
+    // (a slot holding 1.0; multiplying by it is exact).  Empty unless every
+    // reaction has at most three reactants.
+    std::vector<int32_t> rate_desc, drate_desc;
     WarpTable w_lu, w_fwd, w_bwd, w_fwd_t, w_bwd_t, w_forcing, w_jacobian;
     StreamProgram stream;
 

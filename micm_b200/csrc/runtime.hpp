@@ -97,6 +97,8 @@ struct micmb_solver
   micmb_fused_config fused{ 0, 1, 0, 0, 0 };
   micmb::DeviceMemory stream_blocks;       // StreamProgram bytes
   micmb::DeviceMemory stream_block_bytes;  // [n_blocks]
+  micmb::DeviceMemory stream_coef;         // StreamProgram coef_table
+  int32_t n_stream_coef = 0;
 };
 
 struct micmb_state
@@ -118,7 +120,7 @@ struct micmb_state
   int32_t* host_counters = nullptr;  // pinned
   // fused path
   micmb::DeviceMemory lu_slots;
-  int64_t lu_slot_count = 0;
+  int64_t lu_slot_count = 0;  // doubles allocated in lu_slots
   micmb::DeviceMemory attempt_order;  // streamed kernel: block order of one attempt
   double dt_for_launch = 0.0;
 
@@ -147,6 +149,6 @@ namespace micmb
   size_t FusedSharedBytes(const micmb_solver& s, bool lu_in_shared);
   // streamed warp-specialised variant; returns false when it does not apply
   bool SolveFusedStream(micmb_solver& s, micmb_state& st, double dt, const FusedArgs& A);
-  int StreamWarpsPerCta(const micmb_solver& s, int slots, int cap);
+  int StreamWarpsPerCta(const micmb_solver& s, int slots, int cap, bool lu_shared);
   int FusedWarpsPerCta(const micmb_solver& s, const micmb_fused_config& cfg);
 }  // namespace micmb
