@@ -189,6 +189,7 @@ namespace micmb
       const size_t o_kind = pk.add(kind), o_rp = pk.add(rp), o_pcol = pk.add(pcol), o_nm = pk.add(nmult),
                    o_mult = pk.add(mult);
       const size_t o_rs = pk.add(m.react_start), o_ri = pk.add(m.react_ids);
+      const size_t o_ps = pk.add(m.prod_start), o_pi = pk.add(m.prod_ids), o_py = pk.add(m.prod_yield);
       const size_t o_fs = pk.add(m.f_start), o_fr = pk.add(m.f_rxn), o_fc = pk.add(m.f_coef);
       const size_t o_ir = pk.add(m.info_rxn), o_ids = pk.add(m.info_dep_start), o_idi = pk.add(m.info_dep_ids);
       const size_t o_js = pk.add(m.j_start), o_ji = pk.add(m.j_info), o_jc = pk.add(m.j_coef);
@@ -240,6 +241,9 @@ namespace micmb
       d.rate_scale = s.scale_dev.as<const double>();
       d.react_start = reinterpret_cast<const int32_t*>(b + o_rs);
       d.react_ids = reinterpret_cast<const int32_t*>(b + o_ri);
+      d.prod_start = reinterpret_cast<const int32_t*>(b + o_ps);
+      d.prod_ids = reinterpret_cast<const int32_t*>(b + o_pi);
+      d.prod_yield = reinterpret_cast<const double*>(b + o_py);
       d.f_start = reinterpret_cast<const int32_t*>(b + o_fs);
       d.f_rxn = reinterpret_cast<const int32_t*>(b + o_fr);
       d.f_coef = reinterpret_cast<const double*>(b + o_fc);
@@ -837,6 +841,60 @@ extern "C"
       }
       else
         SolvePlain(*solver, *state, dt, step_control, stats, per_cell_status, per_cell_accepted);
+    });
+  }
+
+  int micmb_solve_adjoint(micmb_solver* solver, micmb_state* state, double dt, const double* dloss_dy_final,
+                          double* dloss_dy0, double* dloss_dlogk, int32_t max_checkpoints,
+                          micmb_solver_stats* stats)
+  {
+    return Guard([&] {
+      Need(solver && state && state->solver == solver, "state does not belong to this solver");
+      Need(dloss_dy_final != nullptr, "dloss_dy_final is required");
+      Need(dt > 0 && std::isfinite(dt), "time step must be positive and finite");
+      Need(max_checkpoints >= 1, "max_checkpoints must be at least 1");
+      SetDevice(*solver);
+      micmb_state& st = *state;
+      const auto& m = *solver->mech;
+      const int64_t n = st.n_cells;
+      const size_t var_bytes = st.variables.bytes;
+      const int64_t ck = (int64_t)max_checkpoints * n * m.S;
+      if (!st.adj_y0.p || st.adj_y0.bytes < var_bytes)
+      {
+        st.adj_y0 = DeviceMemory(var_bytes);
+        st.adj_ybar = DeviceMemory(var_bytes);
+      }
+      if (!st.adj_ckpt_y.p || st.adj_ckpt_capacity < ck)
+      {
+        st.adj_ckpt_y = DeviceMemory(sizeof(double) * (size_t)std::max<int64_t>(ck, 1));
+        st.adj_ckpt_h = DeviceMemory(sizeof(double) * (size_t)std::max<int64_t>((int64_t)max_checkpoints * n, 1));
+        st.adj_ckpt_capacity = ck;
+      }
+      if (!st.adj_kbar_cells.p || st.adj_kbar_cells.bytes < sizeof(double) * (size_t)std::max<int64_t>(n * m.R, 1))
+      {
+        st.adj_kbar_cells = DeviceMemory(sizeof(double) * (size_t)std::max<int64_t>(n * m.R, 1));
+        st.adj_kbar = DeviceMemory(sizeof(double) * (size_t)std::max<int32_t>(m.R, 1));
+      }
+      MICMB_CUDA(cudaMemcpyAsync(st.adj_y0.p, st.variables.p, var_bytes, cudaMemcpyDeviceToDevice, st.stream));
+      MICMB_CUDA(cudaMemcpyAsync(st.adj_ybar.p, dloss_dy_final, var_bytes, cudaMemcpyHostToDevice, st.stream));
+      FusedArgs adj{};
+      adj.variables_in = st.variables.as<double>();
+      adj.variables_out = st.variables.as<double>();
+      adj.ckpt_y = st.adj_ckpt_y.as<double>();
+      adj.ckpt_h = st.adj_ckpt_h.as<double>();
+      adj.max_ckpt = max_checkpoints;
+      SolveFused(*solver, st, dt, stats, nullptr, nullptr, &adj);
+      LaunchAdjoint(*solver, st, max_checkpoints);
+      if (dloss_dy0)
+        MICMB_CUDA(cudaMemcpyAsync(dloss_dy0, st.adj_ybar.p, var_bytes, cudaMemcpyDeviceToHost, st.stream));
+      std::vector<double> kcol(std::max<int32_t>(m.R, 1));
+      if (dloss_dlogk && m.R > 0)
+        MICMB_CUDA(cudaMemcpyAsync(kcol.data(), st.adj_kbar.p, sizeof(double) * m.R, cudaMemcpyDeviceToHost,
+                                   st.stream));
+      MICMB_CUDA(cudaStreamSynchronize(st.stream));
+      if (dloss_dlogk)
+        for (int32_t r = 0; r < m.R; ++r)
+          dloss_dlogk[r] = kcol[m.reaction_column[r]];
     });
   }
 

@@ -54,9 +54,12 @@ namespace micmb
     const int32_t* rate_n_mult;
     const double* rate_mult;   // [R][MICMB_MAX_PARAMETERIZED][4]
     const double* rate_scale;  // [R] multiplicative scale (1.0 by default)
-    // reactants by rate column
+    // reactants and products by rate column
     const int32_t* react_start;
     const int32_t* react_ids;
+    const int32_t* prod_start;
+    const int32_t* prod_ids;
+    const double* prod_yield;
     // forcing gather by species
     const int32_t* f_start;
     const int32_t* f_rxn;

@@ -11,9 +11,4 @@ extern "C"
   {
     return MICMB_ERR_UNSUPPORTED;
   }
-  int micmb_solve_adjoint(micmb_solver*, micmb_state*, double, const double*, double*, double*, int32_t,
-                          micmb_solver_stats*)
-  {
-    return MICMB_ERR_UNSUPPORTED;
-  }
 }

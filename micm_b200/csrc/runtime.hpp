@@ -122,6 +122,9 @@ struct micmb_state
   micmb::DeviceMemory lu_slots;
   int64_t lu_slot_count = 0;  // doubles allocated in lu_slots
   micmb::DeviceMemory attempt_order;  // streamed kernel: block order of one attempt
+  // adjoint working set (allocated on first use)
+  micmb::DeviceMemory adj_y0, adj_ybar, adj_ckpt_y, adj_ckpt_h, adj_kbar_cells, adj_kbar;
+  int64_t adj_ckpt_capacity = 0;  // doubles in adj_ckpt_y
   double dt_for_launch = 0.0;
 
   size_t dense_bytes(int32_t ncols) const
@@ -150,5 +153,7 @@ namespace micmb
   // streamed warp-specialised variant; returns false when it does not apply
   bool SolveFusedStream(micmb_solver& s, micmb_state& st, double dt, const FusedArgs& A);
   int StreamWarpsPerCta(const micmb_solver& s, int slots, int cap, bool lu_shared);
+  // discrete adjoint sweep over the checkpoints of a fused solve
+  void LaunchAdjoint(micmb_solver& s, micmb_state& st, int32_t max_ckpt);
   int FusedWarpsPerCta(const micmb_solver& s, const micmb_fused_config& cfg);
 }  // namespace micmb

@@ -221,6 +221,9 @@ def _load_oracle():
                                           _f64p, _i64p, C.c_int]
         lib.om_adjoint_per_cell.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, _f64p, _f64p,
                                             C.c_double, _f64p, _f64p, _f64p, _f64p, _f64p, C.c_int, C.c_int]
+        lib.om_replay_per_cell.argtypes = [C.c_void_p, C.c_void_p, C.c_int, _f64p, _f64p, _i32p, C.c_int, _f64p]
+        lib.om_step_sizes_per_cell.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, _f64p, _f64p,
+                                               C.c_double, _f64p, C.c_int, _f64p, _i32p]
         _om = lib
     return _om
 
@@ -292,6 +295,29 @@ class Restatement:
         if rc:
             raise RuntimeError(self.lib.om_last_error().decode())
         return np.ascontiguousarray(y[:, self.species_columns]), stats
+
+    def step_sizes_per_cell(self, inputs, dt, max_steps=512, k=None):
+        """Accepted step sizes of each cell's solve: (h [n, max_steps], n_steps [n])."""
+        n = len(inputs["temperature"])
+        y0 = np.zeros((n, self.S))
+        y0[:, self.species_columns] = inputs["concentrations"]
+        k = self._k(inputs) if k is None else np.ascontiguousarray(k)
+        h = np.zeros((n, max_steps))
+        steps = np.zeros(n, np.int32)
+        self.lib.om_step_sizes_per_cell(self.handle, C.byref(self.params), n, float(dt), _p(k),
+                                        _p(self.atol_columns), self.mech.relative_tolerance, _p(y0), int(max_steps),
+                                        _p(h), _p(steps, C.c_int32))
+        return h, steps
+
+    def replay_per_cell(self, y0_sys, k, h, n_steps):
+        """y0 (system order) advanced by the given accepted step sizes, no error
+        control, final clamp: the map the discrete adjoint differentiates."""
+        y = np.zeros((len(y0_sys), self.S))
+        y[:, self.species_columns] = y0_sys
+        h = np.ascontiguousarray(h, np.float64)
+        self.lib.om_replay_per_cell(self.handle, C.byref(self.params), len(y), _p(np.ascontiguousarray(k)), _p(h),
+                                    _p(np.ascontiguousarray(n_steps, np.int32), C.c_int32), h.shape[1], _p(y))
+        return np.ascontiguousarray(y[:, self.species_columns])
 
     def adjoint_per_cell(self, inputs, dt, ybar_final_sys, threads=0, max_steps=512, k=None):
         """Returns (y_final, dL/dy0, dL/dlogk [n, R input order]) in system order."""

@@ -1021,6 +1021,92 @@ int om_solve_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n,
   return run(&j, n_threads);
 }
 
+/* One Rosenbrock step of size H from Y (no error estimate), Y <- Y + sum m_s K_s;
+ * the stage recurrences of adjoint_cell's recomputation. */
+static void fixed_step(const om_mech* m, const micmb_rosenbrock_params* p, const double* k, double H, double* Y,
+                       work_t* w)
+{
+  const int S = m->S, ns = p->stages;
+  double* Ys = w->scratch;
+  forcing(m, k, Y, w->F0);
+  neg_jacobian(m, k, Y, w->J);
+  const double alpha = 1.0 / (H * p->gamma[0]);
+  for (int i = 0; i < S; ++i)
+    w->J[m->pos[(size_t)i * S + i]] += alpha;
+  decompose(m, w->J);
+  for (int s = 0; s < ns; ++s)
+  {
+    const int sc = s * (s - 1) / 2;
+    double* Ks = w->K + (size_t)s * S;
+    if (s == 0)
+      memcpy(Ks, w->F0, sizeof(double) * S);
+    else if (p->new_function_evaluation[s])
+    {
+      memcpy(Ys, Y, sizeof(double) * S);
+      for (int j = 0; j < s; ++j)
+        for (int i = 0; i < S; ++i)
+          Ys[i] += p->a[sc + j] * w->K[(size_t)j * S + i];
+      forcing(m, k, Ys, Ks);
+    }
+    if (s + 1 < ns && !p->new_function_evaluation[s + 1])
+      memcpy(w->K + (size_t)(s + 1) * S, Ks, sizeof(double) * S);
+    for (int j = 0; j < s; ++j)
+    {
+      double coh = p->c[sc + j] / H;
+      for (int i = 0; i < S; ++i)
+        Ks[i] += coh * w->K[(size_t)j * S + i];
+    }
+    lu_solve(m, w->J, Ks);
+  }
+  for (int i = 0; i < S; ++i)
+  {
+    double v = Y[i];
+    for (int s = 0; s < ns; ++s)
+      v += p->m[s] * w->K[(size_t)s * S + i];
+    Y[i] = v;
+  }
+}
+
+int om_replay_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n, const double* k, const double* h,
+                       const int32_t* n_steps, int max_steps, double* y)
+{
+  const int S = m->S;
+  work_t w;
+  work_alloc(&w, m, p->stages);
+  for (int c = 0; c < n; ++c)
+  {
+    double* Y = y + (size_t)c * S;
+    for (int q = 0; q < n_steps[c] && q < max_steps; ++q)
+      fixed_step(m, p, k + (size_t)c * m->R, h[(size_t)c * max_steps + q], Y, &w);
+    for (int i = 0; i < S; ++i)
+      Y[i] = Y[i] < 0.0 ? 0.0 : Y[i];
+  }
+  work_free(&w);
+  return 0;
+}
+
+/* accepted step sizes of a per-cell solve: h [cell][max_steps], n_steps [cell] */
+int om_step_sizes_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n, double dt, const double* k,
+                           const double* atol, double rtol, const double* y0, int max_steps, double* h,
+                           int32_t* n_steps)
+{
+  const int S = m->S;
+  work_t w;
+  work_alloc(&w, m, p->stages);
+  double* ck_y = xcalloc((size_t)max_steps * S, sizeof(double));
+  for (int c = 0; c < n; ++c)
+  {
+    int nck = 0;
+    memcpy(w.Y, y0 + (size_t)c * S, sizeof(double) * S);
+    rosenbrock_cell(m, p, dt, k + (size_t)c * m->R, atol, rtol, &w, NULL, ck_y, h + (size_t)c * max_steps, max_steps,
+                    &nck);
+    n_steps[c] = nck;
+  }
+  free(ck_y);
+  work_free(&w);
+  return 0;
+}
+
 int om_adjoint_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n, double dt, const double* k,
                         const double* atol, double rtol, const double* y0, const double* ybar_final,
                         double* y_final, double* ybar0, double* kbar, int max_steps_stored, int n_threads)

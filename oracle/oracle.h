@@ -56,6 +56,16 @@ int om_adjoint_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int 
                         const double* atol, double rtol, const double* y0, const double* ybar_final,
                         double* y_final, double* ybar0, double* kbar, int max_steps_stored, int n_threads);
 
+/* Fixed-step replay of given step sizes (no error control), final clamp as the
+ * solve: the map whose derivative om_adjoint_per_cell computes.  For finite-
+ * difference checks.  h [cell][max_steps], n_steps [cell], y [cell][S] in/out. */
+int om_replay_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n, const double* k, const double* h,
+                       const int32_t* n_steps, int max_steps, double* y);
+/* Accepted step sizes of a per-cell solve from y0 [cell][S]. */
+int om_step_sizes_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n, double dt, const double* k,
+                           const double* atol, double rtol, const double* y0, int max_steps, double* h,
+                           int32_t* n_steps);
+
 #ifdef __cplusplus
 }
 #endif
