@@ -944,6 +944,23 @@ namespace micm
       return Solve(time_step, state);
     }
 
+    // Autotuner (no micm counterpart): time the fused-kernel configurations on
+    // this state, keep the fastest for later fused solves; cached by mechanism
+    // hash in `cache_path` when given.
+    void Autotune(Real time_step, CudaState<L>& state, const char* cache_path = nullptr)
+    {
+      micmb_fused_config chosen{};
+      detail::Check(micmb_autotune(solver_.get(), state.handle_.get(), time_step, cache_path, &chosen));
+    }
+
+    // n_repeats x (UpdateStateParameters + fused Solve) replayed from one CUDA
+    // graph (no micm counterpart); conditions and custom parameters are read
+    // from the device copies the last UpdateStateParameters uploaded.
+    void SolveRepeated(Real time_step, CudaState<L>& state, int32_t n_repeats)
+    {
+      detail::Check(micmb_solve_graph(solver_.get(), state.handle_.get(), time_step, n_repeats));
+    }
+
     // Discrete adjoint of the accepted steps of a per-cell solve (no micm
     // counterpart).  dloss_dy_final and dloss_dy0 are [cell][variable] in the
     // state's VectorMatrix layout; dloss_dlogk is per reaction in input order.

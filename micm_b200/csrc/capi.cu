@@ -754,6 +754,8 @@ extern "C"
       cudaStreamSynchronize(state->stream);
     if (state->host_counters)
       cudaFreeHost(state->host_counters);
+    if (state->graph_exec)
+      cudaGraphExecDestroy(state->graph_exec);
     if (state->own_stream)
       cudaStreamDestroy(state->own_stream);
     delete state;

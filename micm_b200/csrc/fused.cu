@@ -288,7 +288,7 @@ namespace micmb
     if (cfg.ctas_per_sm > 0)
       per_sm = std::min(per_sm, cfg.ctas_per_sm);
     int64_t grid = (int64_t)per_sm * s.sm_count;
-    const int64_t n = st.n_cells;
+    const int64_t n = st.solve_limit > 0 ? std::min<int64_t>(st.solve_limit, st.n_cells) : st.n_cells;
     grid = std::max<int64_t>(1, std::min<int64_t>(grid, (n + warps - 1) / warps));
 
     FusedArgs A{};

@@ -529,10 +529,16 @@ namespace micmb
       add(m.stream.fwd);
       add(m.stream.bwd);
     }
-    if (st.attempt_order.bytes < order.size() * sizeof(int32_t))
-      st.attempt_order = DeviceMemory(order.size() * sizeof(int32_t));
-    MICMB_CUDA(cudaMemcpyAsync(st.attempt_order.p, order.data(), order.size() * sizeof(int32_t),
-                               cudaMemcpyHostToDevice, st.stream));
+    if (order != st.attempt_order_host)
+    {
+      // uploaded once per tableau, so repeated launches (and graph captures) copy nothing
+      MICMB_CUDA(cudaStreamSynchronize(st.stream));  // no earlier launch still reads the old order
+      if (st.attempt_order.bytes < order.size() * sizeof(int32_t))
+        st.attempt_order = DeviceMemory(order.size() * sizeof(int32_t));
+      MICMB_CUDA(cudaMemcpy(st.attempt_order.p, order.data(), order.size() * sizeof(int32_t),
+                            cudaMemcpyHostToDevice));
+      st.attempt_order_host = order;
+    }
     StreamArgs SA{};
     SA.blocks = s.stream_blocks.as<const uint8_t>();
     SA.block_bytes = s.stream_block_bytes.as<const int32_t>();
@@ -548,7 +554,7 @@ namespace micmb
     SA.coef = s.stream_coef.as<const double>();
     SA.n_coef = s.n_stream_coef;
     int64_t grid = (int64_t)s.sm_count * (s.fused.ctas_per_sm > 0 ? s.fused.ctas_per_sm : 1);
-    grid = std::max<int64_t>(1, std::min<int64_t>(grid, (st.n_cells + W - 1) / W));
+    grid = std::max<int64_t>(1, std::min<int64_t>(grid, (A_in.n_cells + W - 1) / W));
     FusedArgs A = A_in;
     if (!lu_shared)
     {

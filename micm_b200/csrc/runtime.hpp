@@ -122,6 +122,12 @@ struct micmb_state
   micmb::DeviceMemory lu_slots;
   int64_t lu_slot_count = 0;  // doubles allocated in lu_slots
   micmb::DeviceMemory attempt_order;  // streamed kernel: block order of one attempt
+  std::vector<int32_t> attempt_order_host;  // what attempt_order holds
+  int64_t solve_limit = 0;                  // fused solves: only the first solve_limit cells (0 = all)
+  // CUDA graph of UpdateStateParameters + fused Solve (micmb_solve_graph)
+  cudaGraphExec_t graph_exec = nullptr;
+  double graph_dt = 0.0;
+  micmb_fused_config graph_config{};
   // adjoint working set (allocated on first use)
   micmb::DeviceMemory adj_y0, adj_ybar, adj_ckpt_y, adj_ckpt_h, adj_kbar_cells, adj_kbar;
   int64_t adj_ckpt_capacity = 0;  // doubles in adj_ckpt_y
@@ -135,6 +141,7 @@ struct micmb_state
 
 namespace micmb
 {
+  extern thread_local std::string g_last_error;  // micmb_last_error()
   void EnsurePlainBuffers(micmb_state& st);
   // plain path: one kernel per stage; returns after the whole solve
   void SolvePlain(micmb_solver& s, micmb_state& st, double dt, int32_t step_control, micmb_solver_stats* stats,

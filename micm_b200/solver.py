@@ -188,6 +188,17 @@ class Solver:
         return SolverResult(stats.state, stats.as_dict(), pst[:n] if per_cell else None,
                             pac[:n] if per_cell else None)
 
+    def autotune(self, dt: float, state: "State", cache_path: Optional[str] = None) -> Dict[str, int]:
+        """Time the fused configurations on this state and keep the fastest."""
+        cfg = FusedConfig()
+        check(lib().micmb_autotune(self.handle, state.handle, float(dt),
+                                   cache_path.encode() if cache_path else None, C.byref(cfg)))
+        return self.get_fused_config()
+
+    def solve_graph(self, dt: float, state: "State", n_repeats: int):
+        """n_repeats x (update_state_parameters + fused per-cell solve) from one CUDA graph."""
+        check(lib().micmb_solve_graph(self.handle, state.handle, float(dt), int(n_repeats)))
+
     def solve_adjoint(self, dt: float, state: "State", dloss_dy_final: np.ndarray, max_checkpoints: int = 256):
         """Returns (dL/dy0 [n, S] state columns, dL/dlog k [R] input order, SolverResult)."""
         n, S, L = state.n_cells, self.mech.n_species, state.L

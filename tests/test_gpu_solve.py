@@ -133,3 +133,4 @@ def test_fused_tiny_and_ragged(cuda_device):
         y, res = solve_gpu(m, inp, 3600.0, 4, "fused", "per_cell", L=8)
         _close(y, y_ref)
         np.testing.assert_array_equal(res[0].per_cell_accepted, st_ref[:, 3])
+
