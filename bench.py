@@ -35,13 +35,14 @@ CONFIG_NAME = "c210_uneven"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cells", type=int, default=1048576)
-    ap.add_argument("--plain-cells", type=int, default=262144,
-                    help="cells for the plain-method comparison line (0 = skip)")
-    ap.add_argument("--cpu-sample", type=int, default=4096, help="cells timed on the host CPU")
+    ap.add_argument("--plain-cells", type=int, default=1048576,
+                    help="cells per GPU for the plain-method comparison (0 = skip)")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing")
+    ap.add_argument("--cpu-sample", type=int, default=65536, help="cells timed on the host CPU")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
 
@@ -153,11 +154,96 @@ def run_reference_arm(args):
     print(json.dumps(line))
 
 
+def flops_per_solve_unit(mech, solver, stages):
+    """Algorithmic FP64 operations of one unit of each kind of work (the
+    operations the exact-order formulation performs; padding excluded)."""
+    info = solver.compiled.info
+    st = solver.compiled.stream_stats()
+    S = mech.n_species
+    react = [sum(1 for x in r.reactants if x >= 0) for r in mech.reactions]
+    f_force = sum(react) + 2 * info["n_forcing_terms"]                 # w_r products, sum of nu w
+    f_jac = sum(n * (n - 1) for n in react) + 2 * info["n_jacobian_terms"] + S   # dw products, sum, alpha
+    f_lu = 2 * info["lu_updates"] + info["lu_lower"] + S                 # updates, pivot scalings, 1/a_kk
+    f_solve = 2 * (st["forward"]["terms"] + st["backward"]["terms"]) + S  # both sweeps, diagonal divides
+    f_attempt = 2 * S * (stages * (stages - 1) // 2) * 2 + 4 * S * stages + 6 * S  # stage sums, m/e sums, norm
+    return dict(force=f_force, jac=f_jac, lu=f_lu, solve=f_solve, attempt=f_attempt)
+
+
+def solve_flops(units, stats):
+    return (stats["function_calls"] * units["force"] + stats["jacobian_updates"] * units["jac"]
+            + stats["decompositions"] * units["lu"] + stats["solves"] * units["solve"]
+            + stats["number_of_steps"] * units["attempt"])
+
+
+def fp64_peak():
+    """Nominal dense FP64 rate of the device: SMs x 64 FMA/clock x 2 x max SM clock
+    (no FP64 figure is measured by the pool's peak probe)."""
+    import torch
+    p = torch.cuda.get_device_properties(torch.cuda.current_device())
+    mhz = 1965.0
+    try:
+        out = subprocess.run(["nvidia-smi", "--query-gpu=clocks.max.sm", "--format=csv,noheader,nounits",
+                              f"--id={torch.cuda.current_device()}"], capture_output=True, text=True, timeout=20)
+        mhz = float(out.stdout.strip().splitlines()[0])
+    except Exception:
+        pass
+    return p.multi_processor_count * 64 * 2 * mhz * 1e6 / 1e12
+
+
+def adjoint_ratio(torch, rank):
+    """Adjoint/forward time on the adjoint configuration (60 species, 131,072 cells)."""
+    from micm_b200 import Solver, synthetic
+    cfg = synthetic.CONFIGS["c60_adjoint"]
+    mech = cfg["mech"]()
+    n = cfg["cells"]
+    inputs = synthetic.cell_inputs(mech, n, cfg["seed"] + 1000 * rank, **cfg["inputs"])
+    solver = Solver(mech, cfg["stages"], vector_length=128)
+    st = solver.get_state(n)
+    st.set_inputs(inputs)
+    rng = np.random.default_rng(cfg["seed"])
+    target = rng.random(n) * 1e-9
+    cols = solver.compiled.species_columns
+
+    def forward():
+        st.sync_inputs_to_device()
+        solver.update_state_parameters(st)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = solver.solve(cfg["dt"], st, method="fused", step_control="per_cell")
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, r
+
+    def adjoint(y_final):
+        g = np.zeros((n, mech.n_species))
+        g[:, cols[0]] = 2.0 * (y_final[:, cols[0]] - target)
+        st.sync_inputs_to_device()
+        solver.update_state_parameters(st)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        solver.solve_adjoint(cfg["dt"], st, g, max_checkpoints=256)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+    forward()
+    tf, res = forward()
+    st.sync_outputs_to_host()
+    y_final = st.variables.copy()
+    st.set_inputs(inputs)
+    adjoint(y_final)
+    ta = adjoint(y_final)
+    return {"config": "c60_adjoint: 60 species, 120 reactions, 131,072 cells, 4-stage, dt=3600 s; "
+                      "loss = sum_c (y_c[0] - target_c)^2; gradients w.r.t. all y0 and all log k",
+            "forward_ms": 1000 * tf, "adjoint_ms": 1000 * ta, "adjoint_over_forward": ta / tf,
+            "accepted_per_cell": res.stats["accepted"] / n,
+            "note": "adjoint time = forward solve with checkpoints + reverse sweep, host gradient copies included"}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference_arm(args)
         return
+    import ctypes
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -170,7 +256,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     from micm_b200 import Solver
     from micm_b200 import solver as sv
-    from micm_b200.mechanism import to_vector_layout, padded_cells
+    from micm_b200._native import check, lib
+    from micm_b200.mechanism import to_vector_layout
 
     cfg, mech, inputs = workload(args.cells, rank)
     L = 128
@@ -179,57 +266,68 @@ def main():
     state.set_inputs(inputs)
     state.sync_inputs_to_device()
     solver.update_state_parameters(state)
-    S = mech.n_species
-    npad = padded_cells(args.cells, L)
+    tuned = solver.autotune(cfg["dt"], state)                  # cells-per-CTA, LU staging, ring depth, variant
+    stream = torch.cuda.current_stream()
+    check(lib().micmb_state_set_stream(state.handle, ctypes.c_void_p(stream.cuda_stream)))
     y0_host = to_vector_layout(state.variables, L)
     y_dev = torch.from_numpy(y0_host).cuda()
-    y_view = device_view(state, sv.BUF_VARIABLES)   # torch view of the state's own buffer
-    stream = torch.cuda.current_stream()
-    import ctypes
-    from micm_b200._native import check, lib
-    check(lib().micmb_state_set_stream(state.handle, ctypes.c_void_p(stream.cuda_stream)))
+    y_view = device_view(state, sv.BUF_VARIABLES)             # torch view of the state's own buffer
 
-    def restore_torch():
-        y_view.copy_(y_dev)
+    def fused_step():
+        y_view.copy_(y_dev)                                    # the step's inputs, already in HBM
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = solver.solve(cfg["dt"], state, method="fused", step_control="per_cell")
+        e1.record(stream)
+        return r, e0, e1
 
-    warm = args.warmup
-    # warmup
-    for _ in range(warm):
-        restore_torch()
-        res = solver.solve(cfg["dt"], state, method="fused", step_control="per_cell")
+    for _ in range(args.warmup):
+        fused_step()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
+    totals = {}
+    kernel_ms = 0.0
     with ClockSampler(local) as clocks:
         torch.cuda.synchronize()
         start.record(stream)
-        stats_sum = None
+        events = []
         for _ in range(args.steps):
-            restore_torch()
-            res = solver.solve(cfg["dt"], state, method="fused", step_control="per_cell")
-            stats_sum = res.stats
+            r, e0, e1 = fused_step()
+            events.append((e0, e1))
+            for key, v in r.stats.items():
+                if isinstance(v, (int, float)):
+                    totals[key] = totals.get(key, 0) + v
         end.record(stream)
         torch.cuda.synchronize()
     ms = start.elapsed_time(end)
+    kernel_ms = sum(a.elapsed_time(b) for a, b in events)
     if dist:
-        t = torch.tensor([ms], device="cuda")
+        t = torch.tensor([ms, kernel_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms, kernel_ms = float(t[0].item()), float(t[1].item())
     value = args.cells * world * args.steps / (ms / 1000.0)
-    attempts_per_cell = stats_sum["number_of_steps"] / args.cells
-    accepted_per_cell = stats_sum["accepted"] / args.cells
+    attempts_per_cell = totals["number_of_steps"] / (args.cells * args.steps)
+    accepted_per_cell = totals["accepted"] / (args.cells * args.steps)
 
-    # e2e: public API with host buffers every step
-    import torch as _t
-    h_vars = _t.from_numpy(y0_host).pin_memory().numpy()
+    # roofline of the fused kernel: FP64 work of the accepted and rejected attempts
+    units = flops_per_solve_unit(mech, solver, cfg["stages"])
+    flops = solve_flops(units, totals) / args.steps            # per launch (one Solve over the shard)
+    achieved = flops / (kernel_ms / args.steps / 1000.0) / 1e12
+    peak = fp64_peak()
+
+    # e2e: the public API with host buffers every step (H2D inputs, D2H results)
+    h_vars = torch.from_numpy(y0_host).pin_memory().numpy()
     cond = np.stack([state.temperature, state.pressure, state.air_density], axis=1)
-    h_cond = _t.from_numpy(to_vector_layout(cond, L)).pin_memory().numpy()
-    h_par = _t.from_numpy(to_vector_layout(state.custom_rate_parameters, L)).pin_memory().numpy()
-    h_out = _t.empty(h_vars.shape[0], dtype=_t.float64).pin_memory().numpy()
+    h_cond = torch.from_numpy(to_vector_layout(cond, L)).pin_memory().numpy()
+    h_par = torch.from_numpy(to_vector_layout(state.custom_rate_parameters, L)).pin_memory().numpy()
+    h_out = torch.empty(h_vars.shape[0], dtype=torch.float64).pin_memory().numpy()
     e2e_steps = max(1, min(args.steps, 2))
-    _t.cuda.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         state.upload(sv.BUF_VARIABLES, h_vars)
@@ -239,27 +337,41 @@ def main():
         solver.solve(cfg["dt"], state, method="fused", step_control="per_cell")
         check(lib().micmb_state_download(state.handle, sv.BUF_VARIABLES,
                                          h_out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+    torch.cuda.synchronize()
     e2e_t = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_t], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
     h2d = h_vars.nbytes + h_cond.nbytes + h_par.nbytes
     d2h = h_out.nbytes
 
-    # plain method on a subset (per-stage kernels), for the fused-vs-plain ratio
+    # plain per-stage kernels on the same shard (one warm-up, one timed solve)
     plain = None
-    if args.plain_cells and rank == 0:
+    if args.plain_cells:
         pc = min(args.plain_cells, args.cells)
-        _, _, pin = workload(pc, rank)
-        pstate = solver.get_state(pc)
-        pstate.set_inputs(pin)
-        pstate.sync_inputs_to_device()
+        y_view.copy_(y_dev)
+        pstate = state if pc == args.cells else None
+        if pstate is None:
+            _, _, pin = workload(pc, rank)
+            pstate = solver.get_state(pc)
+            pstate.set_inputs(pin)
+            pstate.sync_inputs_to_device()
         solver.update_state_parameters(pstate)
-        _t.cuda.synchronize()
+        pview = device_view(pstate, sv.BUF_VARIABLES)
+        p0 = pview.clone()
+        solver.solve(cfg["dt"], pstate, method="plain", step_control="per_cell")
+        pview.copy_(p0)
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
         pres = solver.solve(cfg["dt"], pstate, method="plain", step_control="per_cell")
-        _t.cuda.synchronize()
+        torch.cuda.synchronize()
         pt = time.perf_counter() - t0
-        plain = {"value": pc / pt, "unit": UNIT, "cells": pc, "ms": 1000 * pt,
-                 "attempts_per_cell": pres.stats["number_of_steps"] / pc}
-        del pstate
+        plain = {"value": pc * world / pt, "unit": UNIT, "cells_per_gpu": pc, "ms_per_step": 1000 * pt,
+                 "attempts_per_cell": pres.stats["number_of_steps"] / pc,
+                 "fused_over_plain": value / (pc * world / pt)}
+
+    adj = adjoint_ratio(torch, rank) if not args.no_adjoint else None
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -274,14 +386,24 @@ def main():
             "config": {"workload": f"{CONFIG_NAME}: 210 species, 440 reactions, {args.cells} cells per GPU, "
                                    "half night, T~U(200,310) K, 4-stage Rosenbrock, dt=600 s, per-cell step control, "
                                    "fused persistent kernel",
-                       "cells_per_gpu": args.cells, "vector_length": L, "l2": "inputs exceed L2 (5.5 GB)",
+                       "cells_per_gpu": args.cells, "vector_length": L, "fused_config": tuned,
+                       "l2": "inputs exceed L2 (1.8 GB state + 3.7 GB rate constants); no flush",
                        "lu_nnz": info["jacobian_nnz"], "lu_updates": info["lu_updates"],
                        "attempts_per_cell": attempts_per_cell, "accepted_per_cell": accepted_per_cell},
             "clocks": clocks.summary(),
-            "e2e": {"value": args.cells * e2e_steps / e2e_t, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+            "e2e": {"value": args.cells * world * e2e_steps / e2e_t, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "calls": "upload variables/conditions/custom params, UpdateStateParameters, Solve, "
+                             "download variables (pinned host buffers)"},
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "k_fused_stream (one launch per step)",
+                         "flops_per_launch": flops, "kernel_ms_per_launch": kernel_ms / args.steps,
+                         "peak_source": "nominal FP64 (SMs x 64 FMA/clk x 2 x max SM clock); "
+                                        "MEASURED_PEAKS.json has no FP64 entry"},
             "gpu_launches": args.steps,
             "plain": plain,
+            "adjoint": adj,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))

@@ -284,7 +284,8 @@ typedef struct micmb_fused_config {
   int32_t lu_in_shared;    /* 1 LU factor in shared memory, 0 in a per-warp global (L2) slot */
   int32_t ctas_per_sm;     /* persistent grid = ctas_per_sm * SM count (0 = occupancy) */
   int32_t ring_slots;      /* streamed variant: shared-memory slots for table blocks (0 = 4) */
-  int32_t variant;         /* 0 streamed (TMA-fed, warp-specialised), 1 direct */
+  int32_t variant;         /* 0 streamed (TMA-fed, warp-specialised), 1 direct (warp per cell),
+                              2 one cell per thread (working sets in global memory) */
 } micmb_fused_config;
 int micmb_solver_set_fused_config(micmb_solver* solver, const micmb_fused_config* config);
 int micmb_solver_get_fused_config(micmb_solver* solver, micmb_fused_config* config);

@@ -196,6 +196,8 @@ namespace micmb
       const size_t o_dp = pk.add(m.diag_pos), o_dro = pk.add(diag_row_of);
       const SchedOffsets lu = AddSchedule(pk, m.lu), fw = AddSchedule(pk, m.fwd), bw = AddSchedule(pk, m.bwd),
                          fwt = AddSchedule(pk, m.fwd_t), bwt = AddSchedule(pk, m.bwd_t);
+      const SchedOffsets lus = AddSchedule(pk, m.lu_serial), fws = AddSchedule(pk, m.fwd_serial),
+                         bws = AddSchedule(pk, m.bwd_serial);
       const size_t o_rd = pk.add(m.rate_desc), o_drd = pk.add(m.drate_desc);
       WarpOffsets wl{}, wf{}, wb{}, wft{}, wbt{}, wfo{}, wj{};
       if (m.has_warp_tables)
@@ -260,6 +262,9 @@ namespace micmb
       d.bwd = Resolve(b, bw);
       d.fwd_t = Resolve(b, fwt);
       d.bwd_t = Resolve(b, bwt);
+      d.lu_s = Resolve(b, lus);
+      d.fwd_s = Resolve(b, fws);
+      d.bwd_s = Resolve(b, bws);
       s.diag_row_of = d.diag_row_of;
       d.has_warp = m.has_warp_tables ? 1 : 0;
       d.scratch_zero = m.scratch_zero;
@@ -698,7 +703,8 @@ extern "C"
       Need(solver && config, "null argument");
       Need(config->cells_per_cta >= 0 && config->cells_per_cta <= 12, "cells_per_cta must be 0..12");
       Need(config->ring_slots >= 0 && config->ring_slots <= 8, "ring_slots must be 0..8");
-      Need(config->variant == 0 || config->variant == 1, "variant must be 0 (streamed) or 1 (direct)");
+      Need(config->variant >= 0 && config->variant <= 2,
+           "variant must be 0 (streamed), 1 (direct) or 2 (one cell per thread)");
       solver->fused = *config;
     });
   }

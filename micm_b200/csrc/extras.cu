@@ -130,22 +130,28 @@ extern "C"
         { 0, 0, 0, 2, 0 }, { 0, 0, 0, 4, 0 },  // streamed, LU in global slots, as many cells as fit
         { 6, 0, 0, 4, 0 }, { 4, 0, 0, 4, 0 },  // streamed, fewer cells per CTA
         { 0, 1, 0, 0, 1 }, { 0, 0, 0, 0, 1 },  // direct
+        { 0, 0, 0, 0, 2 }, { 0, 0, 4, 0, 2 },  // one cell per thread (full and limited occupancy)
       };
-      // tune on enough cells to fill every SM a few times over
-      const int64_t trial = std::min<int64_t>(st.n_cells, (int64_t)solver->sm_count * 12 * 8);
+      // tune each candidate on enough cells to fill every SM a few times over:
+      // a few warps per SM for the warp-per-cell variants, up to 1024 threads
+      // per SM for the thread-per-cell variant; compare cells per second
+      auto trial_cells = [&](const micmb_fused_config& c) {
+        const int64_t per_sm = c.variant == 2 ? 2 * 1024 : 12 * 8;
+        return std::min<int64_t>(st.n_cells, (int64_t)solver->sm_count * per_sm);
+      };
       DeviceMemory saved(st.variables.bytes);
       MICMB_CUDA(cudaMemcpyAsync(saved.p, st.variables.p, st.variables.bytes, cudaMemcpyDeviceToDevice, st.stream));
       cudaEvent_t e0, e1;
       MICMB_CUDA(cudaEventCreate(&e0));
       MICMB_CUDA(cudaEventCreate(&e1));
       const micmb_fused_config before = solver->fused;
-      float best_ms = -1.0f;
-      st.solve_limit = trial;
+      double best_rate = -1.0;
       try
       {
         for (const auto& c : candidates)
         {
           solver->fused = c;
+          st.solve_limit = trial_cells(c);
           float ms_min = -1.0f;
           for (int rep = 0; rep < 2; ++rep)
           {
@@ -159,9 +165,10 @@ extern "C"
             MICMB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
             ms_min = (ms_min < 0.0f || ms < ms_min) ? ms : ms_min;
           }
-          if (best_ms < 0.0f || ms_min < best_ms)
+          const double rate = (double)st.solve_limit / std::max(ms_min, 1e-3f);
+          if (rate > best_rate)
           {
-            best_ms = ms_min;
+            best_rate = rate;
             best = c;
           }
         }

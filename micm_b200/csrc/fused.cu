@@ -307,12 +307,11 @@ namespace micmb
     char* cbase = st.counters.as<char>();
     A.next_cell = reinterpret_cast<int32_t*>(cbase + 8);
     A.stats = reinterpret_cast<unsigned long long*>(cbase + 64);
+    // per-cell outputs cover the whole state, whatever prefix this call solves
     if (!st.status.p)
-    {
-      st.status = DeviceMemory(sizeof(int32_t) * std::max<int64_t>(n, 1));
-    }
+      st.status = DeviceMemory(sizeof(int32_t) * std::max<int64_t>(st.n_cells, 1));
     if (!st.accepted.p)
-      st.accepted = DeviceMemory(sizeof(int32_t) * std::max<int64_t>(n, 1));
+      st.accepted = DeviceMemory(sizeof(int32_t) * std::max<int64_t>(st.n_cells, 1));
     A.cell_status = st.status.as<int32_t>();
     A.cell_accepted = st.accepted.as<int32_t>();
     if (!lu_shared)
@@ -333,6 +332,8 @@ namespace micmb
       bool done = false;
       if (s.fused.variant == 0)
         done = SolveFusedStream(s, st, dt, A);
+      else if (s.fused.variant == 2)
+        done = SolveFusedThread(s, st, A, dt);
       if (!done)
       {
         const StepBounds B = step_bounds(s.params, dt);

@@ -1,0 +1,284 @@
+// fused_thread.cu -- the persistent fused solve with one grid cell per thread.
+//
+// Every thread of a resident grid owns a private working set (state, stages,
+// rate constants, rates and the LU factor) in global memory, laid out so that
+// the 32 threads of a warp touch 32 consecutive doubles for the same entry:
+// every access of the sparse kernels is a full 256-byte line.  A warp runs
+// attempts in lockstep -- forcing (only where a step starts), -J, the LU in
+// micm's update order, the stages and the error norm -- so all its threads
+// follow the same instruction stream over the mechanism's tables, and a
+// thread whose cell finishes takes the next unsolved cell from a global atomic
+// counter between two attempts.  Per-cell results are bit-identical to the
+// plain per-stage kernels: the same routines in the same order.
+#include "runtime.hpp"
+
+#include <algorithm>
+
+namespace micmb
+{
+  namespace
+  {
+    constexpr int kThreadsPerBlock = 128;
+
+    __device__ __forceinline__ size_t cell_base(int64_t c, int32_t L, int32_t ncol)
+    {
+      return (size_t)(c / L) * (size_t)L * (size_t)ncol + (size_t)(c % L);
+    }
+
+    // entry offsets (each entry = 32 doubles, one per lane) of a thread's working set
+    struct ThreadLayout
+    {
+      int32_t oY, oYn, oF0, oFc, oK, oLU, oInv, oKk, oScr, per_slot;
+    };
+
+    ThreadLayout MakeThreadLayout(int32_t S, int32_t R, int32_t stages, int32_t n_info, int32_t nnz)
+    {
+      ThreadLayout t;
+      int32_t o = 0;
+      t.oY = o;
+      o += S;
+      t.oYn = o;
+      o += S;
+      t.oF0 = o;
+      o += S;
+      t.oFc = o;
+      o += S;
+      t.oK = o;
+      o += stages * S;
+      t.oLU = o;
+      o += nnz;
+      t.oInv = o;
+      o += S;
+      t.oKk = o;
+      o += R;
+      t.oScr = o;
+      o += (R > n_info ? R : n_info);
+      t.per_slot = o;
+      return t;
+    }
+
+    __device__ __forceinline__ void count_attempt(CellCtl& cc, const DevParams& P)
+    {
+      cc.decompositions += 1;
+      cc.solves += P.stages;
+      for (int32_t s = 1; s < P.stages; ++s)
+        cc.function_calls += P.new_f[s] ? 1 : 0;
+    }
+
+    __global__ void __launch_bounds__(kThreadsPerBlock)
+        k_fused_thread(DevMech M, DevParams P, StepBounds B, FusedArgs A, double* ws, ThreadLayout T)
+    {
+      const int lane = threadIdx.x & 31;
+      const int64_t wslot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+      double* w = ws + (size_t)wslot * (size_t)T.per_slot * 32 + lane;
+      const int32_t S = M.S, R = M.R, L = A.L;
+      Strided Y{ w + (size_t)T.oY * 32, 32 };
+      Strided Yn{ w + (size_t)T.oYn * 32, 32 };
+      Strided F0{ w + (size_t)T.oF0 * 32, 32 };
+      Strided Fc{ w + (size_t)T.oFc * 32, 32 };
+      double* Kb = w + (size_t)T.oK * 32;
+      Strided LU{ w + (size_t)T.oLU * 32, 32 };
+      Strided inv{ w + (size_t)T.oInv * 32, 32 };
+      Strided kk{ w + (size_t)T.oKk * 32, 32 };
+      Strided scr{ w + (size_t)T.oScr * 32, 32 };
+      auto Kv = [&](int32_t st) { return Strided{ Kb + (size_t)st * S * 32, 32 }; };
+
+      long long acc[8] = { 0 };
+      CellCtl c;
+      ctl_init(c, B);
+      int64_t cell = 0;
+      int32_t n_ckpt = 0;
+      bool have = false, need_f0 = false;
+
+      auto write_out = [&]() {
+        const size_t by = cell_base(cell, L, S);
+        for (int32_t i = 0; i < S; ++i)
+        {
+          const double v = Y[i];
+          A.variables_out[by + (size_t)i * L] = (v < 0.0) ? 0.0 : v;
+        }
+        if (A.cell_status)
+          A.cell_status[cell] = c.state;
+        if (A.cell_accepted)
+          A.cell_accepted[cell] = A.ckpt_y ? n_ckpt : c.accepted;
+        acc[0] += c.function_calls;
+        acc[1] += c.jacobian_updates;
+        acc[2] += c.number_of_steps;
+        acc[3] += c.accepted;
+        acc[4] += c.rejected;
+        acc[5] += c.decompositions;
+        acc[6] += c.solves;
+        acc[7] += (c.state == MICMB_SOLVER_CONVERGED) ? 0 : 1;
+      };
+      // take cells until one needs an attempt (or none are left)
+      auto claim = [&]() {
+        for (;;)
+        {
+          cell = atomicAdd(A.next_cell, 1);
+          if (cell >= A.n_cells)
+          {
+            have = false;
+            return;
+          }
+          const size_t by = cell_base(cell, L, S);
+          const size_t bk = cell_base(cell, L, R);
+          for (int32_t i = 0; i < S; ++i)
+            Y[i] = A.variables_in[by + (size_t)i * L];
+          for (int32_t r = 0; r < R; ++r)
+            kk[r] = A.rate_constants[bk + (size_t)r * L];
+          ctl_init(c, B);
+          n_ckpt = 0;
+          if (ctl_begin_step(c, P, B))
+          {
+            c.function_calls += 1;
+            c.jacobian_updates += 1;
+            need_f0 = true;
+            have = true;
+            return;
+          }
+          write_out();
+        }
+      };
+
+      claim();
+      while (__any_sync(0xffffffffu, have))
+      {
+        if (!have)
+          continue;
+        if (need_f0)
+        {
+          reaction_rates<1>(M, kk, Y, scr, 0);
+          forcing_gather<1>(M, scr, F0, 0);
+        }
+        const double H = c.H;
+        const double alpha = 1.0 / (H * P.gamma0);
+        jacobian_rates<1>(M, kk, Y, scr, 0);
+        jacobian_gather<1>(M, scr, LU, alpha, true, 0);
+        lu_decompose<1>(M.lu_s, M.diag_row_of, LU, inv, 0);
+        bool fc_is_src = false;
+        for (int32_t st = 0; st < P.stages; ++st)
+        {
+          const int32_t sc = st * (st - 1) / 2;
+          if (st > 0 && P.new_f[st])
+          {
+            for (int32_t i = 0; i < S; ++i)
+            {
+              double v = Y[i];
+              for (int32_t j = 0; j < st; ++j)
+                v += P.a[sc + j] * Kv(j)[i];
+              Yn[i] = v;
+            }
+            reaction_rates<1>(M, kk, Yn, scr, 0);
+            forcing_gather<1>(M, scr, Fc, 0);
+            fc_is_src = true;
+          }
+          double coh[6];
+          for (int32_t j = 0; j < st; ++j)
+            coh[j] = P.c[sc + j] / H;
+          Strided Ks = Kv(st);
+          for (int32_t i = 0; i < S; ++i)
+          {
+            double v = fc_is_src ? Fc[i] : F0[i];
+            for (int32_t j = 0; j < st; ++j)
+              v += coh[j] * Kv(j)[i];
+            Ks[i] = v;
+          }
+          solve_lower<1>(M.fwd_s, LU, Ks, 0);
+          solve_upper<1>(M.bwd_s, LU, Ks, 0);
+        }
+        // Ynew, error partial sums in the 32-lane-stripe order of the warp kernels
+        double part[32];
+#pragma unroll
+        for (int l = 0; l < 32; ++l)
+          part[l] = 0.0;
+        for (int32_t i = 0; i < S; ++i)
+        {
+          double v = Y[i];
+          double e = 0.0;
+          for (int32_t st = 0; st < P.stages; ++st)
+          {
+            const double kv = Kv(st)[i];
+            v += P.m[st] * kv;
+            e += P.e[st] * kv;
+          }
+          Yn[i] = v;
+          part[i & 31] += scaled_sq(Y[i], v, e, A.atol[i], A.rtol);
+        }
+        const double sum = butterfly_sum_serial(part);
+        const double rms = sqrt(sum / (double)S);
+        const double error = (rms < 1.0e-10) ? 1.0e-10 : rms;
+        count_attempt(c, P);
+        const double h_used = c.H;
+        const int res = ctl_after_error(c, P, B, error);
+        if (res == 1)
+        {
+          if (A.ckpt_y)
+          {
+            double* dst = A.ckpt_y + ((size_t)cell * A.max_ckpt + n_ckpt) * S;
+            for (int32_t i = 0; i < S; ++i)
+              dst[i] = Y[i];
+            A.ckpt_h[(size_t)cell * A.max_ckpt + n_ckpt] = h_used;
+            ++n_ckpt;
+          }
+          for (int32_t i = 0; i < S; ++i)
+            Y[i] = Yn[i];
+          bool more = ctl_begin_step(c, P, B);
+          if (more && A.ckpt_y && n_ckpt >= A.max_ckpt)
+          {
+            c.state = MICMB_SOLVER_CONVERGENCE_EXCEEDED_MAX_STEPS;
+            more = false;
+          }
+          if (more)
+          {
+            c.function_calls += 1;
+            c.jacobian_updates += 1;
+            need_f0 = true;
+          }
+          else
+          {
+            write_out();
+            claim();
+          }
+        }
+        else if (res == 0)
+          need_f0 = false;
+        else
+        {
+          write_out();
+          claim();
+        }
+      }
+      for (int q = 0; q < 8; ++q)
+      {
+        // one atomic per warp and counter
+        long long v = acc[q];
+        for (int off = 16; off > 0; off >>= 1)
+          v += __shfl_xor_sync(0xffffffffu, v, off);
+        if (lane == 0 && v)
+          atomicAdd(A.stats + q, (unsigned long long)v);
+      }
+    }
+  }  // namespace
+
+  bool SolveFusedThread(micmb_solver& s, micmb_state& st, const FusedArgs& A_in, double dt)
+  {
+    const auto& m = *s.mech;
+    const ThreadLayout T = MakeThreadLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz);
+    int per_sm = 0;
+    MICMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused_thread, kThreadsPerBlock, 0));
+    if (per_sm < 1)
+      return false;
+    if (s.fused.ctas_per_sm > 0)
+      per_sm = std::min(per_sm, s.fused.ctas_per_sm);
+    int64_t grid = (int64_t)per_sm * s.sm_count;
+    grid = std::max<int64_t>(1, std::min<int64_t>(grid, (A_in.n_cells + kThreadsPerBlock - 1) / kThreadsPerBlock));
+    const int64_t doubles = grid * kThreadsPerBlock * (int64_t)T.per_slot;
+    if (!st.thread_ws.p || st.thread_ws.bytes < (size_t)doubles * sizeof(double))
+      st.thread_ws = DeviceMemory((size_t)doubles * sizeof(double));
+    const StepBounds B = step_bounds(s.params, dt);
+    k_fused_thread<<<(unsigned)grid, kThreadsPerBlock, 0, st.stream>>>(s.dev, s.params, B, A_in,
+                                                                        st.thread_ws.as<double>(), T);
+    MICMB_CUDA(cudaGetLastError());
+    return true;
+  }
+}  // namespace micmb

@@ -133,6 +133,28 @@ namespace micmb
       return s;
     }
 
+    // One thread visiting every item in order, each with all of its terms:
+    // one level, no partial sums (the order the items were built in already
+    // respects their dependencies).
+    LevelSchedule SerialSchedule(const std::vector<RawItem>& items)
+    {
+      LevelSchedule s;
+      s.level_start = { 0, (int32_t)items.size() };
+      s.term_start.push_back(0);
+      for (const RawItem& it : items)
+      {
+        s.item_target.push_back(it.target);
+        s.item_aux.push_back(it.aux);
+        for (const auto& t : it.terms)
+        {
+          s.term_a.push_back(t.first);
+          s.term_b.push_back(t.second);
+        }
+        s.term_start.push_back((int32_t)s.term_a.size());
+      }
+      return s;
+    }
+
     // Lane-interleave a level schedule (see WarpTable).  `meta(i)` packs item i,
     // `pack(t)` packs term t, `coef` (optional) is per term; padding terms
     // are `dummy` with coefficient 0.  `cls(i)` (0 or kSegRecip) keeps items
@@ -764,6 +786,7 @@ namespace micmb
             add(j, mn);
       }
       m.lu = Schedule(items);
+      m.lu_serial = SerialSchedule(items);
     }
 
     // 9. triangular solves (linear_solver_in_place.inl:49-103, 113-167) and
@@ -785,6 +808,7 @@ namespace micmb
         f.push_back(std::move(it));
       }
       m.fwd = Schedule(f);
+      m.fwd_serial = SerialSchedule(f);
       // backward: visit i = S-1 .. 0; item index v = S-1-i
       for (int32_t v = 0; v < S; ++v)
       {
@@ -801,6 +825,7 @@ namespace micmb
         b.push_back(std::move(it));
       }
       m.bwd = Schedule(b);
+      m.bwd_serial = SerialSchedule(b);
       for (int32_t i = 0; i < S; ++i)
       {
         RawItem it;

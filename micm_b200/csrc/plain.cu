@@ -149,7 +149,7 @@ namespace micmb
       const int32_t L = a.L;
       Strided J{ a.jac + cell_base(c, L, M.nnz), L };
       Strided inv{ a.inv + cell_base(c, L, M.S), L };
-      lu_decompose<1>(M.lu, M.diag_row_of, J, inv, 0);
+      lu_decompose<1>(M.lu_s, M.diag_row_of, J, inv, 0);
     }
 
     // Ynew = Y + sum_j a_sj K_j ; Fcur = f(Ynew)
@@ -190,19 +190,19 @@ namespace micmb
       Strided F{ (src_is_f0 ? a.f0 : a.fcur) + bs, L };
       Strided Ks{ a.K + bk + (size_t)s * S * L, L };
       const int32_t sc = s * (s - 1) / 2;
+      double coh[6];
+      for (int32_t j = 0; j < s; ++j)
+        coh[j] = P.c[sc + j] / H;
       for (int32_t i = 0; i < S; ++i)
       {
         double v = F[i];
         for (int32_t j = 0; j < s; ++j)
-        {
-          const double c_over_h = P.c[sc + j] / H;
-          v += c_over_h * a.K[bk + (size_t)(j * S + i) * L];
-        }
+          v += coh[j] * a.K[bk + (size_t)(j * S + i) * L];
         Ks[i] = v;
       }
       Strided J{ a.jac + cell_base(c, L, M.nnz), L };
-      solve_lower<1>(M.fwd, J, Ks, 0);
-      solve_upper<1>(M.bwd, J, Ks, 0);
+      solve_lower<1>(M.fwd_s, J, Ks, 0);
+      solve_upper<1>(M.bwd_s, J, Ks, 0);
     }
 
     // Ynew = Y + sum m_s K_s ; Yerr = sum e_s K_s ; per-cell error partial sums
@@ -619,7 +619,7 @@ namespace micmb
       const int32_t L = a.L;
       Strided J{ a.jac + cell_base(c, L, M.nnz), L };
       Strided inv{ a.inv + cell_base(c, L, M.S), L };
-      lu_decompose<1>(M.lu, M.diag_row_of, J, inv, 0);
+      lu_decompose<1>(M.lu_s, M.diag_row_of, J, inv, 0);
     }
 
     __global__ void k_linear_solve_all(DevMech M, PlainArgs a)
@@ -630,8 +630,8 @@ namespace micmb
       const int32_t L = a.L;
       Strided J{ a.jac + cell_base(c, L, M.nnz), L };
       Strided x{ a.f0 + cell_base(c, L, M.S), L };
-      solve_lower<1>(M.fwd, J, x, 0);
-      solve_upper<1>(M.bwd, J, x, 0);
+      solve_lower<1>(M.fwd_s, J, x, 0);
+      solve_upper<1>(M.bwd_s, J, x, 0);
     }
 
     // errors are in f0, y in variables, ynew in the ynew buffer

@@ -121,6 +121,7 @@ struct micmb_state
   // fused path
   micmb::DeviceMemory lu_slots;
   int64_t lu_slot_count = 0;  // doubles allocated in lu_slots
+  micmb::DeviceMemory thread_ws;  // one-cell-per-thread variant: per-thread working sets
   micmb::DeviceMemory attempt_order;  // streamed kernel: block order of one attempt
   std::vector<int32_t> attempt_order_host;  // what attempt_order holds
   int64_t solve_limit = 0;                  // fused solves: only the first solve_limit cells (0 = all)
@@ -159,6 +160,8 @@ namespace micmb
   size_t FusedSharedBytes(const micmb_solver& s, bool lu_in_shared);
   // streamed warp-specialised variant; returns false when it does not apply
   bool SolveFusedStream(micmb_solver& s, micmb_state& st, double dt, const FusedArgs& A);
+  // one cell per thread, working sets in global memory
+  bool SolveFusedThread(micmb_solver& s, micmb_state& st, const FusedArgs& A, double dt);
   int StreamWarpsPerCta(const micmb_solver& s, int slots, int cap, bool lu_shared);
   // discrete adjoint sweep over the checkpoints of a fused solve
   void LaunchAdjoint(micmb_solver& s, micmb_state& st, int32_t max_ckpt);

@@ -31,6 +31,7 @@ def _significant(g, scale):
 
 @pytest.mark.parametrize("name,n,config", [("c60_adjoint", 96, None),
                                            ("c60_adjoint", 64, dict(variant=1)),
+                                           ("c60_adjoint", 64, dict(variant=2)),
                                            ("c210", 8, None)])
 def test_adjoint_matches_oracle(cuda_device, name, n, config):
     cfg, mech, inputs, solver, st = _setup(name, n, 41, config)

@@ -3,6 +3,7 @@ import numpy as np
 import pytest
 
 from micm_b200 import Solver, synthetic
+from micm_b200.solver import CONVERGED
 
 from gpu_helpers import make_state
 
@@ -56,3 +57,19 @@ def test_autotune_keeps_state_and_caches(cuda_device, tmp_path):
     assert other.autotune(cfg["dt"], st3, cache) == chosen
     with open(cache) as f:
         assert len(f.read().splitlines()) == 1
+
+
+def test_solve_after_autotune_on_more_cells_than_the_trial(cuda_device):
+    """The autotuner times a prefix of the state; per-cell outputs of the
+    following full solve must still cover every cell."""
+    cfg = synthetic.CONFIGS["c210"]
+    mech = cfg["mech"]()
+    n = 20000  # more than the autotuner's prefix (SMs x 96 cells)
+    inputs = synthetic.cell_inputs(mech, n, 23, **cfg["inputs"])
+    solver = Solver(mech, cfg["stages"], vector_length=128)
+    st = make_state(solver, inputs)
+    solver.update_state_parameters(st)
+    solver.autotune(60.0, st)
+    res = solver.solve(60.0, st, method="fused", step_control="per_cell", per_cell=True)
+    assert res.converged
+    assert len(res.per_cell_status) == n and np.all(res.per_cell_status == CONVERGED)
