@@ -200,6 +200,9 @@ def adjoint_ratio(torch, rank):
     solver = Solver(mech, cfg["stages"], vector_length=128)
     st = solver.get_state(n)
     st.set_inputs(inputs)
+    st.sync_inputs_to_device()
+    solver.update_state_parameters(st)
+    tuned = solver.autotune(cfg["dt"], st)
     rng = np.random.default_rng(cfg["seed"])
     target = rng.random(n) * 1e-9
     cols = solver.compiled.species_columns
@@ -234,7 +237,7 @@ def adjoint_ratio(torch, rank):
     return {"config": "c60_adjoint: 60 species, 120 reactions, 131,072 cells, 4-stage, dt=3600 s; "
                       "loss = sum_c (y_c[0] - target_c)^2; gradients w.r.t. all y0 and all log k",
             "forward_ms": 1000 * tf, "adjoint_ms": 1000 * ta, "adjoint_over_forward": ta / tf,
-            "accepted_per_cell": res.stats["accepted"] / n,
+            "accepted_per_cell": res.stats["accepted"] / n, "fused_config": tuned,
             "note": "adjoint time = forward solve with checkpoints + reverse sweep, host gradient copies included"}
 
 

@@ -331,6 +331,387 @@ namespace micmb
       }
     }
 
+    // ---- one cell per thread: the same recurrences over private working sets ----
+
+    // entry offsets of a thread's working set (each entry is 32 doubles, one per lane)
+    struct AdjThreadLayout
+    {
+      int32_t oy, oF0, oFc, oInv, oYb, oTmp, oYs, oK, oKb, oGb, oRb, oKk, oKbar, oScr, oLU, per_slot;
+    };
+
+    AdjThreadLayout MakeAdjThreadLayout(int32_t S, int32_t R, int32_t ns, int32_t n_info, int32_t nnz)
+    {
+      AdjThreadLayout t;
+      int32_t o = 0;
+      auto take = [&](int32_t n) {
+        const int32_t at = o;
+        o += n;
+        return at;
+      };
+      t.oy = take(S);
+      t.oF0 = take(S);
+      t.oFc = take(S);
+      t.oInv = take(S);
+      t.oYb = take(S);
+      t.oTmp = take(S);
+      t.oYs = take(ns * S);
+      t.oK = take(ns * S);
+      t.oKb = take(ns * S);
+      t.oGb = take(ns * S);
+      t.oRb = take(ns * S);
+      t.oKk = take(R);
+      t.oKbar = take(R);
+      t.oScr = take(R > n_info ? R : n_info);
+      t.oLU = take(nnz);
+      t.per_slot = o;
+      return t;
+    }
+
+    template<class V>
+    __device__ __forceinline__ double nu_dot_t(const DevMech& M, int32_t r, V v)
+    {
+      double s = 0.0;
+      for (int32_t i = M.prod_start[r]; i < M.prod_start[r + 1]; ++i)
+        s += M.prod_yield[i] * v[M.prod_ids[i]];
+      for (int32_t i = M.react_start[r]; i < M.react_start[r + 1]; ++i)
+        s -= v[M.react_ids[i]];
+      return s;
+    }
+
+    template<class V>
+    __device__ __forceinline__ double prod_except_t(const DevMech& M, int32_t r, V y, int32_t a, int32_t b)
+    {
+      double v = 1.0;
+      for (int32_t i = M.react_start[r]; i < M.react_start[r + 1]; ++i)
+        if (i != a && i != b)
+          v *= y[M.react_ids[i]];
+      return v;
+    }
+
+    // yb += J(y)^T g ; kb[r] += (nu_r . g) w_r(y)  (reactions in order, as the oracle)
+    template<class V>
+    __device__ void vjp_f_t(const DevMech& M, V kk, V y, V g, V yb, V kb)
+    {
+      for (int32_t r = 0; r < M.R; ++r)
+      {
+        const double c = nu_dot_t(M, r, g);
+        if (c == 0.0)
+          continue;
+        kb[r] += c * (kk[r] * prod_except_t(M, r, y, -1, -1));
+        for (int32_t i = M.react_start[r]; i < M.react_start[r + 1]; ++i)
+          yb[M.react_ids[i]] += c * kk[r] * prod_except_t(M, r, y, i, -1);
+      }
+    }
+
+    template<class V>
+    __device__ void jacobian_term_t(const DevMech& M, V kk, V y, V Rb, V Kv, V yb, V kb)
+    {
+      for (int32_t r = 0; r < M.R; ++r)
+      {
+        const double rho = nu_dot_t(M, r, Rb);
+        if (rho == 0.0)
+          continue;
+        const int32_t r0 = M.react_start[r], r1 = M.react_start[r + 1];
+        double gk = 0.0;
+        for (int32_t i = r0; i < r1; ++i)
+          gk += kk[r] * prod_except_t(M, r, y, i, -1) * Kv[M.react_ids[i]];
+        kb[r] += rho * gk;
+        for (int32_t i = r0; i < r1; ++i)
+          for (int32_t j = r0; j < r1; ++j)
+            if (i != j)
+              yb[M.react_ids[j]] += rho * kk[r] * prod_except_t(M, r, y, i, j) * Kv[M.react_ids[i]];
+      }
+    }
+
+    // vjp_f_t over fixed-width reactant lists (rate_desc)
+    template<class V>
+    __device__ void vjp_narrow(const DevMech& M, V kk, V y, V g, V yb, V kb)
+    {
+      const int32_t S = M.S;
+      for (int32_t r = 0; r < M.R; ++r)
+      {
+        const double c = nu_dot_t(M, r, g);
+        if (c == 0.0)
+          continue;
+        const int4 d = M.rate_desc[r];
+        const int32_t id[3] = { d.x, d.y, d.z };
+        double yv[3];
+        int32_t nr = 0;
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+        {
+          yv[q] = id[q] < S ? y[id[q]] : 1.0;
+          nr += id[q] < S ? 1 : 0;
+        }
+        const double k = kk[r];
+        kb[r] += c * (k * (((1.0 * yv[0]) * yv[1]) * yv[2]));
+        for (int q = 0; q < nr; ++q)
+        {
+          double v = 1.0;
+          for (int o = 0; o < nr; ++o)
+            if (o != q)
+              v *= yv[o];
+          yb[id[q]] += c * k * v;
+        }
+      }
+    }
+
+    // Reactions with at most three reactants (rate_desc): one pass over the
+    // reactions at the step's starting state applies J(y)^T Gbar_0 and the
+    // second-order terms of every stage, with w_r's partial derivatives formed
+    // once per reaction instead of once per use.
+    template<class V>
+    __device__ void step_terms_narrow(const DevMech& M, int32_t ns, V kk, V y, V Gb0, const V* Rb, const V* K, V yb,
+                                      V kb)
+    {
+      const int32_t S = M.S;
+      for (int32_t r = 0; r < M.R; ++r)
+      {
+        const int4 d = M.rate_desc[r];
+        const int32_t id[3] = { d.x, d.y, d.z };
+        int32_t nr = 0;
+        double yv[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+        {
+          yv[q] = id[q] < S ? y[id[q]] : 1.0;
+          nr += id[q] < S ? 1 : 0;
+        }
+        const double k = kk[r];
+        // first derivatives k * prod of the other reactants (in reactant order)
+        double P1[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+        {
+          double v = 1.0;
+#pragma unroll
+          for (int o = 0; o < 3; ++o)
+            if (o != q && o < nr)
+              v *= yv[o];
+          P1[q] = v;
+        }
+        // J(y)^T Gbar_0
+        const double c = nu_dot_t(M, r, Gb0);
+        if (c != 0.0)
+        {
+          kb[r] += c * (k * (((1.0 * (nr > 0 ? yv[0] : 1.0)) * (nr > 1 ? yv[1] : 1.0)) * (nr > 2 ? yv[2] : 1.0)));
+          for (int q = 0; q < nr; ++q)
+            yb[id[q]] += c * k * P1[q];
+        }
+        // second-order terms of every stage
+        for (int32_t st = 0; st < ns; ++st)
+        {
+          const double rho = nu_dot_t(M, r, Rb[st]);
+          if (rho == 0.0)
+            continue;
+          double kv[3];
+          for (int q = 0; q < nr; ++q)
+            kv[q] = K[st][id[q]];
+          double gk = 0.0;
+          for (int q = 0; q < nr; ++q)
+            gk += k * P1[q] * kv[q];
+          kb[r] += rho * gk;
+          for (int q = 0; q < nr; ++q)
+            for (int o = 0; o < nr; ++o)
+              if (q != o)
+              {
+                double v = 1.0;  // product of the reactants other than q and o
+                for (int z = 0; z < nr; ++z)
+                  if (z != q && z != o)
+                    v *= yv[z];
+                yb[id[o]] += rho * k * v * kv[q];
+              }
+        }
+      }
+    }
+
+    __global__ void __launch_bounds__(128) k_adjoint_thread(DevMech M, DevParams P, AdjArgs A, AdjThreadLayout T,
+                                                           double* ws)
+    {
+      const int lane = threadIdx.x & 31;
+      const int64_t wslot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+      double* w = ws + (size_t)wslot * (size_t)T.per_slot * 32 + lane;
+      const int32_t S = M.S, R = M.R, L = A.L, ns = P.stages;
+      auto at = [&](int32_t entry) { return Strided{ w + (size_t)entry * 32, 32 }; };
+      Strided y = at(T.oy), F0 = at(T.oF0), Fc = at(T.oFc), inv = at(T.oInv), yb = at(T.oYb), tmp = at(T.oTmp);
+      Strided kk = at(T.oKk), kb = at(T.oKbar), scr = at(T.oScr), LU = at(T.oLU);
+      auto Ys = [&](int32_t s) { return at(T.oYs + s * S); };
+      auto K = [&](int32_t s) { return at(T.oK + s * S); };
+      auto Kb = [&](int32_t s) { return at(T.oKb + s * S); };
+      auto Gb = [&](int32_t s) { return at(T.oGb + s * S); };
+      auto Rb = [&](int32_t s) { return at(T.oRb + s * S); };
+
+      int64_t cell = 0;
+      int32_t n = -1;  // checkpoint being processed; -1: no cell
+      auto finish = [&]() {
+        const size_t by = cell_base(cell, L, S);
+        for (int32_t i = 0; i < S; ++i)
+          A.ybar0[by + (size_t)i * L] = yb[i];
+        for (int32_t r = 0; r < R; ++r)
+          A.kbar[(size_t)cell * R + r] = kb[r];
+      };
+      auto claim = [&]() {
+        for (;;)
+        {
+          cell = atomicAdd(A.next_cell, 1);
+          if (cell >= A.n_cells)
+          {
+            n = -1;
+            return;
+          }
+          const size_t by = cell_base(cell, L, S);
+          const size_t bk = cell_base(cell, L, R);
+          for (int32_t r = 0; r < R; ++r)
+          {
+            kk[r] = A.rate_constants[bk + (size_t)r * L];
+            kb[r] = 0.0;
+          }
+          const int32_t n_ck = A.n_ckpt[cell];
+          if (n_ck > 0)
+          {
+            n = n_ck - 1;
+            return;
+          }
+          for (int32_t i = 0; i < S; ++i)
+            yb[i] = (A.y0[by + (size_t)i * L] < 0.0) ? 0.0 : A.ybar_final[by + (size_t)i * L];
+          finish();
+        }
+      };
+
+      claim();
+      while (__any_sync(0xffffffffu, n >= 0))
+      {
+        if (n < 0)
+          continue;
+        const size_t by = cell_base(cell, L, S);
+        const double* yc = A.ckpt_y + ((size_t)cell * A.max_ckpt + n) * S;
+        const double H = A.ckpt_h[(size_t)cell * A.max_ckpt + n];
+        for (int32_t i = 0; i < S; ++i)
+          y[i] = yc[i];
+        // ---- recompute the accepted step ----
+        reaction_rates<1>(M, kk, y, scr, 0);
+        forcing_gather<1>(M, scr, F0, 0);
+        const double alpha = 1.0 / (H * P.gamma0);
+        jacobian_rates<1>(M, kk, y, scr, 0);
+        jacobian_gather<1>(M, scr, LU, alpha, true, 0);
+        lu_decompose<1>(M.lu_s, M.diag_row_of, LU, inv, 0);
+        bool fc_is_src = false;
+        for (int32_t st = 0; st < ns; ++st)
+        {
+          const int32_t sc = st * (st - 1) / 2;
+          Strided Yst = Ys(st);
+          if (st > 0 && P.new_f[st])
+          {
+            for (int32_t i = 0; i < S; ++i)
+            {
+              double v = y[i];
+              for (int32_t j = 0; j < st; ++j)
+                v += P.a[sc + j] * K(j)[i];
+              Yst[i] = v;
+            }
+            reaction_rates<1>(M, kk, Yst, scr, 0);
+            forcing_gather<1>(M, scr, Fc, 0);
+            fc_is_src = true;
+          }
+          else
+            for (int32_t i = 0; i < S; ++i)
+              Yst[i] = y[i];
+          double coh[kMaxAdjStages];
+          for (int32_t j = 0; j < st; ++j)
+            coh[j] = P.c[sc + j] / H;
+          Strided Ks = K(st);
+          for (int32_t i = 0; i < S; ++i)
+          {
+            double v = fc_is_src ? Fc[i] : F0[i];
+            for (int32_t j = 0; j < st; ++j)
+              v += coh[j] * K(j)[i];
+            Ks[i] = v;
+          }
+          solve_lower<1>(M.fwd_s, LU, Ks, 0);
+          solve_upper<1>(M.bwd_s, LU, Ks, 0);
+        }
+        if (n == A.n_ckpt[cell] - 1)
+          for (int32_t i = 0; i < S; ++i)
+          {
+            double v = y[i];
+            for (int32_t st = 0; st < ns; ++st)
+              v += P.m[st] * K(st)[i];
+            yb[i] = (v < 0.0) ? 0.0 : A.ybar_final[by + (size_t)i * L];
+          }
+        // ---- reverse sweep ----
+        for (int32_t i = 0; i < S; ++i)
+        {
+          const double g = yb[i];
+          for (int32_t st = 0; st < ns; ++st)
+          {
+            Kb(st)[i] = P.m[st] * g;
+            Gb(st)[i] = 0.0;
+          }
+        }
+        for (int32_t st = ns - 1; st >= 0; --st)
+        {
+          const int32_t sc = st * (st - 1) / 2;
+          Strided rb = Rb(st);
+          for (int32_t i = 0; i < S; ++i)
+            rb[i] = Kb(st)[i];
+          solve_upper<1>(M.fwd_t_s, LU, rb, 0);  // U^T w = Kbar (divides by u_ii)
+          solve_lower<1>(M.bwd_t_s, LU, rb, 0);  // L^T z = w
+          double coh[kMaxAdjStages];
+          for (int32_t j = 0; j < st; ++j)
+            coh[j] = P.c[sc + j] / H;
+          for (int32_t i = 0; i < S; ++i)
+          {
+            const double v = rb[i];
+            Gb(st)[i] += v;
+            for (int32_t j = 0; j < st; ++j)
+              Kb(j)[i] += coh[j] * v;
+          }
+          if (st == 0)
+            continue;
+          if (P.new_f[st])
+          {
+            for (int32_t i = 0; i < S; ++i)
+              tmp[i] = 0.0;
+            if (M.rate_desc)
+              vjp_narrow(M, kk, Ys(st), Gb(st), tmp, kb);
+            else
+              vjp_f_t(M, kk, Ys(st), Gb(st), tmp, kb);
+            for (int32_t i = 0; i < S; ++i)
+            {
+              const double t = tmp[i];
+              yb[i] += t;
+              for (int32_t j = 0; j < st; ++j)
+                Kb(j)[i] += P.a[sc + j] * t;
+            }
+          }
+          else
+            for (int32_t i = 0; i < S; ++i)
+              Gb(st - 1)[i] += Gb(st)[i];
+        }
+        if (M.rate_desc)
+        {
+          Strided rbs[kMaxAdjStages], ks[kMaxAdjStages];
+          for (int32_t st = 0; st < ns; ++st)
+          {
+            rbs[st] = Rb(st);
+            ks[st] = K(st);
+          }
+          step_terms_narrow(M, ns, kk, y, Gb(0), rbs, ks, yb, kb);
+        }
+        else
+        {
+          vjp_f_t(M, kk, y, Gb(0), yb, kb);
+          for (int32_t st = 0; st < ns; ++st)
+            jacobian_term_t(M, kk, y, Rb(st), K(st), yb, kb);
+        }
+        if (--n < 0)
+        {
+          finish();
+          claim();
+        }
+      }
+    }
+
     // out[r] = sum over cells of kbar[cell][r], in a fixed order (deterministic)
     __global__ void k_sum_cells(const double* kbar, int64_t n_cells, int32_t R, double* out)
     {
@@ -352,9 +733,58 @@ namespace micmb
     }
   }  // namespace
 
+  // one cell per thread: per-thread working sets in global memory, no atomics
+  void LaunchAdjointThread(micmb_solver& s, micmb_state& st, int32_t max_ckpt)
+  {
+    const auto& m = *s.mech;
+    if (s.params.stages > kMaxAdjStages)
+      throw Error(MICMB_ERR_UNSUPPORTED, "too many stages for the adjoint kernel");
+    const AdjThreadLayout T = MakeAdjThreadLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz);
+    int per_sm = 0;
+    MICMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adjoint_thread, 128, 0));
+    if (per_sm < 1)
+      throw Error(MICMB_ERR_UNSUPPORTED, "adjoint kernel cannot be resident");
+    const int64_t n = st.n_cells;
+    int64_t grid = (int64_t)per_sm * s.sm_count;
+    grid = std::max<int64_t>(1, std::min<int64_t>(grid, (n + 127) / 128));
+    const int64_t doubles = grid * 128 * (int64_t)T.per_slot;
+    if (!st.thread_ws.p || st.thread_ws.bytes < (size_t)doubles * sizeof(double))
+      st.thread_ws = DeviceMemory((size_t)doubles * sizeof(double));
+    AdjArgs A{};
+    A.n_cells = n;
+    A.L = st.L;
+    A.max_ckpt = max_ckpt;
+    A.rate_constants = st.rate_constants.as<double>();
+    A.y0 = st.adj_y0.as<double>();
+    A.ybar_final = st.adj_ybar.as<double>();
+    A.ckpt_y = st.adj_ckpt_y.as<double>();
+    A.ckpt_h = st.adj_ckpt_h.as<double>();
+    A.n_ckpt = st.accepted.as<int32_t>();
+    A.ybar0 = st.adj_ybar.as<double>();
+    A.kbar = st.adj_kbar_cells.as<double>();
+    char* cbase = st.counters.as<char>();
+    A.next_cell = reinterpret_cast<int32_t*>(cbase + 8);
+    MICMB_CUDA(cudaMemsetAsync(cbase + 8, 0, 8, st.stream));
+    if (n > 0)
+    {
+      k_adjoint_thread<<<(unsigned)grid, 128, 0, st.stream>>>(s.dev, s.params, A, T, st.thread_ws.as<double>());
+      MICMB_CUDA(cudaGetLastError());
+    }
+    if (m.R > 0)
+    {
+      k_sum_cells<<<(unsigned)m.R, 256, 0, st.stream>>>(A.kbar, n, m.R, st.adj_kbar.as<double>());
+      MICMB_CUDA(cudaGetLastError());
+    }
+  }
+
   void LaunchAdjoint(micmb_solver& s, micmb_state& st, int32_t max_ckpt)
   {
     const auto& m = *s.mech;
+    if (s.fused.variant == 2)
+    {
+      LaunchAdjointThread(s, st, max_ckpt);
+      return;
+    }
     if (!s.dev.has_warp)
       throw Error(MICMB_ERR_UNSUPPORTED, "mechanism exceeds the fused kernel's 16-bit table positions");
     if (s.params.stages > kMaxAdjStages)

@@ -197,7 +197,8 @@ namespace micmb
       const SchedOffsets lu = AddSchedule(pk, m.lu), fw = AddSchedule(pk, m.fwd), bw = AddSchedule(pk, m.bwd),
                          fwt = AddSchedule(pk, m.fwd_t), bwt = AddSchedule(pk, m.bwd_t);
       const SchedOffsets lus = AddSchedule(pk, m.lu_serial), fws = AddSchedule(pk, m.fwd_serial),
-                         bws = AddSchedule(pk, m.bwd_serial);
+                         bws = AddSchedule(pk, m.bwd_serial), fwts = AddSchedule(pk, m.fwd_t_serial),
+                         bwts = AddSchedule(pk, m.bwd_t_serial);
       const size_t o_rd = pk.add(m.rate_desc), o_drd = pk.add(m.drate_desc);
       WarpOffsets wl{}, wf{}, wb{}, wft{}, wbt{}, wfo{}, wj{};
       if (m.has_warp_tables)
@@ -265,6 +266,8 @@ namespace micmb
       d.lu_s = Resolve(b, lus);
       d.fwd_s = Resolve(b, fws);
       d.bwd_s = Resolve(b, bws);
+      d.fwd_t_s = Resolve(b, fwts);
+      d.bwd_t_s = Resolve(b, bwts);
       s.diag_row_of = d.diag_row_of;
       d.has_warp = m.has_warp_tables ? 1 : 0;
       d.scratch_zero = m.scratch_zero;

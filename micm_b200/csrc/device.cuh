@@ -74,7 +74,7 @@ namespace micmb
     const int32_t* diag_pos;     // [S] storage position of a_ii
     const int32_t* diag_row_of;  // [nnz] row i if the position holds a_ii, else -1
     DevSchedule lu, fwd, bwd, fwd_t, bwd_t;
-    DevSchedule lu_s, fwd_s, bwd_s;  // serial forms (one thread per cell)
+    DevSchedule lu_s, fwd_s, bwd_s, fwd_t_s, bwd_t_s;  // serial forms (one thread per cell)
     // warp-interleaved tables (fused kernel); dummy slots: LU[nnz], x[S], scratch[scratch_zero]
     int32_t has_warp;
     int32_t scratch_zero;

@@ -841,6 +841,7 @@ namespace micmb
         ft.push_back(std::move(it));
       }
       m.fwd_t = Schedule(ft);
+      m.fwd_t_serial = SerialSchedule(ft);
       for (int32_t v = 0; v < S; ++v)
       {
         const int32_t i = S - 1 - v;
@@ -856,6 +857,7 @@ namespace micmb
         bt.push_back(std::move(it));
       }
       m.bwd_t = Schedule(bt);
+      m.bwd_t_serial = SerialSchedule(bt);
     }
 
     // 10. warp-interleaved tables for the fused kernel (16-bit operand positions)

@@ -151,7 +151,7 @@ namespace micmb
     LevelSchedule bwd_t;   // L^T z = w: target i, terms (L_ji pos, j)
     // the same LU and solves as single-level lists in visiting order, every
     // item whole (no partial sums): the order one thread per cell runs them
-    LevelSchedule lu_serial, fwd_serial, bwd_serial;
+    LevelSchedule lu_serial, fwd_serial, bwd_serial, fwd_t_serial, bwd_t_serial;
 
     // warp-interleaved forms for the fused kernel (empty when the mechanism
     // exceeds 16-bit positions); dummy operands: LU slot nnz, vector slot S,
