@@ -30,6 +30,7 @@ sys.path.insert(0, ROOT)
 METRIC = "cell-solves/s @1M cells, FP64 rtol1e-6 (fused vs plain); adjoint/forward time"
 UNIT = "cell-solves/s"
 CONFIG_NAME = "c210_uneven"
+KERNEL_OF_VARIANT = {0: "k_fused_stream", 1: "k_fused", 2: "k_fused_thread"}
 
 
 def parse():
@@ -42,6 +43,8 @@ def parse():
     ap.add_argument("--plain-cells", type=int, default=1048576,
                     help="cells per GPU for the plain-method comparison (0 = skip)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="fixed fused configuration (one cell per thread) instead of the autotuner")
     ap.add_argument("--cpu-sample", type=int, default=65536, help="cells timed on the host CPU")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -169,6 +172,49 @@ def flops_per_solve_unit(mech, solver, stages):
     return dict(force=f_force, jac=f_jac, lu=f_lu, solve=f_solve, attempt=f_attempt)
 
 
+def bytes_per_solve_unit(mech, solver, stages):
+    """Compulsory HBM bytes of one unit of each kind of work when every working
+    set lives in HBM (the plain kernels and the one-cell-per-thread kernel):
+    -J assembly writes the factor (zeroed, then read-modify-written), the LU
+    reads and writes it, each stage solve reads it once and its vector twice,
+    a forcing evaluation reads the rate constants and three state-sized
+    vectors, and each attempt's stage sums and error norm stream state-sized
+    vectors."""
+    info = solver.compiled.info
+    S, R, nnz = mech.n_species, mech.n_reactions, info["jacobian_nnz"]
+    n_axpy = stages * (stages - 1) + 2
+    return dict(force=8 * (R + 3 * S), jac=8 * 3 * nnz, lu=8 * (2 * nnz + 2 * S), solve=8 * (nnz + 2 * S),
+                attempt=8 * (3 * S * n_axpy + 4 * S))
+
+
+def solve_bytes(units, stats):
+    return (stats["function_calls"] * units["force"] + stats["jacobian_updates"] * units["jac"]
+            + stats["decompositions"] * units["lu"] + stats["solves"] * units["solve"]
+            + stats["number_of_steps"] * units["attempt"])
+
+
+def hbm_peak():
+    """HBM copy bandwidth measured on this pool (MEASURED_PEAKS.json), else the fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def measured_traffic(cells):
+    """DRAM bytes of one fused launch over `cells` cells, scaled from the committed capture."""
+    path = os.path.join(ROOT, "profiles", "k_fused_thread_c210_65536cells.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_cell_solve:"):
+                    return float(line.split(":")[1]) * cells
+    except OSError:
+        pass
+    return None
+
+
 def solve_flops(units, stats):
     return (stats["function_calls"] * units["force"] + stats["jacobian_updates"] * units["jac"]
             + stats["decompositions"] * units["lu"] + stats["solves"] * units["solve"]
@@ -269,7 +315,11 @@ def main():
     state.set_inputs(inputs)
     state.sync_inputs_to_device()
     solver.update_state_parameters(state)
-    tuned = solver.autotune(cfg["dt"], state)                  # cells-per-CTA, LU staging, ring depth, variant
+    if args.no_autotune:
+        solver.set_fused_config(variant=2, lu_in_shared=0)
+        tuned = solver.get_fused_config()
+    else:
+        tuned = solver.autotune(cfg["dt"], state)              # cells-per-CTA, LU staging, ring depth, variant
     stream = torch.cuda.current_stream()
     check(lib().micmb_state_set_stream(state.handle, ctypes.c_void_p(stream.cuda_stream)))
     y0_host = to_vector_layout(state.variables, L)
@@ -315,11 +365,17 @@ def main():
     attempts_per_cell = totals["number_of_steps"] / (args.cells * args.steps)
     accepted_per_cell = totals["accepted"] / (args.cells * args.steps)
 
-    # roofline of the fused kernel: FP64 work of the accepted and rejected attempts
+    # roofline of the fused kernel.  One cell per thread keeps every working set
+    # in HBM, so the bound is the compulsory traffic of that formulation
+    # (bytes_per_solve_unit); the FP64 work is reported beside it.
+    bunits = bytes_per_solve_unit(mech, solver, cfg["stages"])
+    algo_bytes = solve_bytes(bunits, totals) / args.steps      # per launch (one Solve over the shard)
+    kernel_s = kernel_ms / args.steps / 1000.0
+    achieved_gbs = algo_bytes / kernel_s / 1e9
+    peak_gbs, peak_src = hbm_peak()
     units = flops_per_solve_unit(mech, solver, cfg["stages"])
-    flops = solve_flops(units, totals) / args.steps            # per launch (one Solve over the shard)
-    achieved = flops / (kernel_ms / args.steps / 1000.0) / 1e12
-    peak = fp64_peak()
+    flops = solve_flops(units, totals) / args.steps
+    traffic = measured_traffic(args.cells)
 
     # e2e: the public API with host buffers every step (H2D inputs, D2H results)
     h_vars = torch.from_numpy(y0_host).pin_memory().numpy()
@@ -370,9 +426,14 @@ def main():
         pres = solver.solve(cfg["dt"], pstate, method="plain", step_control="per_cell")
         torch.cuda.synchronize()
         pt = time.perf_counter() - t0
+        plain_gbs = solve_bytes(bytes_per_solve_unit(mech, solver, cfg["stages"]), pres.stats) / pt / 1e9
         plain = {"value": pc * world / pt, "unit": UNIT, "cells_per_gpu": pc, "ms_per_step": 1000 * pt,
                  "attempts_per_cell": pres.stats["number_of_steps"] / pc,
-                 "fused_over_plain": value / (pc * world / pt)}
+                 "fused_over_plain": value / (pc * world / pt),
+                 "roofline": {"bound": "hbm", "achieved": plain_gbs, "peak": peak_gbs, "unit": "GB/s",
+                              "frac": plain_gbs / peak_gbs,
+                              "note": "algorithmic bytes of the per-stage kernels over the solve's wall time "
+                                      "(launches and host synchronisation included)"}}
 
     adj = adjoint_ratio(torch, rank) if not args.no_adjoint else None
 
@@ -398,12 +459,16 @@ def main():
                     "d2h_bytes_per_step": d2h,
                     "calls": "upload variables/conditions/custom params, UpdateStateParameters, Solve, "
                              "download variables (pinned host buffers)"},
-            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "kernel": "k_fused_stream (one launch per step)",
-                         "flops_per_launch": flops, "kernel_ms_per_launch": kernel_ms / args.steps,
-                         "peak_source": "nominal FP64 (SMs x 64 FMA/clk x 2 x max SM clock); "
-                                        "MEASURED_PEAKS.json has no FP64 entry"},
+            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": peak_gbs, "unit": "GB/s",
+                         "frac": achieved_gbs / peak_gbs, "traffic": traffic,
+                         "kernel": KERNEL_OF_VARIANT.get(tuned["variant"], "fused") + " (one launch per step)",
+                         "algorithmic_bytes_per_launch": algo_bytes, "kernel_ms_per_launch": kernel_ms / args.steps,
+                         "peak_source": peak_src,
+                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of a 65,536-cell capture "
+                                           "(profiles/k_fused_thread_c210_65536cells.md) scaled by cells",
+                         "fp64": {"achieved_tflops": flops / kernel_s / 1e12, "peak_tflops": fp64_peak(),
+                                  "frac": flops / kernel_s / 1e12 / fp64_peak(), "flops_per_launch": flops,
+                                  "peak_source": "nominal (SMs x 64 FMA/clk x 2 x max SM clock)"}},
             "gpu_launches": args.steps,
             "plain": plain,
             "adjoint": adj,

@@ -19,6 +19,9 @@ namespace micmb
   namespace
   {
     constexpr int kThreadsPerBlock = 128;
+    // no register cap: at 96 registers (20 resident warps per SM) the kernel runs
+    // faster than capped at 64 (32 warps), where it spills
+    constexpr int kMinBlocks = 1;
 
     __device__ __forceinline__ size_t cell_base(int64_t c, int32_t L, int32_t ncol)
     {
@@ -65,7 +68,7 @@ namespace micmb
         cc.function_calls += P.new_f[s] ? 1 : 0;
     }
 
-    __global__ void __launch_bounds__(kThreadsPerBlock)
+    __global__ void __launch_bounds__(kThreadsPerBlock, kMinBlocks)
         k_fused_thread(DevMech M, DevParams P, StepBounds B, FusedArgs A, double* ws, ThreadLayout T)
     {
       const int lane = threadIdx.x & 31;

@@ -115,9 +115,12 @@ class CompiledMechanism:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h and h.value and _native._lib is not None:
-            _native._lib.micmb_mechanism_destroy(h)
-            self.handle = None
+        try:
+            if h and h.value and _native._lib is not None:
+                _native._lib.micmb_mechanism_destroy(h)
+                self.handle = None
+        except (AttributeError, TypeError):  # interpreter shutdown: the library is already unloaded
+            pass
 
 
 @dataclasses.dataclass
@@ -150,9 +153,12 @@ class Solver:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h and h.value and _native._lib is not None:
-            _native._lib.micmb_solver_destroy(h)
-            self.handle = None
+        try:
+            if h and h.value and _native._lib is not None:
+                _native._lib.micmb_solver_destroy(h)
+                self.handle = None
+        except (AttributeError, TypeError):  # interpreter shutdown: the library is already unloaded
+            pass
 
     def set_rate_scale(self, scale: np.ndarray):
         scale = np.ascontiguousarray(scale, dtype=np.float64)
@@ -240,9 +246,12 @@ class State:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h and h.value and _native._lib is not None:
-            _native._lib.micmb_state_destroy(h)
-            self.handle = None
+        try:
+            if h and h.value and _native._lib is not None:
+                _native._lib.micmb_state_destroy(h)
+                self.handle = None
+        except (AttributeError, TypeError):  # interpreter shutdown: the library is already unloaded
+            pass
 
     # micm State::operator[](species) / SetConcentrations in system order
     def set_concentrations(self, y_system_order: np.ndarray):
