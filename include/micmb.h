@@ -332,6 +332,17 @@ int micmb_linear_solve(micmb_solver* solver, micmb_state* state);
 int micmb_normalized_error(micmb_solver* solver, micmb_state* state, double* global_out,
                            double* per_cell_out);
 
+/* The global value of micmb_normalized_error, computed without allocating
+ * (no counterpart in micm).  Scratch is a fixed file-scope device array for at
+ * most 65536 cells; larger states return MICMB_ERR_INVALID_ARGUMENT.  The
+ * buffers read (variables, MICMB_BUF_SCRATCH_Y, MICMB_BUF_FORCING, absolute
+ * tolerances) must already exist: upload them first.  Nothing in the scratch
+ * needs to start at zero.  The first call on a device looks up the scratch
+ * address (cudaGetSymbolAddress); make it before any stream capture.  There is
+ * one scratch area per device: overlapping calls on the same device race on
+ * it, so serialise them. */
+int micmb_normalized_error_noalloc(micmb_solver* solver, micmb_state* state, double* global_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,6 +66,7 @@ def lib():
             "micmb_lu_decompose": [vp, vp],
             "micmb_linear_solve": [vp, vp],
             "micmb_normalized_error": [vp, vp, f64p, f64p],
+            "micmb_normalized_error_noalloc": [vp, vp, f64p],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
