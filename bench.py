@@ -98,6 +98,21 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def max_over_ranks(values, dist, device):
+    """Element-wise maximum of per-rank timings (the slowest rank sets the job time)."""
+    if not dist:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def job_throughput(cells_per_rank: int, world: int, steps: int, seconds: float) -> float:
+    """Cell-solves per second of the whole job: every rank solves its own shard."""
+    return cells_per_rank * world * steps / seconds
+
+
 def workload(cells: int, rank: int = 0):
     from micm_b200 import synthetic
     cfg = synthetic.CONFIGS[CONFIG_NAME]
@@ -357,11 +372,8 @@ def main():
         torch.cuda.synchronize()
     ms = start.elapsed_time(end)
     kernel_ms = sum(a.elapsed_time(b) for a, b in events)
-    if dist:
-        t = torch.tensor([ms, kernel_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, kernel_ms = float(t[0].item()), float(t[1].item())
-    value = args.cells * world * args.steps / (ms / 1000.0)
+    ms, kernel_ms = max_over_ranks([ms, kernel_ms], dist, "cuda")
+    value = job_throughput(args.cells, world, args.steps, ms / 1000.0)
     attempts_per_cell = totals["number_of_steps"] / (args.cells * args.steps)
     accepted_per_cell = totals["accepted"] / (args.cells * args.steps)
 
@@ -398,10 +410,7 @@ def main():
                                          h_out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
     torch.cuda.synchronize()
     e2e_t = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_t], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_t = float(t.item())
+    (e2e_t,) = max_over_ranks([e2e_t], dist, "cuda")
     h2d = h_vars.nbytes + h_cond.nbytes + h_par.nbytes
     d2h = h_out.nbytes
 
@@ -455,7 +464,7 @@ def main():
                        "lu_nnz": info["jacobian_nnz"], "lu_updates": info["lu_updates"],
                        "attempts_per_cell": attempts_per_cell, "accepted_per_cell": accepted_per_cell},
             "clocks": clocks.summary(),
-            "e2e": {"value": args.cells * world * e2e_steps / e2e_t, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "e2e": {"value": job_throughput(args.cells, world, e2e_steps, e2e_t), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
                     "calls": "upload variables/conditions/custom params, UpdateStateParameters, Solve, "
                              "download variables (pinned host buffers)"},
