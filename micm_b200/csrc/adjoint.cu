@@ -52,6 +52,7 @@ namespace micmb
       const double* ybar_final;      // vector layout [S]
       const double* ckpt_y;          // [cell][max_ckpt][S]
       const double* ckpt_h;          // [cell][max_ckpt]
+      const double* ckpt_k;          // [cell][max_ckpt][stages][S] stored stage vectors, or null
       const int32_t* n_ckpt;         // [cell]
       double* ybar0;                 // vector layout [S]
       double* kbar;                  // [cell][R]
@@ -588,47 +589,77 @@ namespace micmb
         const double H = A.ckpt_h[(size_t)cell * A.max_ckpt + n];
         for (int32_t i = 0; i < S; ++i)
           y[i] = yc[i];
-        // ---- recompute the accepted step ----
-        reaction_rates<1>(M, kk, y, scr, 0);
-        forcing_gather<1>(M, scr, F0, 0);
+        // ---- the accepted step's factor, stages and stage inputs ----
         const double alpha = 1.0 / (H * P.gamma0);
         jacobian_rates<1>(M, kk, y, scr, 0);
         jacobian_gather<1>(M, scr, LU, alpha, true, 0);
         lu_decompose<1>(M.lu_s, M.diag_row_of, LU, inv, 0);
-        bool fc_is_src = false;
-        for (int32_t st = 0; st < ns; ++st)
+        if (A.ckpt_k)
         {
-          const int32_t sc = st * (st - 1) / 2;
-          Strided Yst = Ys(st);
-          if (st > 0 && P.new_f[st])
+          // stages stored by the forward pass; stage inputs rebuilt from them
+          const double* kc = A.ckpt_k + ((size_t)cell * A.max_ckpt + n) * (size_t)ns * S;
+          for (int32_t st = 0; st < ns; ++st)
           {
+            Strided Ks = K(st);
+            for (int32_t i = 0; i < S; ++i)
+              Ks[i] = kc[(size_t)st * S + i];
+          }
+          for (int32_t st = 0; st < ns; ++st)
+          {
+            const int32_t sc = st * (st - 1) / 2;
+            Strided Yst = Ys(st);
+            if (st > 0 && P.new_f[st])
+              for (int32_t i = 0; i < S; ++i)
+              {
+                double v = y[i];
+                for (int32_t j = 0; j < st; ++j)
+                  v += P.a[sc + j] * K(j)[i];
+                Yst[i] = v;
+              }
+            else
+              for (int32_t i = 0; i < S; ++i)
+                Yst[i] = y[i];
+          }
+        }
+        else
+        {
+          reaction_rates<1>(M, kk, y, scr, 0);
+          forcing_gather<1>(M, scr, F0, 0);
+          bool fc_is_src = false;
+          for (int32_t st = 0; st < ns; ++st)
+          {
+            const int32_t sc = st * (st - 1) / 2;
+            Strided Yst = Ys(st);
+            if (st > 0 && P.new_f[st])
+            {
+              for (int32_t i = 0; i < S; ++i)
+              {
+                double v = y[i];
+                for (int32_t j = 0; j < st; ++j)
+                  v += P.a[sc + j] * K(j)[i];
+                Yst[i] = v;
+              }
+              reaction_rates<1>(M, kk, Yst, scr, 0);
+              forcing_gather<1>(M, scr, Fc, 0);
+              fc_is_src = true;
+            }
+            else
+              for (int32_t i = 0; i < S; ++i)
+                Yst[i] = y[i];
+            double coh[kMaxAdjStages];
+            for (int32_t j = 0; j < st; ++j)
+              coh[j] = P.c[sc + j] / H;
+            Strided Ks = K(st);
             for (int32_t i = 0; i < S; ++i)
             {
-              double v = y[i];
+              double v = fc_is_src ? Fc[i] : F0[i];
               for (int32_t j = 0; j < st; ++j)
-                v += P.a[sc + j] * K(j)[i];
-              Yst[i] = v;
+                v += coh[j] * K(j)[i];
+              Ks[i] = v;
             }
-            reaction_rates<1>(M, kk, Yst, scr, 0);
-            forcing_gather<1>(M, scr, Fc, 0);
-            fc_is_src = true;
+            solve_lower<1>(M.fwd_s, LU, Ks, 0);
+            solve_upper<1>(M.bwd_s, LU, Ks, 0);
           }
-          else
-            for (int32_t i = 0; i < S; ++i)
-              Yst[i] = y[i];
-          double coh[kMaxAdjStages];
-          for (int32_t j = 0; j < st; ++j)
-            coh[j] = P.c[sc + j] / H;
-          Strided Ks = K(st);
-          for (int32_t i = 0; i < S; ++i)
-          {
-            double v = fc_is_src ? Fc[i] : F0[i];
-            for (int32_t j = 0; j < st; ++j)
-              v += coh[j] * K(j)[i];
-            Ks[i] = v;
-          }
-          solve_lower<1>(M.fwd_s, LU, Ks, 0);
-          solve_upper<1>(M.bwd_s, LU, Ks, 0);
         }
         if (n == A.n_ckpt[cell] - 1)
           for (int32_t i = 0; i < S; ++i)
@@ -759,6 +790,7 @@ namespace micmb
     A.ybar_final = st.adj_ybar.as<double>();
     A.ckpt_y = st.adj_ckpt_y.as<double>();
     A.ckpt_h = st.adj_ckpt_h.as<double>();
+    A.ckpt_k = st.adj_ckpt_k.p ? st.adj_ckpt_k.as<double>() : nullptr;
     A.n_ckpt = st.accepted.as<int32_t>();
     A.ybar0 = st.adj_ybar.as<double>();
     A.kbar = st.adj_kbar_cells.as<double>();

@@ -875,10 +875,26 @@ extern "C"
         st.adj_y0 = DeviceMemory(var_bytes);
         st.adj_ybar = DeviceMemory(var_bytes);
       }
-      if (!st.adj_ckpt_y.p || st.adj_ckpt_capacity < ck)
+      // The adjoint runs on the one-cell-per-thread kernels whatever fused
+      // configuration the forward solves use: that forward also stores each
+      // accepted step's stage vectors, so the backward sweep rebuilds only the
+      // LU factor.
+      const micmb_fused_config tuned = solver->fused;
+      solver->fused = micmb_fused_config{ 0, 0, 0, 0, 2 };
+      struct Restore
       {
+        micmb_solver* s;
+        micmb_fused_config c;
+        ~Restore() { s->fused = c; }
+      } restore{ solver, tuned };
+      const bool store_k = true;
+      if (!st.adj_ckpt_y.p || st.adj_ckpt_capacity < ck || (store_k && !st.adj_ckpt_k.p))
+      {
+        st.adj_ckpt_k = DeviceMemory();
         st.adj_ckpt_y = DeviceMemory(sizeof(double) * (size_t)std::max<int64_t>(ck, 1));
         st.adj_ckpt_h = DeviceMemory(sizeof(double) * (size_t)std::max<int64_t>((int64_t)max_checkpoints * n, 1));
+        if (store_k)
+          st.adj_ckpt_k = DeviceMemory(sizeof(double) * (size_t)std::max<int64_t>(ck * solver->params.stages, 1));
         st.adj_ckpt_capacity = ck;
       }
       if (!st.adj_kbar_cells.p || st.adj_kbar_cells.bytes < sizeof(double) * (size_t)std::max<int64_t>(n * m.R, 1))
@@ -893,6 +909,7 @@ extern "C"
       adj.variables_out = st.variables.as<double>();
       adj.ckpt_y = st.adj_ckpt_y.as<double>();
       adj.ckpt_h = st.adj_ckpt_h.as<double>();
+      adj.ckpt_k = store_k ? st.adj_ckpt_k.as<double>() : nullptr;
       adj.max_ckpt = max_checkpoints;
       SolveFused(*solver, st, dt, stats, nullptr, nullptr, &adj);
       LaunchAdjoint(*solver, st, max_checkpoints);

@@ -3,6 +3,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <fstream>
 #include <sstream>
 #include <string>
@@ -145,31 +146,62 @@ extern "C"
       MICMB_CUDA(cudaEventCreate(&e0));
       MICMB_CUDA(cudaEventCreate(&e1));
       const micmb_fused_config before = solver->fused;
-      double best_rate = -1.0;
+      const bool verbose = std::getenv("MICMB_AUTOTUNE_VERBOSE") != nullptr;
+      // cells per second of one configuration over the first `cells` cells (best of `reps`)
+      auto rate_of = [&](const micmb_fused_config& c, int64_t cells, int reps) {
+        solver->fused = c;
+        st.solve_limit = cells;
+        float ms_min = -1.0f;
+        for (int rep = 0; rep < reps; ++rep)
+        {
+          MICMB_CUDA(cudaMemcpyAsync(st.variables.p, saved.p, st.variables.bytes, cudaMemcpyDeviceToDevice,
+                                     st.stream));
+          MICMB_CUDA(cudaEventRecord(e0, st.stream));
+          SolveFused(*solver, st, dt, nullptr, nullptr, nullptr, nullptr);
+          MICMB_CUDA(cudaEventRecord(e1, st.stream));
+          CheckFusedError(st);
+          float ms = 0.0f;
+          MICMB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          ms_min = (ms_min < 0.0f || ms < ms_min) ? ms : ms_min;
+        }
+        const double rate = 1e3 * (double)cells / std::max(ms_min, 1e-3f);
+        if (verbose)
+          std::fprintf(stderr, "micmb_autotune: variant %d cells_per_cta %d lu_in_shared %d ring_slots %d "
+                               "ctas_per_sm %d: %lld cells in %.3f ms -> %.0f cells/s\n",
+                       c.variant, c.cells_per_cta, c.lu_in_shared, c.ring_slots, c.ctas_per_sm, (long long)cells,
+                       ms_min, rate);
+        return rate;
+      };
       try
       {
+        // stage 1: every candidate on a short trial, best configuration of each variant
+        micmb_fused_config best_of[3];
+        double rate_of_best[3] = { -1.0, -1.0, -1.0 };
         for (const auto& c : candidates)
         {
-          solver->fused = c;
-          st.solve_limit = trial_cells(c);
-          float ms_min = -1.0f;
-          for (int rep = 0; rep < 2; ++rep)
+          const double r = rate_of(c, trial_cells(c), 2);
+          if (r > rate_of_best[c.variant])
           {
-            MICMB_CUDA(cudaMemcpyAsync(st.variables.p, saved.p, st.variables.bytes, cudaMemcpyDeviceToDevice,
-                                       st.stream));
-            MICMB_CUDA(cudaEventRecord(e0, st.stream));
-            SolveFused(*solver, st, dt, nullptr, nullptr, nullptr, nullptr);
-            MICMB_CUDA(cudaEventRecord(e1, st.stream));
-            CheckFusedError(st);
-            float ms = 0.0f;
-            MICMB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            ms_min = (ms_min < 0.0f || ms < ms_min) ? ms : ms_min;
+            rate_of_best[c.variant] = r;
+            best_of[c.variant] = c;
           }
-          const double rate = (double)st.solve_limit / std::max(ms_min, 1e-3f);
-          if (rate > best_rate)
+        }
+        // stage 2: the variants' winners on the state itself (up to 2^20 cells).  Cells
+        // take very different step counts, so how long the last cells keep the GPU
+        // busy depends on how many cells each resident warp or thread gets; a short
+        // trial cannot show that for the thread-per-cell variant.
+        const double lead = std::max(rate_of_best[0], std::max(rate_of_best[1], rate_of_best[2]));
+        const int64_t full = std::min<int64_t>(st.n_cells, (int64_t)1 << 20);
+        double best_rate = -1.0;
+        for (int v = 0; v < 3; ++v)
+        {
+          if (rate_of_best[v] < 0.0 || (v == 1 && rate_of_best[v] < 0.5 * lead))
+            continue;
+          const double r = rate_of(best_of[v], full, 1);
+          if (r > best_rate)
           {
-            best_rate = rate;
-            best = c;
+            best_rate = r;
+            best = best_of[v];
           }
         }
       }

@@ -19,9 +19,10 @@ namespace micmb
   namespace
   {
     constexpr int kThreadsPerBlock = 128;
-    // no register cap: at 96 registers (20 resident warps per SM) the kernel runs
-    // faster than capped at 64 (32 warps), where it spills
-    constexpr int kMinBlocks = 1;
+    // five blocks (20 warps) per SM: about 96 registers per thread.  Fewer blocks
+    // let the compiler take 180 registers (8 warps per SM, half the speed);
+    // eight blocks cap it at 64 and it spills (a few percent slower)
+    constexpr int kMinBlocks = 5;
 
     __device__ __forceinline__ size_t cell_base(int64_t c, int32_t L, int32_t ncol)
     {
@@ -220,6 +221,13 @@ namespace micmb
             double* dst = A.ckpt_y + ((size_t)cell * A.max_ckpt + n_ckpt) * S;
             for (int32_t i = 0; i < S; ++i)
               dst[i] = Y[i];
+            if (A.ckpt_k)
+            {
+              double* kd = A.ckpt_k + ((size_t)cell * A.max_ckpt + n_ckpt) * (size_t)P.stages * S;
+              for (int32_t st = 0; st < P.stages; ++st)
+                for (int32_t i = 0; i < S; ++i)
+                  kd[(size_t)st * S + i] = Kv(st)[i];
+            }
             A.ckpt_h[(size_t)cell * A.max_ckpt + n_ckpt] = h_used;
             ++n_ckpt;
           }

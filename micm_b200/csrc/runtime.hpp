@@ -78,6 +78,8 @@ namespace micmb
     // adjoint checkpoints (null for a plain forward solve)
     double* ckpt_y;              // [n_cells][max_ckpt][S]
     double* ckpt_h;              // [n_cells][max_ckpt]
+    double* ckpt_k;              // [n_cells][max_ckpt][stages][S] stage vectors of each accepted step,
+                                 // or null (one-cell-per-thread variant only)
     int32_t max_ckpt;
   };
 }  // namespace micmb
@@ -130,7 +132,7 @@ struct micmb_state
   double graph_dt = 0.0;
   micmb_fused_config graph_config{};
   // adjoint working set (allocated on first use)
-  micmb::DeviceMemory adj_y0, adj_ybar, adj_ckpt_y, adj_ckpt_h, adj_kbar_cells, adj_kbar;
+  micmb::DeviceMemory adj_y0, adj_ybar, adj_ckpt_y, adj_ckpt_h, adj_ckpt_k, adj_kbar_cells, adj_kbar;
   int64_t adj_ckpt_capacity = 0;  // doubles in adj_ckpt_y
   double dt_for_launch = 0.0;
 
