@@ -812,7 +812,7 @@ namespace micmb
   void LaunchAdjoint(micmb_solver& s, micmb_state& st, int32_t max_ckpt)
   {
     const auto& m = *s.mech;
-    if (s.fused.variant == 2)
+    if (s.fused.variant != 1)
     {
       LaunchAdjointThread(s, st, max_ckpt);
       return;

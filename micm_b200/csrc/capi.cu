@@ -875,12 +875,12 @@ extern "C"
         st.adj_y0 = DeviceMemory(var_bytes);
         st.adj_ybar = DeviceMemory(var_bytes);
       }
-      // The adjoint runs on the one-cell-per-thread kernels whatever fused
-      // configuration the forward solves use: that forward also stores each
-      // accepted step's stage vectors, so the backward sweep rebuilds only the
-      // LU factor.
+      // The forward pass (streamed or thread variant) stores each accepted
+      // step's stage vectors beside the checkpoint, so the backward sweep (one
+      // cell per thread) rebuilds only the LU factor.
       const micmb_fused_config tuned = solver->fused;
-      solver->fused = micmb_fused_config{ 0, 0, 0, 0, 2 };
+      if (tuned.variant == 1)  // the direct variant keeps no stage vectors: use the thread variant
+        solver->fused = micmb_fused_config{ 0, 0, 0, 0, 2 };
       struct Restore
       {
         micmb_solver* s;

@@ -439,6 +439,13 @@ namespace micmb
               double* dst = A.ckpt_y + ((size_t)wc.cell * A.max_ckpt + wc.n_ckpt) * S;
               for (int32_t i = lane; i < S; i += kWarp)
                 dst[i] = Y[i];
+              if (A.ckpt_k)
+              {
+                double* kd = A.ckpt_k + ((size_t)wc.cell * A.max_ckpt + wc.n_ckpt) * (size_t)P.stages * S;
+                for (int32_t st = 0; st < P.stages; ++st)
+                  for (int32_t i = lane; i < S; i += kWarp)
+                    kd[(size_t)st * S + i] = K[(size_t)st * VS + i];
+              }
               if (lane == 0)
                 A.ckpt_h[(size_t)wc.cell * A.max_ckpt + wc.n_ckpt] = h_used;
               ++wc.n_ckpt;
