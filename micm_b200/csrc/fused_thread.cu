@@ -18,11 +18,10 @@ namespace micmb
 {
   namespace
   {
+    // 128-thread blocks; with no minimum-blocks hint the compiler settles on
+    // 96 registers (20 resident warps per SM).  Hints of 5 or 8 blocks per SM
+    // measured 10 % slower, a hint of 1 block lets it take 180 registers.
     constexpr int kThreadsPerBlock = 128;
-    // five blocks (20 warps) per SM: about 96 registers per thread.  Fewer blocks
-    // let the compiler take 180 registers (8 warps per SM, half the speed);
-    // eight blocks cap it at 64 and it spills (a few percent slower)
-    constexpr int kMinBlocks = 5;
 
     __device__ __forceinline__ size_t cell_base(int64_t c, int32_t L, int32_t ncol)
     {
@@ -69,7 +68,7 @@ namespace micmb
         cc.function_calls += P.new_f[s] ? 1 : 0;
     }
 
-    __global__ void __launch_bounds__(kThreadsPerBlock, kMinBlocks)
+    __global__ void __launch_bounds__(kThreadsPerBlock)
         k_fused_thread(DevMech M, DevParams P, StepBounds B, FusedArgs A, double* ws, ThreadLayout T)
     {
       const int lane = threadIdx.x & 31;
