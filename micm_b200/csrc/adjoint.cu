@@ -59,6 +59,7 @@ namespace micmb
       double* lu_global;             // per-warp LU slots (nullptr: LU in shared memory)
       int64_t lu_slot_stride;
       int32_t* next_cell;
+      const int32_t* order;          // cells in decreasing step count (thread kernel), or null
     };
 
     struct AdjLayout
@@ -554,12 +555,13 @@ namespace micmb
       auto claim = [&]() {
         for (;;)
         {
-          cell = atomicAdd(A.next_cell, 1);
-          if (cell >= A.n_cells)
+          const int64_t k = atomicAdd(A.next_cell, 1);
+          if (k >= A.n_cells)
           {
             n = -1;
             return;
           }
+          cell = A.order ? A.order[k] : k;
           const size_t by = cell_base(cell, L, S);
           const size_t bk = cell_base(cell, L, R);
           for (int32_t r = 0; r < R; ++r)
@@ -743,6 +745,35 @@ namespace micmb
       }
     }
 
+    // Cells in decreasing order of accepted steps (counting sort on the step
+    // count): the backward sweep takes the longest cells first, so the last
+    // cells finish together, and the 32 cells of a warp have similar counts.
+    __global__ void k_step_histogram(const int32_t* n_ckpt, int64_t n, int32_t max_ckpt, int32_t* bins)
+    {
+      const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+      if (c < n)
+        atomicAdd(bins + (max_ckpt - min(max(n_ckpt[c], 0), max_ckpt)), 1);
+    }
+
+    __global__ void k_step_offsets(int32_t* bins, int32_t n_bins)
+    {
+      int32_t run = 0;
+      for (int32_t b = 0; b < n_bins; ++b)
+      {
+        const int32_t v = bins[b];
+        bins[b] = run;
+        run += v;
+      }
+    }
+
+    __global__ void k_step_scatter(const int32_t* n_ckpt, int64_t n, int32_t max_ckpt, int32_t* cursor,
+                                   int32_t* order)
+    {
+      const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+      if (c < n)
+        order[atomicAdd(cursor + (max_ckpt - min(max(n_ckpt[c], 0), max_ckpt)), 1)] = (int32_t)c;
+    }
+
     // out[r] = sum over cells of kbar[cell][r], in a fixed order (deterministic)
     __global__ void k_sum_cells(const double* kbar, int64_t n_cells, int32_t R, double* out)
     {
@@ -799,6 +830,19 @@ namespace micmb
     MICMB_CUDA(cudaMemsetAsync(cbase + 8, 0, 8, st.stream));
     if (n > 0)
     {
+      const int32_t n_bins = max_ckpt + 1;
+      const size_t need = sizeof(int32_t) * ((size_t)n + (size_t)n_bins);
+      if (!st.adj_order.p || st.adj_order.bytes < need)
+        st.adj_order = DeviceMemory(need);
+      int32_t* order = st.adj_order.as<int32_t>();
+      int32_t* bins = order + n;
+      const unsigned blocks = (unsigned)((n + 255) / 256);
+      MICMB_CUDA(cudaMemsetAsync(bins, 0, sizeof(int32_t) * n_bins, st.stream));
+      k_step_histogram<<<blocks, 256, 0, st.stream>>>(A.n_ckpt, n, max_ckpt, bins);
+      k_step_offsets<<<1, 1, 0, st.stream>>>(bins, n_bins);
+      k_step_scatter<<<blocks, 256, 0, st.stream>>>(A.n_ckpt, n, max_ckpt, bins, order);
+      MICMB_CUDA(cudaGetLastError());
+      A.order = order;
       k_adjoint_thread<<<(unsigned)grid, 128, 0, st.stream>>>(s.dev, s.params, A, T, st.thread_ws.as<double>());
       MICMB_CUDA(cudaGetLastError());
     }

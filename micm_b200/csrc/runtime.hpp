@@ -133,6 +133,7 @@ struct micmb_state
   micmb_fused_config graph_config{};
   // adjoint working set (allocated on first use)
   micmb::DeviceMemory adj_y0, adj_ybar, adj_ckpt_y, adj_ckpt_h, adj_ckpt_k, adj_kbar_cells, adj_kbar;
+  micmb::DeviceMemory adj_order;  // backward sweep: cells by decreasing step count, then bins
   int64_t adj_ckpt_capacity = 0;  // doubles in adj_ckpt_y
   double dt_for_launch = 0.0;
 
