@@ -8,6 +8,7 @@ copy) and solves every cell; inputs (1.8 GB state + 3.7 GB rate constants)
 exceed the 126 MB L2, so no flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py --workload c600     # 600 species / 1,500 reactions, 262,144 cells
 
 N > 1 runs under torchrun: each rank solves its own 1M-cell shard (weak
 scaling; cells are independent, no collective on the data path).
@@ -29,8 +30,25 @@ sys.path.insert(0, ROOT)
 
 METRIC = "cell-solves/s @1M cells, FP64 rtol1e-6 (fused vs plain); adjoint/forward time"
 UNIT = "cell-solves/s"
-CONFIG_NAME = "c210_uneven"
 KERNEL_OF_VARIANT = {0: "k_fused_stream", 1: "k_fused", 2: "k_fused_thread"}
+# workload -> cells per GPU, description, the adjoint timing that goes with it
+# (configuration, cells, checkpoints per cell), host-CPU sample, ncu capture of
+# the fused kernel whose DRAM bytes per cell-solve scale the traffic figure
+WORKLOADS = {
+    "c210_uneven": dict(cells=1048576, cpu_sample=65536,
+                        text="210 species, 440 reactions, {cells} cells per GPU, half night, T~U(200,310) K, "
+                             "4-stage Rosenbrock, dt=600 s, per-cell step control, fused persistent kernel",
+                        l2="inputs exceed L2 (1.8 GB state + 3.7 GB rate constants); no flush",
+                        adjoint=("c60_adjoint", 131072, 256),
+                        profile="k_fused_thread_c210_65536cells.md"),
+    "c600": dict(cells=262144, cpu_sample=16384,
+                 text="600 species, 1,500 reactions, {cells} cells per GPU, 4-stage Rosenbrock, dt=600 s, "
+                      "per-cell step control, fused persistent kernel (LU factor of 11,304 entries per cell, "
+                      "beyond shared memory)",
+                 l2="inputs exceed L2 (1.3 GB state + 3.1 GB rate constants); no flush",
+                 adjoint=("c600", 262144, 160),
+                 profile="k_fused_thread_c600_16384cells.md"),
+}
 
 
 def parse():
@@ -39,15 +57,24 @@ def parse():
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--cells", type=int, default=1048576)
-    ap.add_argument("--plain-cells", type=int, default=1048576,
-                    help="cells per GPU for the plain-method comparison (0 = skip)")
+    ap.add_argument("--workload", default="c210_uneven", choices=sorted(WORKLOADS))
+    ap.add_argument("--cells", type=int, default=None, help="cells per GPU (default: the workload's)")
+    ap.add_argument("--plain-cells", type=int, default=None,
+                    help="cells per GPU for the plain-method comparison (0 = skip; default: --cells)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward timing")
     ap.add_argument("--no-autotune", action="store_true",
                     help="fixed fused configuration (one cell per thread) instead of the autotuner")
-    ap.add_argument("--cpu-sample", type=int, default=65536, help="cells timed on the host CPU")
+    ap.add_argument("--cpu-sample", type=int, default=None, help="cells timed on the host CPU")
     ap.add_argument("--no-cpu", action="store_true")
-    return ap.parse_args()
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    if args.cells is None:
+        args.cells = w["cells"]
+    if args.plain_cells is None:
+        args.plain_cells = args.cells
+    if args.cpu_sample is None:
+        args.cpu_sample = w["cpu_sample"]
+    return args
 
 
 class ClockSampler:
@@ -113,9 +140,9 @@ def job_throughput(cells_per_rank: int, world: int, steps: int, seconds: float) 
     return cells_per_rank * world * steps / seconds
 
 
-def workload(cells: int, rank: int = 0):
+def workload(name: str, cells: int, rank: int = 0):
     from micm_b200 import synthetic
-    cfg = synthetic.CONFIGS[CONFIG_NAME]
+    cfg = synthetic.CONFIGS[name]
     mech = cfg["mech"]()
     inputs = synthetic.cell_inputs(mech, cells, cfg["seed"] + 1000 * rank, **cfg["inputs"])
     return cfg, mech, inputs
@@ -142,7 +169,7 @@ def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    cfg, mech, inputs = workload(min(args.cells, args.cpu_sample * max(1, args.steps + args.warmup)))
+    cfg, mech, inputs = workload(args.workload, min(args.cells, args.cpu_sample * max(1, args.steps + args.warmup)))
     import oracle
     if not oracle.reference_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmicm_ref.so was not built"}))
@@ -163,8 +190,9 @@ def run_reference_arm(args):
             "warmup": args.warmup, "ms_per_step": 1000 * t / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "impl": "reference",
-            "config": {"workload": f"{CONFIG_NAME}: 210 species, 440 reactions, 4-stage Rosenbrock, dt=600 s, "
-                                   f"per-cell step control; each step a {n}-cell sample",
+            "config": {"workload": f"{args.workload}: "
+                                   + WORKLOADS[args.workload]["text"].format(cells=args.cells)
+                                   + f"; each step a {n}-cell sample on the host",
                        "cells_per_step": n},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                              "sample": f"{n} cells per step, 1-cell micm States over {threads} threads"},
@@ -217,9 +245,9 @@ def hbm_peak():
         return 6650.0, "fallback 6.65 TB/s"
 
 
-def measured_traffic(cells):
+def measured_traffic(profile, cells):
     """DRAM bytes of one fused launch over `cells` cells, scaled from the committed capture."""
-    path = os.path.join(ROOT, "profiles", "k_fused_thread_c210_65536cells.md")
+    path = os.path.join(ROOT, "profiles", profile)
     try:
         with open(path) as f:
             for line in f:
@@ -251,19 +279,23 @@ def fp64_peak():
     return p.multi_processor_count * 64 * 2 * mhz * 1e6 / 1e12
 
 
-def adjoint_ratio(torch, rank):
-    """Adjoint/forward time on the adjoint configuration (60 species, 131,072 cells)."""
+def adjoint_ratio(torch, rank, name, n, max_checkpoints, fused_config=None):
+    """Adjoint/forward time of `n` cells of configuration `name` (autotuned
+    unless the fused configuration is given)."""
     from micm_b200 import Solver, synthetic
-    cfg = synthetic.CONFIGS["c60_adjoint"]
+    cfg = synthetic.CONFIGS[name]
     mech = cfg["mech"]()
-    n = cfg["cells"]
     inputs = synthetic.cell_inputs(mech, n, cfg["seed"] + 1000 * rank, **cfg["inputs"])
     solver = Solver(mech, cfg["stages"], vector_length=128)
     st = solver.get_state(n)
     st.set_inputs(inputs)
     st.sync_inputs_to_device()
     solver.update_state_parameters(st)
-    tuned = solver.autotune(cfg["dt"], st)
+    if fused_config:
+        solver.set_fused_config(**fused_config)
+        tuned = solver.get_fused_config()
+    else:
+        tuned = solver.autotune(cfg["dt"], st)
     rng = np.random.default_rng(cfg["seed"])
     target = rng.random(n) * 1e-9
     cols = solver.compiled.species_columns
@@ -284,7 +316,7 @@ def adjoint_ratio(torch, rank):
         solver.update_state_parameters(st)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        solver.solve_adjoint(cfg["dt"], st, g, max_checkpoints=256)
+        solver.solve_adjoint(cfg["dt"], st, g, max_checkpoints=max_checkpoints)
         torch.cuda.synchronize()
         return time.perf_counter() - t0
 
@@ -295,7 +327,8 @@ def adjoint_ratio(torch, rank):
     st.set_inputs(inputs)
     adjoint(y_final)
     ta = adjoint(y_final)
-    return {"config": "c60_adjoint: 60 species, 120 reactions, 131,072 cells, 4-stage, dt=3600 s; "
+    return {"config": f"{name}: {mech.n_species} species, {mech.n_reactions} reactions, {n} cells, "
+                      f"{cfg['stages']}-stage, dt={cfg['dt']:g} s, at most {max_checkpoints} accepted steps per cell; "
                       "loss = sum_c (y_c[0] - target_c)^2; gradients w.r.t. all y0 and all log k",
             "forward_ms": 1000 * tf, "adjoint_ms": 1000 * ta, "adjoint_over_forward": ta / tf,
             "accepted_per_cell": res.stats["accepted"] / n, "fused_config": tuned,
@@ -323,7 +356,8 @@ def main():
     from micm_b200._native import check, lib
     from micm_b200.mechanism import to_vector_layout
 
-    cfg, mech, inputs = workload(args.cells, rank)
+    W = WORKLOADS[args.workload]
+    cfg, mech, inputs = workload(args.workload, args.cells, rank)
     L = 128
     solver = Solver(mech, cfg["stages"], vector_length=L)
     state = solver.get_state(args.cells)
@@ -387,7 +421,7 @@ def main():
     peak_gbs, peak_src = hbm_peak()
     units = flops_per_solve_unit(mech, solver, cfg["stages"])
     flops = solve_flops(units, totals) / args.steps
-    traffic = measured_traffic(args.cells)
+    traffic = measured_traffic(W["profile"], args.cells)
 
     # e2e: the public API with host buffers every step (H2D inputs, D2H results)
     h_vars = torch.from_numpy(y0_host).pin_memory().numpy()
@@ -421,7 +455,7 @@ def main():
         y_view.copy_(y_dev)
         pstate = state if pc == args.cells else None
         if pstate is None:
-            _, _, pin = workload(pc, rank)
+            _, _, pin = workload(args.workload, pc, rank)
             pstate = solver.get_state(pc)
             pstate.set_inputs(pin)
             pstate.sync_inputs_to_device()
@@ -444,7 +478,16 @@ def main():
                               "note": "algorithmic bytes of the per-stage kernels over the solve's wall time "
                                       "(launches and host synchronisation included)"}}
 
-    adj = adjoint_ratio(torch, rank) if not args.no_adjoint else None
+    # the solve states are released before the adjoint timing, which sizes its
+    # checkpoint chunks from the free device memory
+    pview = p0 = pstate = y_view = y_dev = None
+    state = None
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    adj = None
+    if not args.no_adjoint:
+        same = W["adjoint"][0] == args.workload            # same mechanism: keep the configuration tuned above
+        adj = adjoint_ratio(torch, rank, *W["adjoint"], fused_config=tuned if same else None)
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -456,11 +499,9 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": f"{CONFIG_NAME}: 210 species, 440 reactions, {args.cells} cells per GPU, "
-                                   "half night, T~U(200,310) K, 4-stage Rosenbrock, dt=600 s, per-cell step control, "
-                                   "fused persistent kernel",
+            "config": {"workload": f"{args.workload}: " + W["text"].format(cells=args.cells),
                        "cells_per_gpu": args.cells, "vector_length": L, "fused_config": tuned,
-                       "l2": "inputs exceed L2 (1.8 GB state + 3.7 GB rate constants); no flush",
+                       "l2": W["l2"],
                        "lu_nnz": info["jacobian_nnz"], "lu_updates": info["lu_updates"],
                        "attempts_per_cell": attempts_per_cell, "accepted_per_cell": accepted_per_cell},
             "clocks": clocks.summary(),
@@ -473,8 +514,8 @@ def main():
                          "kernel": KERNEL_OF_VARIANT.get(tuned["variant"], "fused") + " (one launch per step)",
                          "algorithmic_bytes_per_launch": algo_bytes, "kernel_ms_per_launch": kernel_ms / args.steps,
                          "peak_source": peak_src,
-                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of a 65,536-cell capture "
-                                           "(profiles/k_fused_thread_c210_65536cells.md) scaled by cells",
+                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of the capture in "
+                                           f"profiles/{W['profile']}, scaled by cells",
                          "fp64": {"achieved_tflops": flops / kernel_s / 1e12, "peak_tflops": fp64_peak(),
                                   "frac": flops / kernel_s / 1e12 / fp64_peak(), "flops_per_launch": flops,
                                   "peak_source": "nominal (SMs x 64 FMA/clk x 2 x max SM clock)"}},

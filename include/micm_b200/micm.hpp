@@ -26,6 +26,7 @@
 #include <array>
 #include <cmath>
 #include <cstddef>
+#include <cstdint>
 #include <iomanip>
 #include <iostream>
 #include <limits>
@@ -959,6 +960,13 @@ namespace micm
     void SolveRepeated(Real time_step, CudaState<L>& state, int32_t n_repeats)
     {
       detail::Check(micmb_solve_graph(solver_.get(), state.handle_.get(), time_step, n_repeats));
+    }
+
+    // Device bytes SolveAdjoint may hold in checkpoints (0: 80 % of the free
+    // device memory); cells are swept in chunks that fit.
+    void SetAdjointMemoryLimit(std::int64_t bytes)
+    {
+      detail::Check(micmb_set_adjoint_memory_limit(solver_.get(), bytes));
     }
 
     // Discrete adjoint of the accepted steps of a per-cell solve (no micm

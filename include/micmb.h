@@ -308,10 +308,22 @@ int micmb_solve_graph(micmb_solver* solver, micmb_state* state, double dt, int32
  *                   may be NULL
  * Buffers are host pointers.  The state's variables hold the final values
  * afterwards, as after micmb_solve.  max_checkpoints bounds accepted steps
- * per cell (cells beyond it report MICMB_SOLVER_CONVERGENCE_EXCEEDED_MAX_STEPS). */
+ * per cell (cells beyond it report MICMB_SOLVER_CONVERGENCE_EXCEEDED_MAX_STEPS).
+ * Checkpoints take max_checkpoints * (n_species + 1) doubles per cell, plus
+ * max_checkpoints * stages * n_species when the accepted steps' stage vectors
+ * are kept.  Cells are solved and swept in chunks (multiples of the vector
+ * length) that fit the solver's adjoint memory limit; stage vectors are kept
+ * unless that would make a chunk smaller than the cells the forward kernel
+ * keeps resident, in which case the sweep recomputes them.  Results do not
+ * depend on the chunking. */
 int micmb_solve_adjoint(micmb_solver* solver, micmb_state* state, double dt,
                         const double* dloss_dy_final, double* dloss_dy0, double* dloss_dlogk,
                         int32_t max_checkpoints, micmb_solver_stats* stats);
+/* Device bytes micmb_solve_adjoint may hold in checkpoints (0, the default:
+ * 80 % of the device memory free at the call, counting checkpoints it already
+ * holds).  A limit below one vector-length group of cells makes
+ * micmb_solve_adjoint return MICMB_ERR_OUT_OF_MEMORY. */
+int micmb_set_adjoint_memory_limit(micmb_solver* solver, int64_t bytes);
 
 /* ---- single-stage entry points (per-kernel parity with micm's drivers) ---- */
 /* ProcessSet::AddForcingTerms (process_set.hpp:524-590; src/process/process_set.cu:10-74):

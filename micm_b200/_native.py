@@ -60,6 +60,7 @@ def lib():
             "micmb_autotune": [vp, vp, C.c_double, C.c_char_p, C.POINTER(FusedConfig)],
             "micmb_solve_graph": [vp, vp, C.c_double, C.c_int32],
             "micmb_solve_adjoint": [vp, vp, C.c_double, f64p, f64p, f64p, C.c_int32, C.POINTER(SolverStats)],
+            "micmb_set_adjoint_memory_limit": [vp, C.c_int64],
             "micmb_add_forcing_terms": [vp, vp],
             "micmb_subtract_jacobian_terms": [vp, vp],
             "micmb_alpha_minus_jacobian": [vp, vp, C.c_double],

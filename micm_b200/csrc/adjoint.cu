@@ -795,8 +795,36 @@ namespace micmb
     }
   }  // namespace
 
+  namespace
+  {
+    // arguments for cells [begin, begin + count) of the state; begin is a
+    // multiple of L, so every vector-layout array of the chunk starts at
+    // begin * columns and is laid out like a state of `count` cells.  The
+    // checkpoints hold the chunk's cells only.
+    AdjArgs ChunkArgs(micmb_solver& s, micmb_state& st, int32_t max_ckpt, int64_t begin, int64_t count)
+    {
+      const auto& m = *s.mech;
+      AdjArgs A{};
+      A.n_cells = count;
+      A.L = st.L;
+      A.max_ckpt = max_ckpt;
+      A.rate_constants = st.rate_constants.as<double>() + (size_t)begin * m.R;
+      A.y0 = st.adj_y0.as<double>() + (size_t)begin * m.S;
+      A.ybar_final = st.adj_ybar.as<double>() + (size_t)begin * m.S;
+      A.ckpt_y = st.adj_ckpt_y.as<double>();
+      A.ckpt_h = st.adj_ckpt_h.as<double>();
+      A.ckpt_k = st.adj_ckpt_k.p ? st.adj_ckpt_k.as<double>() : nullptr;
+      A.n_ckpt = st.accepted.as<int32_t>() + begin;
+      A.ybar0 = st.adj_ybar.as<double>() + (size_t)begin * m.S;  // overwritten cell by cell after its last read
+      A.kbar = st.adj_kbar_cells.as<double>() + (size_t)begin * m.R;
+      char* cbase = st.counters.as<char>();
+      A.next_cell = reinterpret_cast<int32_t*>(cbase + 8);
+      return A;
+    }
+  }  // namespace
+
   // one cell per thread: per-thread working sets in global memory, no atomics
-  void LaunchAdjointThread(micmb_solver& s, micmb_state& st, int32_t max_ckpt)
+  void LaunchAdjointThread(micmb_solver& s, micmb_state& st, int32_t max_ckpt, int64_t begin, int64_t count)
   {
     const auto& m = *s.mech;
     if (s.params.stages > kMaxAdjStages)
@@ -806,28 +834,14 @@ namespace micmb
     MICMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adjoint_thread, 128, 0));
     if (per_sm < 1)
       throw Error(MICMB_ERR_UNSUPPORTED, "adjoint kernel cannot be resident");
-    const int64_t n = st.n_cells;
+    const int64_t n = count;
     int64_t grid = (int64_t)per_sm * s.sm_count;
     grid = std::max<int64_t>(1, std::min<int64_t>(grid, (n + 127) / 128));
     const int64_t doubles = grid * 128 * (int64_t)T.per_slot;
     if (!st.thread_ws.p || st.thread_ws.bytes < (size_t)doubles * sizeof(double))
       st.thread_ws = DeviceMemory((size_t)doubles * sizeof(double));
-    AdjArgs A{};
-    A.n_cells = n;
-    A.L = st.L;
-    A.max_ckpt = max_ckpt;
-    A.rate_constants = st.rate_constants.as<double>();
-    A.y0 = st.adj_y0.as<double>();
-    A.ybar_final = st.adj_ybar.as<double>();
-    A.ckpt_y = st.adj_ckpt_y.as<double>();
-    A.ckpt_h = st.adj_ckpt_h.as<double>();
-    A.ckpt_k = st.adj_ckpt_k.p ? st.adj_ckpt_k.as<double>() : nullptr;
-    A.n_ckpt = st.accepted.as<int32_t>();
-    A.ybar0 = st.adj_ybar.as<double>();
-    A.kbar = st.adj_kbar_cells.as<double>();
-    char* cbase = st.counters.as<char>();
-    A.next_cell = reinterpret_cast<int32_t*>(cbase + 8);
-    MICMB_CUDA(cudaMemsetAsync(cbase + 8, 0, 8, st.stream));
+    AdjArgs A = ChunkArgs(s, st, max_ckpt, begin, count);
+    MICMB_CUDA(cudaMemsetAsync(A.next_cell, 0, 8, st.stream));
     if (n > 0)
     {
       const int32_t n_bins = max_ckpt + 1;
@@ -846,19 +860,35 @@ namespace micmb
       k_adjoint_thread<<<(unsigned)grid, 128, 0, st.stream>>>(s.dev, s.params, A, T, st.thread_ws.as<double>());
       MICMB_CUDA(cudaGetLastError());
     }
+  }
+
+  int64_t AdjointThreadWorkspaceDoubles(const micmb_solver& s, int64_t n_cells)
+  {
+    const auto& m = *s.mech;
+    const AdjThreadLayout T = MakeAdjThreadLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz);
+    int per_sm = 0;
+    MICMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adjoint_thread, 128, 0));
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((int64_t)per_sm * s.sm_count, (n_cells + 127) / 128));
+    return grid * 128 * (int64_t)T.per_slot;
+  }
+
+  void ReduceAdjointParameters(micmb_solver& s, micmb_state& st)
+  {
+    const auto& m = *s.mech;
     if (m.R > 0)
     {
-      k_sum_cells<<<(unsigned)m.R, 256, 0, st.stream>>>(A.kbar, n, m.R, st.adj_kbar.as<double>());
+      k_sum_cells<<<(unsigned)m.R, 256, 0, st.stream>>>(st.adj_kbar_cells.as<double>(), st.n_cells, m.R,
+                                                         st.adj_kbar.as<double>());
       MICMB_CUDA(cudaGetLastError());
     }
   }
 
-  void LaunchAdjoint(micmb_solver& s, micmb_state& st, int32_t max_ckpt)
+  void LaunchAdjoint(micmb_solver& s, micmb_state& st, int32_t max_ckpt, int64_t begin, int64_t count)
   {
     const auto& m = *s.mech;
     if (s.fused.variant != 1)
     {
-      LaunchAdjointThread(s, st, max_ckpt);
+      LaunchAdjointThread(s, st, max_ckpt, begin, count);
       return;
     }
     if (!s.dev.has_warp)
@@ -882,22 +912,12 @@ namespace micmb
     MICMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adjoint, warps * kWarp, smem));
     if (per_sm < 1)
       throw Error(MICMB_ERR_UNSUPPORTED, "adjoint kernel cannot be resident");
-    const int64_t n = st.n_cells;
+    const int64_t n = count;
     int64_t grid = (int64_t)per_sm * s.sm_count;
     grid = std::max<int64_t>(1, std::min<int64_t>(grid, (n + warps - 1) / warps));
 
-    AdjArgs A{};
-    A.n_cells = n;
-    A.L = st.L;
-    A.max_ckpt = max_ckpt;
-    A.rate_constants = st.rate_constants.as<double>();
-    A.y0 = st.adj_y0.as<double>();
-    A.ybar_final = st.adj_ybar.as<double>();
-    A.ckpt_y = st.adj_ckpt_y.as<double>();
-    A.ckpt_h = st.adj_ckpt_h.as<double>();
-    A.n_ckpt = st.accepted.as<int32_t>();
-    A.ybar0 = st.adj_ybar.as<double>();  // overwritten cell by cell after its last read
-    A.kbar = st.adj_kbar_cells.as<double>();
+    AdjArgs A = ChunkArgs(s, st, max_ckpt, begin, count);
+    A.ckpt_k = nullptr;  // the warp kernel recomputes the stages
     if (!lu_shared)
     {
       const int64_t slots = grid * warps;
@@ -910,17 +930,10 @@ namespace micmb
       A.lu_global = st.lu_slots.as<double>();
       A.lu_slot_stride = stride;
     }
-    char* cbase = st.counters.as<char>();
-    A.next_cell = reinterpret_cast<int32_t*>(cbase + 8);
-    MICMB_CUDA(cudaMemsetAsync(cbase + 8, 0, 8, st.stream));
+    MICMB_CUDA(cudaMemsetAsync(A.next_cell, 0, 8, st.stream));
     if (n > 0)
     {
       k_adjoint<<<(unsigned)grid, warps * kWarp, smem, st.stream>>>(s.dev, s.params, A, W);
-      MICMB_CUDA(cudaGetLastError());
-    }
-    if (m.R > 0)
-    {
-      k_sum_cells<<<(unsigned)m.R, 256, 0, st.stream>>>(A.kbar, n, m.R, st.adj_kbar.as<double>());
       MICMB_CUDA(cudaGetLastError());
     }
   }

@@ -855,6 +855,15 @@ extern "C"
     });
   }
 
+  int micmb_set_adjoint_memory_limit(micmb_solver* solver, int64_t bytes)
+  {
+    return Guard([&] {
+      Need(solver != nullptr, "no solver");
+      Need(bytes >= 0, "memory limit must be >= 0");
+      solver->adjoint_memory_limit = bytes;
+    });
+  }
+
   int micmb_solve_adjoint(micmb_solver* solver, micmb_state* state, double dt, const double* dloss_dy_final,
                           double* dloss_dy0, double* dloss_dlogk, int32_t max_checkpoints,
                           micmb_solver_stats* stats)
@@ -869,7 +878,6 @@ extern "C"
       const auto& m = *solver->mech;
       const int64_t n = st.n_cells;
       const size_t var_bytes = st.variables.bytes;
-      const int64_t ck = (int64_t)max_checkpoints * n * m.S;
       if (!st.adj_y0.p || st.adj_y0.bytes < var_bytes)
       {
         st.adj_y0 = DeviceMemory(var_bytes);
@@ -879,7 +887,9 @@ extern "C"
       // step's stage vectors beside the checkpoint, so the backward sweep (one
       // cell per thread) rebuilds only the LU factor.
       const micmb_fused_config tuned = solver->fused;
-      if (tuned.variant == 1)  // the direct variant keeps no stage vectors: use the thread variant
+      // the direct kernel keeps no stage vectors; it also runs when variant 0 is
+      // configured but the mechanism has no streamed schedule: use the thread variant
+      if (tuned.variant == 1 || (tuned.variant == 0 && !StreamVariantApplies(*solver)))
         solver->fused = micmb_fused_config{ 0, 0, 0, 0, 2 };
       struct Restore
       {
@@ -887,32 +897,114 @@ extern "C"
         micmb_fused_config c;
         ~Restore() { s->fused = c; }
       } restore{ solver, tuned };
-      const bool store_k = true;
-      if (!st.adj_ckpt_y.p || st.adj_ckpt_capacity < ck || (store_k && !st.adj_ckpt_k.p))
-      {
-        st.adj_ckpt_k = DeviceMemory();
-        st.adj_ckpt_y = DeviceMemory(sizeof(double) * (size_t)std::max<int64_t>(ck, 1));
-        st.adj_ckpt_h = DeviceMemory(sizeof(double) * (size_t)std::max<int64_t>((int64_t)max_checkpoints * n, 1));
-        if (store_k)
-          st.adj_ckpt_k = DeviceMemory(sizeof(double) * (size_t)std::max<int64_t>(ck * solver->params.stages, 1));
-        st.adj_ckpt_capacity = ck;
-      }
       if (!st.adj_kbar_cells.p || st.adj_kbar_cells.bytes < sizeof(double) * (size_t)std::max<int64_t>(n * m.R, 1))
       {
         st.adj_kbar_cells = DeviceMemory(sizeof(double) * (size_t)std::max<int64_t>(n * m.R, 1));
         st.adj_kbar = DeviceMemory(sizeof(double) * (size_t)std::max<int32_t>(m.R, 1));
       }
+      if (!st.status.p)
+        st.status = DeviceMemory(sizeof(int32_t) * std::max<int64_t>(n, 1));
+      if (!st.accepted.p)
+        st.accepted = DeviceMemory(sizeof(int32_t) * std::max<int64_t>(n, 1));
+      // per-thread working sets do not shrink with the chunk: size them first
+      const int64_t ws = std::max(FusedThreadWorkspaceDoubles(*solver, n), AdjointThreadWorkspaceDoubles(*solver, n));
+      if (!st.thread_ws.p || st.thread_ws.bytes < (size_t)ws * sizeof(double))
+      {
+        st.thread_ws = DeviceMemory();
+        st.thread_ws = DeviceMemory((size_t)ws * sizeof(double));
+      }
+
+      // Checkpoints take max_checkpoints * (S + 1) doubles per cell, the stored
+      // stage vectors max_checkpoints * stages * S more.  Cells are solved and
+      // swept in chunks (multiples of L) that fit the memory limit; when stored
+      // stages would leave a chunk smaller than the cells the forward kernel
+      // keeps resident, the stages are recomputed in the sweep instead.
+      const int64_t per_cell_y = (int64_t)max_checkpoints * (m.S + 1) * (int64_t)sizeof(double);
+      const int64_t per_cell_k = (int64_t)max_checkpoints * solver->params.stages * m.S * (int64_t)sizeof(double);
+      int64_t budget = solver->adjoint_memory_limit;
+      if (budget <= 0)
+      {
+        size_t free_b = 0, total_b = 0;
+        MICMB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        const size_t held = st.adj_ckpt_y.bytes + st.adj_ckpt_h.bytes + st.adj_ckpt_k.bytes;
+        budget = (int64_t)(0.8 * (double)(free_b + held));
+      }
+      const int64_t L = st.L;
+      // equal chunks (multiples of L) of at most budget / per_cell cells; 0 if one group does not fit
+      auto balanced_chunk = [&](int64_t per_cell) -> int64_t {
+        const int64_t most = budget / per_cell / L * L;
+        if (most < 1 || n < 1)
+          return most < 1 ? 0 : std::max<int64_t>(n, 1);
+        const int64_t parts = (n + most - 1) / most;
+        return std::min<int64_t>(n, ((n + parts - 1) / parts + L - 1) / L * L);
+      };
+      const int64_t busy = std::min<int64_t>(n, FusedThreadResidentCells(*solver));
+      int64_t chunk = balanced_chunk(per_cell_y + per_cell_k);
+      bool store_k = true;
+      if (chunk < busy && balanced_chunk(per_cell_y) > chunk)
+      {
+        chunk = balanced_chunk(per_cell_y);
+        store_k = false;
+      }
+      if (n > 0 && chunk < 1)
+        throw Error(MICMB_ERR_OUT_OF_MEMORY, "adjoint checkpoints of one cell group exceed the memory limit");
+      chunk = std::max<int64_t>(chunk, 1);
+      const int64_t ck = (int64_t)max_checkpoints * chunk * m.S;
+      if (!store_k)
+        st.adj_ckpt_k = DeviceMemory();
+      if (!st.adj_ckpt_y.p || st.adj_ckpt_capacity < ck || (store_k && st.adj_ckpt_k.bytes < sizeof(double) *
+                                                                                  (size_t)ck * solver->params.stages))
+      {
+        st.adj_ckpt_y = DeviceMemory();
+        st.adj_ckpt_h = DeviceMemory();
+        st.adj_ckpt_k = DeviceMemory();
+        st.adj_ckpt_y = DeviceMemory(sizeof(double) * (size_t)std::max<int64_t>(ck, 1));
+        st.adj_ckpt_h = DeviceMemory(sizeof(double) * (size_t)std::max<int64_t>((int64_t)max_checkpoints * chunk, 1));
+        if (store_k)
+          st.adj_ckpt_k = DeviceMemory(sizeof(double) * (size_t)std::max<int64_t>(ck * solver->params.stages, 1));
+        st.adj_ckpt_capacity = ck;
+      }
       MICMB_CUDA(cudaMemcpyAsync(st.adj_y0.p, st.variables.p, var_bytes, cudaMemcpyDeviceToDevice, st.stream));
       MICMB_CUDA(cudaMemcpyAsync(st.adj_ybar.p, dloss_dy_final, var_bytes, cudaMemcpyHostToDevice, st.stream));
-      FusedArgs adj{};
-      adj.variables_in = st.variables.as<double>();
-      adj.variables_out = st.variables.as<double>();
-      adj.ckpt_y = st.adj_ckpt_y.as<double>();
-      adj.ckpt_h = st.adj_ckpt_h.as<double>();
-      adj.ckpt_k = store_k ? st.adj_ckpt_k.as<double>() : nullptr;
-      adj.max_ckpt = max_checkpoints;
-      SolveFused(*solver, st, dt, stats, nullptr, nullptr, &adj);
-      LaunchAdjoint(*solver, st, max_checkpoints);
+      micmb_solver_stats total{};
+      total.state = MICMB_SOLVER_CONVERGED;
+      for (int64_t begin = 0; begin < n; begin += chunk)
+      {
+        const int64_t count = std::min<int64_t>(chunk, n - begin);
+        FusedArgs adj{};
+        adj.n_cells = count;
+        adj.variables_in = st.variables.as<double>() + (size_t)begin * m.S;
+        adj.variables_out = st.variables.as<double>() + (size_t)begin * m.S;
+        adj.rate_constants = st.rate_constants.as<double>() + (size_t)begin * m.R;
+        adj.cell_status = st.status.as<int32_t>() + begin;
+        adj.cell_accepted = st.accepted.as<int32_t>() + begin;
+        adj.ckpt_y = st.adj_ckpt_y.as<double>();
+        adj.ckpt_h = st.adj_ckpt_h.as<double>();
+        adj.ckpt_k = store_k ? st.adj_ckpt_k.as<double>() : nullptr;
+        adj.max_ckpt = max_checkpoints;
+        micmb_solver_stats cs{};
+        SolveFused(*solver, st, dt, stats ? &cs : nullptr, nullptr, nullptr, &adj);
+        LaunchAdjoint(*solver, st, max_checkpoints, begin, count);
+        if (stats)
+        {
+          total.function_calls += cs.function_calls;
+          total.jacobian_updates += cs.jacobian_updates;
+          total.number_of_steps += cs.number_of_steps;
+          total.accepted += cs.accepted;
+          total.rejected += cs.rejected;
+          total.decompositions += cs.decompositions;
+          total.solves += cs.solves;
+          total.cells_not_converged += cs.cells_not_converged;
+          if (total.state == MICMB_SOLVER_CONVERGED)
+            total.state = cs.state;
+        }
+      }
+      ReduceAdjointParameters(*solver, st);
+      if (stats)
+      {
+        total.final_time = dt;
+        *stats = total;
+      }
       if (dloss_dy0)
         MICMB_CUDA(cudaMemcpyAsync(dloss_dy0, st.adj_ybar.p, var_bytes, cudaMemcpyDeviceToHost, st.stream));
       std::vector<double> kcol(std::max<int32_t>(m.R, 1));

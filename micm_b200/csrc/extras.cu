@@ -177,8 +177,13 @@ extern "C"
         // stage 1: every candidate on a short trial, best configuration of each variant
         micmb_fused_config best_of[3];
         double rate_of_best[3] = { -1.0, -1.0, -1.0 };
+        // a mechanism beyond 16-bit byte offsets has no streamed schedule (variant
+        // 0 would run the direct kernel), beyond 16-bit positions no warp tables
+        const bool has_stream = solver->dev.has_warp && solver->stream_blocks.p;
         for (const auto& c : candidates)
         {
+          if ((c.variant == 0 && !has_stream) || (c.variant == 1 && !solver->dev.has_warp))
+            continue;
           const double r = rate_of(c, trial_cells(c), 2);
           if (r > rate_of_best[c.variant])
           {

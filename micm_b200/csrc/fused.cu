@@ -288,7 +288,10 @@ namespace micmb
     if (cfg.ctas_per_sm > 0)
       per_sm = std::min(per_sm, cfg.ctas_per_sm);
     int64_t grid = (int64_t)per_sm * s.sm_count;
-    const int64_t n = st.solve_limit > 0 ? std::min<int64_t>(st.solve_limit, st.n_cells) : st.n_cells;
+    // an adjoint chunk brings its own cell range (n_cells > 0, pointers already offset)
+    const int64_t n = (adj && adj->n_cells > 0)
+                          ? adj->n_cells
+                          : (st.solve_limit > 0 ? std::min<int64_t>(st.solve_limit, st.n_cells) : st.n_cells);
     grid = std::max<int64_t>(1, std::min<int64_t>(grid, (n + warps - 1) / warps));
 
     FusedArgs A{};
@@ -301,7 +304,8 @@ namespace micmb
       A.variables_in = st.variables.as<double>();
       A.variables_out = st.variables.as<double>();
     }
-    A.rate_constants = st.rate_constants.as<double>();
+    if (!A.rate_constants)
+      A.rate_constants = st.rate_constants.as<double>();
     A.atol = st.atol.as<double>();
     A.rtol = st.rtol;
     char* cbase = st.counters.as<char>();
@@ -312,8 +316,10 @@ namespace micmb
       st.status = DeviceMemory(sizeof(int32_t) * std::max<int64_t>(st.n_cells, 1));
     if (!st.accepted.p)
       st.accepted = DeviceMemory(sizeof(int32_t) * std::max<int64_t>(st.n_cells, 1));
-    A.cell_status = st.status.as<int32_t>();
-    A.cell_accepted = st.accepted.as<int32_t>();
+    if (!A.cell_status)
+      A.cell_status = st.status.as<int32_t>();
+    if (!A.cell_accepted)
+      A.cell_accepted = st.accepted.as<int32_t>();
     if (!lu_shared)
     {
       const int64_t slots = grid * warps;
@@ -336,6 +342,8 @@ namespace micmb
         done = SolveFusedThread(s, st, A, dt);
       if (!done)
       {
+        if (A.ckpt_k)
+          throw Error(MICMB_ERR_INTERNAL, "the direct fused kernel stores no stage vectors");
         const StepBounds B = step_bounds(s.params, dt);
         kernel<<<(unsigned)grid, threads, smem, st.stream>>>(s.dev, s.params, B, A, W);
         MICMB_CUDA(cudaGetLastError());

@@ -508,16 +508,22 @@ namespace micmb
     return 0;
   }
 
+  bool StreamVariantApplies(const micmb_solver& s)
+  {
+    if (!s.dev.has_warp || !s.stream_blocks.p)
+      return false;
+    const int slots = std::max(2, std::min(kMaxSlots, s.fused.ring_slots > 0 ? s.fused.ring_slots : 4));
+    return StreamWarpsPerCta(s, slots, s.fused.cells_per_cta, s.fused.lu_in_shared != 0) >= 1;
+  }
+
   bool SolveFusedStream(micmb_solver& s, micmb_state& st, double dt, const FusedArgs& A_in)
   {
     const auto& m = *s.mech;
-    if (!s.dev.has_warp || !s.stream_blocks.p)
+    if (!StreamVariantApplies(s))
       return false;
     const int slots = std::max(2, std::min(kMaxSlots, s.fused.ring_slots > 0 ? s.fused.ring_slots : 4));
     const bool lu_shared = s.fused.lu_in_shared != 0;
     const int W = StreamWarpsPerCta(s, slots, s.fused.cells_per_cta, lu_shared);
-    if (W < 1)
-      return false;
     const Layout LY =
         MakeLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz, s.n_stream_coef, W, slots, lu_shared);
     // per-attempt block order: F0 forcing, -J, LU, then per stage [forcing], forward, backward

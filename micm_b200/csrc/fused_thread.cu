@@ -270,6 +270,24 @@ namespace micmb
     }
   }  // namespace
 
+  int64_t FusedThreadResidentCells(const micmb_solver& s)
+  {
+    int per_sm = 0;
+    MICMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused_thread, kThreadsPerBlock, 0));
+    if (s.fused.variant == 2 && s.fused.ctas_per_sm > 0)
+      per_sm = std::min(per_sm, s.fused.ctas_per_sm);
+    return (int64_t)std::max(per_sm, 1) * s.sm_count * kThreadsPerBlock;
+  }
+
+  int64_t FusedThreadWorkspaceDoubles(const micmb_solver& s, int64_t n_cells)
+  {
+    const auto& m = *s.mech;
+    const ThreadLayout T = MakeThreadLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz);
+    const int64_t threads = std::min<int64_t>(FusedThreadResidentCells(s),
+                                              (n_cells + kThreadsPerBlock - 1) / kThreadsPerBlock * kThreadsPerBlock);
+    return std::max<int64_t>(threads, kThreadsPerBlock) * (int64_t)T.per_slot;
+  }
+
   bool SolveFusedThread(micmb_solver& s, micmb_state& st, const FusedArgs& A_in, double dt)
   {
     const auto& m = *s.mech;

@@ -101,6 +101,7 @@ struct micmb_solver
   micmb::DeviceMemory stream_block_bytes;  // [n_blocks]
   micmb::DeviceMemory stream_coef;         // StreamProgram coef_table
   int32_t n_stream_coef = 0;
+  int64_t adjoint_memory_limit = 0;  // bytes of adjoint checkpoints (0 = from free device memory)
 };
 
 struct micmb_state
@@ -163,10 +164,21 @@ namespace micmb
   size_t FusedSharedBytes(const micmb_solver& s, bool lu_in_shared);
   // streamed warp-specialised variant; returns false when it does not apply
   bool SolveFusedStream(micmb_solver& s, micmb_state& st, double dt, const FusedArgs& A);
+  // whether the streamed variant runs for the solver's mechanism and configuration
+  bool StreamVariantApplies(const micmb_solver& s);
   // one cell per thread, working sets in global memory
   bool SolveFusedThread(micmb_solver& s, micmb_state& st, const FusedArgs& A, double dt);
   int StreamWarpsPerCta(const micmb_solver& s, int slots, int cap, bool lu_shared);
-  // discrete adjoint sweep over the checkpoints of a fused solve
-  void LaunchAdjoint(micmb_solver& s, micmb_state& st, int32_t max_ckpt);
+  // discrete adjoint sweep over the checkpoints of a fused solve of cells
+  // [begin, begin + count) (begin a multiple of L; checkpoints hold those cells only)
+  void LaunchAdjoint(micmb_solver& s, micmb_state& st, int32_t max_ckpt, int64_t begin, int64_t count);
+  // dloss/dlog k summed over all cells in a fixed order, after every chunk's sweep
+  void ReduceAdjointParameters(micmb_solver& s, micmb_state& st);
+  // doubles of per-thread working set the backward sweep needs for n_cells cells
+  int64_t AdjointThreadWorkspaceDoubles(const micmb_solver& s, int64_t n_cells);
+  // doubles of per-thread working set the one-cell-per-thread forward needs
+  int64_t FusedThreadWorkspaceDoubles(const micmb_solver& s, int64_t n_cells);
+  // cells the one-cell-per-thread forward keeps resident at once
+  int64_t FusedThreadResidentCells(const micmb_solver& s);
   int FusedWarpsPerCta(const micmb_solver& s, const micmb_fused_config& cfg);
 }  // namespace micmb

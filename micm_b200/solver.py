@@ -166,7 +166,8 @@ class Solver:
         check(lib().micmb_solver_set_rate_scale(self.handle, _f64(scale)))
 
     def set_fused_config(self, cells_per_cta=0, lu_in_shared=1, ctas_per_sm=0, ring_slots=0, variant=0):
-        """variant 0: TMA-streamed warp-specialised kernel; 1: direct kernel."""
+        """variant 0: TMA-streamed warp-specialised kernel; 1: direct kernel (warp per cell);
+        2: one cell per thread, working sets in global memory."""
         cfg = FusedConfig(int(cells_per_cta), int(lu_in_shared), int(ctas_per_sm), int(ring_slots), int(variant))
         check(lib().micmb_solver_set_fused_config(self.handle, C.byref(cfg)))
 
@@ -204,6 +205,11 @@ class Solver:
     def solve_graph(self, dt: float, state: "State", n_repeats: int):
         """n_repeats x (update_state_parameters + fused per-cell solve) from one CUDA graph."""
         check(lib().micmb_solve_graph(self.handle, state.handle, float(dt), int(n_repeats)))
+
+    def set_adjoint_memory_limit(self, n_bytes: int):
+        """Device bytes solve_adjoint may hold in checkpoints (0: 80% of the free device memory).
+        Cells are solved and swept in chunks that fit; results do not depend on the chunking."""
+        check(lib().micmb_set_adjoint_memory_limit(self.handle, int(n_bytes)))
 
     def solve_adjoint(self, dt: float, state: "State", dloss_dy_final: np.ndarray, max_checkpoints: int = 256):
         """Returns (dL/dy0 [n, S] state columns, dL/dlog k [R] input order, SolverResult)."""

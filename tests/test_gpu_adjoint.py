@@ -32,7 +32,8 @@ def _significant(g, scale):
 @pytest.mark.parametrize("name,n,config", [("c60_adjoint", 96, None),
                                            ("c60_adjoint", 64, dict(variant=1)),
                                            ("c60_adjoint", 64, dict(variant=2)),
-                                           ("c210", 8, None)])
+                                           ("c210", 8, None),
+                                           ("c600", 6, None)])
 def test_adjoint_matches_oracle(cuda_device, name, n, config):
     cfg, mech, inputs, solver, st = _setup(name, n, 41, config)
     k = np.ascontiguousarray(st.rate_constants())        # the GPU's own rate constants
@@ -58,6 +59,42 @@ def test_adjoint_matches_oracle(cuda_device, name, n, config):
     gk_ref_sum = gk_ref.sum(axis=0)
     ks = np.abs(gk_ref_sum).max()
     np.testing.assert_allclose(gk, gk_ref_sum, rtol=1e-8, atol=1e-9 * ks)
+
+
+@pytest.mark.parametrize("config", [None, dict(variant=2)])
+def test_adjoint_chunks_and_recomputed_stages_change_nothing(cuda_device, config):
+    """A memory limit that splits the cells into 32-cell chunks, with the
+    stages recomputed in the sweep instead of stored, gives the same bits."""
+    cfg, mech, inputs, solver, st = _setup("c60_adjoint", 100, 43, config)
+    rng = np.random.default_rng(9)
+    ybar = rng.normal(size=(100, mech.n_species))
+    g0_a, gk_a, res_a = solver.solve_adjoint(cfg["dt"], st, ybar, max_checkpoints=300)
+    st.sync_outputs_to_host()
+    y_a = st.concentrations().copy()
+    per_cell_y = 300 * (mech.n_species + 1) * 8
+    solver.set_adjoint_memory_limit(32 * per_cell_y + 100)
+    st.set_concentrations(inputs["concentrations"])
+    st.sync_inputs_to_device()
+    g0_b, gk_b, res_b = solver.solve_adjoint(cfg["dt"], st, ybar, max_checkpoints=300)
+    st.sync_outputs_to_host()
+    np.testing.assert_array_equal(st.concentrations(), y_a)
+    np.testing.assert_array_equal(g0_b, g0_a)
+    np.testing.assert_array_equal(gk_b, gk_a)
+    assert res_b.stats["accepted"] == res_a.stats["accepted"]
+    assert res_b.stats["number_of_steps"] == res_a.stats["number_of_steps"]
+
+
+def test_adjoint_memory_limit_below_one_group(cuda_device):
+    from micm_b200._native import MicmbError
+    cfg, mech, inputs, solver, st = _setup("c60_adjoint", 40, 44)
+    solver.set_adjoint_memory_limit(1000)
+    with pytest.raises(MicmbError):
+        solver.solve_adjoint(cfg["dt"], st, np.ones((40, mech.n_species)), max_checkpoints=300)
+    solver.set_adjoint_memory_limit(0)
+    st.set_concentrations(inputs["concentrations"])
+    st.sync_inputs_to_device()
+    _, _, res = solver.solve_adjoint(cfg["dt"], st, np.ones((40, mech.n_species)), max_checkpoints=300)
+    assert res.converged
 
 
 def test_adjoint_matches_finite_differences(cuda_device):

@@ -59,13 +59,17 @@ def test_tableaus_global(cuda_device, stages):
 
 
 @pytest.mark.parametrize("method", ["plain", "fused"])
-@pytest.mark.parametrize("name", ["syn60", "syn210", "all_kinds"])
+@pytest.mark.parametrize("name", ["syn60", "syn210", "syn600", "all_kinds"])
 def test_per_cell(cuda_device, method, name):
     if name == "all_kinds":
         m, inp, dt, stages = all_rate_types(), all_rate_types_inputs(200, 8), 50.0, 3
     elif name == "syn60":
         m = synthetic.synthetic_mechanism(60, 120, seed=601)
         inp, dt, stages = synthetic.cell_inputs(m, 512, seed=602), 3600.0, 4
+    elif name == "syn600":
+        # 600 species / 1,500 reactions: the LU factor (11,304 entries) outgrows shared memory
+        m = synthetic.CONFIGS["c600"]["mech"]()
+        inp, dt, stages = synthetic.cell_inputs(m, 96, seed=6003), 600.0, 4
     else:
         m = synthetic.synthetic_mechanism(210, 440, seed=2101)
         inp, dt, stages = synthetic.cell_inputs(m, 256, seed=2102), 600.0, 4
@@ -122,6 +126,18 @@ def test_fused_variants_bitwise(cuda_device, config):
     np.testing.assert_array_equal(y_f, y_p)
     np.testing.assert_array_equal(r_f[0].per_cell_accepted, r_p[0].per_cell_accepted)
     assert r_f[0].stats["number_of_steps"] == r_p[0].stats["number_of_steps"]
+
+
+@pytest.mark.parametrize("config", [dict(variant=0), dict(variant=1), dict(variant=2)])
+def test_large_mechanism_variants_bitwise(cuda_device, config):
+    """600 species: no streamed schedule (operands beyond 16-bit byte offsets),
+    so variant 0 runs the direct kernel; every variant equals the plain path."""
+    m = synthetic.CONFIGS["c600"]["mech"]()
+    inp = synthetic.cell_inputs(m, 70, seed=6004)
+    y_p, r_p = solve_gpu(m, inp, 600.0, 4, "plain", "per_cell", L=32)
+    y_f, r_f = solve_gpu(m, inp, 600.0, 4, "fused", "per_cell", L=32, fused_config=config)
+    np.testing.assert_array_equal(y_f, y_p)
+    np.testing.assert_array_equal(r_f[0].per_cell_accepted, r_p[0].per_cell_accepted)
 
 
 def test_fused_tiny_and_ragged(cuda_device):

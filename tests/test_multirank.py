@@ -31,7 +31,7 @@ def _rank_main(rank, world, port, cells, out_path):
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         import bench
-        cfg, mech, inputs = bench.workload(cells, rank)
+        cfg, mech, inputs = bench.workload("c210_uneven", cells, rank)
         R = oracle.Restatement(mech, tableau_kind=cfg["stages"])
         y, stats = R.solve_per_cell(inputs, cfg["dt"], threads=1)
         # a deliberately uneven per-rank time: the job time must be the maximum
@@ -62,7 +62,7 @@ def test_two_ranks_solve_disjoint_shards_and_agree_on_time(tmp_path):
     # and each shard's solve equals the same cells solved by a single process
     import bench
     for rank, r in enumerate((r0, r1)):
-        cfg, mech, inputs = bench.workload(cells, rank)
+        cfg, mech, inputs = bench.workload("c210_uneven", cells, rank)
         R = oracle.Restatement(mech, tableau_kind=cfg["stages"])
         y, stats = R.solve_per_cell(inputs, cfg["dt"], threads=1)
         np.testing.assert_array_equal(r["y"], y)
