@@ -9,6 +9,7 @@ exceed the 126 MB L2, so no flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
     python bench.py --workload c600     # 600 species / 1,500 reactions, 262,144 cells
+    python bench.py --workload ts1      # micm's TS1 benchmark mechanism, 1,048,576 cells, dt = 30 s
 
 N > 1 runs under torchrun: each rank solves its own 1M-cell shard (weak
 scaling; cells are independent, no collective on the data path).
@@ -47,7 +48,12 @@ WORKLOADS = {
                       "beyond shared memory)",
                  l2="inputs exceed L2 (1.3 GB state + 3.1 GB rate constants); no flush",
                  adjoint=("c600", 262144, 160),
-                 profile="k_fused_thread_c600_16384cells.md"),
+                 profile="k_fused_thread_c600_65536cells.md"),
+    "ts1": dict(cells=1048576, cpu_sample=65536,
+                text="micm's TS1 benchmark mechanism (209 species, 547 reactions) on {cells} cells per GPU, "
+                     "micm_bench's initial state on every cell, 3-stage Rosenbrock, dt=30 s, fused persistent kernel",
+                l2="inputs exceed L2 (1.8 GB state + 4.6 GB rate constants); no flush",
+                adjoint=None, profile="k_fused_thread_ts1_65536cells.md"),
 }
 
 
@@ -142,6 +148,11 @@ def job_throughput(cells_per_rank: int, world: int, steps: int, seconds: float) 
 
 def workload(name: str, cells: int, rank: int = 0):
     from micm_b200 import synthetic
+    if name == "ts1":
+        # micm_bench's TS1 case: the same initial state on every cell
+        from micm_b200 import ts1
+        cfg = dict(stages=ts1.TABLEAU, dt=ts1.DT, seed=0, inputs={})
+        return cfg, ts1.mechanism(), ts1.inputs(cells)
     cfg = synthetic.CONFIGS[name]
     mech = cfg["mech"]()
     inputs = synthetic.cell_inputs(mech, cells, cfg["seed"] + 1000 * rank, **cfg["inputs"])
@@ -485,7 +496,7 @@ def main():
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
     adj = None
-    if not args.no_adjoint:
+    if not args.no_adjoint and W["adjoint"]:
         same = W["adjoint"][0] == args.workload            # same mechanism: keep the configuration tuned above
         adj = adjoint_ratio(torch, rank, *W["adjoint"], fused_config=tuned if same else None)
 

@@ -282,7 +282,10 @@ int micmb_solve(micmb_solver* solver, micmb_state* state, double dt, int32_t met
 typedef struct micmb_fused_config {
   int32_t cells_per_cta;   /* consumer warps (one cell each) per CTA, 0..12, 0 = as many as fit */
   int32_t lu_in_shared;    /* 1 LU factor in shared memory, 0 in a per-warp global (L2) slot */
-  int32_t ctas_per_sm;     /* persistent grid = ctas_per_sm * SM count (0 = occupancy) */
+  int32_t ctas_per_sm;     /* persistent grid = ctas_per_sm * SM count (0 = occupancy); variant 2
+                              also picks its kernel build by it: 1..5 the 96-register kernel,
+                              6..8 the 64-register one, 9..12 the 40-register one, 0 or above 12
+                              the 32-register one (every warp slot of the SM) */
   int32_t ring_slots;      /* streamed variant: shared-memory slots for table blocks (0 = 4) */
   int32_t variant;         /* 0 streamed (TMA-fed, warp-specialised), 1 direct (warp per cell),
                               2 one cell per thread (working sets in global memory) */

@@ -527,8 +527,8 @@ namespace micmb
       }
     }
 
-    __global__ void __launch_bounds__(128) k_adjoint_thread(DevMech M, DevParams P, AdjArgs A, AdjThreadLayout T,
-                                                           double* ws)
+    __device__ __forceinline__ void adjoint_thread_body(const DevMech& M, const DevParams& P, const AdjArgs& A,
+                                                        const AdjThreadLayout& T, double* ws)
     {
       const int lane = threadIdx.x & 31;
       const int64_t wslot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -745,6 +745,24 @@ namespace micmb
       }
     }
 
+    // 96 registers, 5 blocks of 128 per SM, no spills.  A full-occupancy build
+    // (32 registers, as the forward kernel's fastest) measured slower here:
+    // 1.38 s against 1.16 s on 131,072 cells of the 60-species mechanism, and
+    // 67.6 s against 52.5 s on 262,144 cells of the 600-species one, where its
+    // larger working-set footprint also leaves less memory for checkpoints.
+    __global__ void __launch_bounds__(128, 5)
+        k_adjoint_thread(DevMech M, DevParams P, AdjArgs A, AdjThreadLayout T, double* ws)
+    {
+      adjoint_thread_body(M, P, A, T, ws);
+    }
+
+    using AdjThreadKernel = void (*)(DevMech, DevParams, AdjArgs, AdjThreadLayout, double*);
+
+    AdjThreadKernel AdjointThreadKernelFor(const micmb_solver&)
+    {
+      return k_adjoint_thread;
+    }
+
     // Cells in decreasing order of accepted steps (counting sort on the step
     // count): the backward sweep takes the longest cells first, so the last
     // cells finish together, and the 32 cells of a warp have similar counts.
@@ -830,8 +848,9 @@ namespace micmb
     if (s.params.stages > kMaxAdjStages)
       throw Error(MICMB_ERR_UNSUPPORTED, "too many stages for the adjoint kernel");
     const AdjThreadLayout T = MakeAdjThreadLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz);
+    const AdjThreadKernel kernel = AdjointThreadKernelFor(s);
     int per_sm = 0;
-    MICMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adjoint_thread, 128, 0));
+    MICMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, 0));
     if (per_sm < 1)
       throw Error(MICMB_ERR_UNSUPPORTED, "adjoint kernel cannot be resident");
     const int64_t n = count;
@@ -857,7 +876,7 @@ namespace micmb
       k_step_scatter<<<blocks, 256, 0, st.stream>>>(A.n_ckpt, n, max_ckpt, bins, order);
       MICMB_CUDA(cudaGetLastError());
       A.order = order;
-      k_adjoint_thread<<<(unsigned)grid, 128, 0, st.stream>>>(s.dev, s.params, A, T, st.thread_ws.as<double>());
+      kernel<<<(unsigned)grid, 128, 0, st.stream>>>(s.dev, s.params, A, T, st.thread_ws.as<double>());
       MICMB_CUDA(cudaGetLastError());
     }
   }
@@ -867,7 +886,7 @@ namespace micmb
     const auto& m = *s.mech;
     const AdjThreadLayout T = MakeAdjThreadLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz);
     int per_sm = 0;
-    MICMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adjoint_thread, 128, 0));
+    MICMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, AdjointThreadKernelFor(s), 128, 0));
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((int64_t)per_sm * s.sm_count, (n_cells + 127) / 128));
     return grid * 128 * (int64_t)T.per_slot;
   }

@@ -528,6 +528,37 @@ namespace micmb
     return part[0];
   }
 
+  // 5-bit bit reversal (compile-time when t is)
+  __host__ __device__ constexpr int bitrev5(int t)
+  {
+    return ((t & 1) << 4) | ((t & 2) << 2) | (t & 4) | ((t & 8) >> 2) | ((t & 16) >> 4);
+  }
+
+  // The sum butterfly_sum_serial forms from part[l] = sum of term(i) over
+  // i = l, l + 32, ... < n (increasing i), without the 32 partial sums: the
+  // stripes are visited in the tree's leaf order (bit-reversed l), and a
+  // five-level stack joins them pairwise as a binary counter does, so every
+  // addition has the same operands as in the butterfly (x + y == y + x).
+  template<class F>
+  __device__ __forceinline__ double stripe_tree_sum(int32_t n, F term)
+  {
+    double stack[5];
+    double v = 0.0;
+#pragma unroll 1
+    for (int t = 0; t < 32; ++t)
+    {
+      v = 0.0;
+      for (int32_t i = bitrev5(t); i < n; i += 32)
+        v += term(i);
+      int level = 0;
+      for (; level < 5 && ((t >> level) & 1); ++level)
+        v = stack[level] + v;
+      if (level < 5)
+        stack[level] = v;
+    }
+    return v;
+  }
+
   // ---------------------------------------------------------------------
   // step control (rosenbrock.inl:80-293)
   // ---------------------------------------------------------------------

@@ -131,7 +131,8 @@ extern "C"
         { 0, 0, 0, 2, 0 }, { 0, 0, 0, 4, 0 },  // streamed, LU in global slots, as many cells as fit
         { 6, 0, 0, 4, 0 }, { 4, 0, 0, 4, 0 },  // streamed, fewer cells per CTA
         { 0, 1, 0, 0, 1 }, { 0, 0, 0, 0, 1 },  // direct
-        { 0, 0, 0, 0, 2 }, { 0, 0, 4, 0, 2 },  // one cell per thread (full and limited occupancy)
+        { 0, 0, 0, 0, 2 }, { 0, 0, 12, 0, 2 },  // one cell per thread: 32-, 40-, 64- and 96-register builds
+        { 0, 0, 8, 0, 2 }, { 0, 0, 5, 0, 2 },
       };
       // tune each candidate on enough cells to fill every SM a few times over:
       // a few warps per SM for the warp-per-cell variants, up to 1024 threads

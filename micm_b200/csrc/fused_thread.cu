@@ -18,9 +18,14 @@ namespace micmb
 {
   namespace
   {
-    // 128-thread blocks; with no minimum-blocks hint the compiler settles on
-    // 96 registers (20 resident warps per SM).  Hints of 5 or 8 blocks per SM
-    // measured 10 % slower, a hint of 1 block lets it take 180 registers.
+    // 128-thread blocks.  The kernel is compiled for four residencies (the
+    // minimum-blocks hint of __launch_bounds__): 16 blocks per SM (32
+    // registers, 64 warps: every warp slot, with spills), 12 (40 registers),
+    // 8 (64 registers) and 5 (96 registers, no spills, 20 warps).  More
+    // resident warps hide more HBM latency, fewer registers spill more; on the
+    // 210- and 600-species mechanisms and TS1 the full-occupancy build measured
+    // fastest (11-34 % over the 96-register one).  micmb_fused_config.ctas_per_sm
+    // selects the build; the autotuner times them.
     constexpr int kThreadsPerBlock = 128;
 
     __device__ __forceinline__ size_t cell_base(int64_t c, int32_t L, int32_t ncol)
@@ -68,8 +73,8 @@ namespace micmb
         cc.function_calls += P.new_f[s] ? 1 : 0;
     }
 
-    __global__ void __launch_bounds__(kThreadsPerBlock)
-        k_fused_thread(DevMech M, DevParams P, StepBounds B, FusedArgs A, double* ws, ThreadLayout T)
+    __device__ __forceinline__ void fused_thread_body(const DevMech& M, const DevParams& P, const StepBounds& B,
+                                                      const FusedArgs& A, double* ws, const ThreadLayout& T)
     {
       const int lane = threadIdx.x & 31;
       const int64_t wslot = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -86,7 +91,11 @@ namespace micmb
       Strided scr{ w + (size_t)T.oScr * 32, 32 };
       auto Kv = [&](int32_t st) { return Strided{ Kb + (size_t)st * S * 32, 32 }; };
 
-      long long acc[8] = { 0 };
+      // solver statistics of the block's finished cells (one global atomic per block and counter)
+      __shared__ unsigned long long block_stats[8];
+      if (threadIdx.x < 8)
+        block_stats[threadIdx.x] = 0;
+      __syncthreads();
       CellCtl c;
       ctl_init(c, B);
       int64_t cell = 0;
@@ -104,14 +113,15 @@ namespace micmb
           A.cell_status[cell] = c.state;
         if (A.cell_accepted)
           A.cell_accepted[cell] = A.ckpt_y ? n_ckpt : c.accepted;
-        acc[0] += c.function_calls;
-        acc[1] += c.jacobian_updates;
-        acc[2] += c.number_of_steps;
-        acc[3] += c.accepted;
-        acc[4] += c.rejected;
-        acc[5] += c.decompositions;
-        acc[6] += c.solves;
-        acc[7] += (c.state == MICMB_SOLVER_CONVERGED) ? 0 : 1;
+        atomicAdd(block_stats + 0, (unsigned long long)c.function_calls);
+        atomicAdd(block_stats + 1, (unsigned long long)c.jacobian_updates);
+        atomicAdd(block_stats + 2, (unsigned long long)c.number_of_steps);
+        atomicAdd(block_stats + 3, (unsigned long long)c.accepted);
+        atomicAdd(block_stats + 4, (unsigned long long)c.rejected);
+        atomicAdd(block_stats + 5, (unsigned long long)c.decompositions);
+        atomicAdd(block_stats + 6, (unsigned long long)c.solves);
+        if (c.state != MICMB_SOLVER_CONVERGED)
+          atomicAdd(block_stats + 7, 1ull);
       };
       // take cells until one needs an attempt (or none are left)
       auto claim = [&]() {
@@ -189,13 +199,8 @@ namespace micmb
           solve_lower<1>(M.fwd_s, LU, Ks, 0);
           solve_upper<1>(M.bwd_s, LU, Ks, 0);
         }
-        // Ynew, error partial sums in the 32-lane-stripe order of the warp kernels
-        double part[32];
-#pragma unroll
-        for (int l = 0; l < 32; ++l)
-          part[l] = 0.0;
-        for (int32_t i = 0; i < S; ++i)
-        {
+        // Ynew, and the error norm summed in the 32-lane-stripe order of the warp kernels
+        const double sum = stripe_tree_sum(S, [&](int32_t i) {
           double v = Y[i];
           double e = 0.0;
           for (int32_t st = 0; st < P.stages; ++st)
@@ -205,9 +210,8 @@ namespace micmb
             e += P.e[st] * kv;
           }
           Yn[i] = v;
-          part[i & 31] += scaled_sq(Y[i], v, e, A.atol[i], A.rtol);
-        }
-        const double sum = butterfly_sum_serial(part);
+          return scaled_sq(Y[i], v, e, A.atol[i], A.rtol);
+        });
         const double rms = sqrt(sum / (double)S);
         const double error = (rms < 1.0e-10) ? 1.0e-10 : rms;
         count_attempt(c, P);
@@ -258,25 +262,62 @@ namespace micmb
           claim();
         }
       }
-      for (int q = 0; q < 8; ++q)
-      {
-        // one atomic per warp and counter
-        long long v = acc[q];
-        for (int off = 16; off > 0; off >>= 1)
-          v += __shfl_xor_sync(0xffffffffu, v, off);
-        if (lane == 0 && v)
-          atomicAdd(A.stats + q, (unsigned long long)v);
-      }
+      __syncthreads();
+      if (threadIdx.x < 8 && block_stats[threadIdx.x])
+        atomicAdd(A.stats + threadIdx.x, block_stats[threadIdx.x]);
+    }
+
+    __global__ void __launch_bounds__(kThreadsPerBlock, 5)
+        k_fused_thread_r96(DevMech M, DevParams P, StepBounds B, FusedArgs A, double* ws, ThreadLayout T)
+    {
+      fused_thread_body(M, P, B, A, ws, T);
+    }
+
+    __global__ void __launch_bounds__(kThreadsPerBlock, 8)
+        k_fused_thread_r64(DevMech M, DevParams P, StepBounds B, FusedArgs A, double* ws, ThreadLayout T)
+    {
+      fused_thread_body(M, P, B, A, ws, T);
+    }
+
+    __global__ void __launch_bounds__(kThreadsPerBlock, 12)
+        k_fused_thread_r40(DevMech M, DevParams P, StepBounds B, FusedArgs A, double* ws, ThreadLayout T)
+    {
+      fused_thread_body(M, P, B, A, ws, T);
+    }
+
+    __global__ void __launch_bounds__(kThreadsPerBlock, 16)
+        k_fused_thread(DevMech M, DevParams P, StepBounds B, FusedArgs A, double* ws, ThreadLayout T)
+    {
+      fused_thread_body(M, P, B, A, ws, T);
+    }
+
+    using ThreadKernel = void (*)(DevMech, DevParams, StepBounds, FusedArgs, double*, ThreadLayout);
+
+    // the build a configuration asks for (ctas_per_sm; 0 = full occupancy)
+    ThreadKernel ThreadKernelFor(const micmb_fused_config& cfg)
+    {
+      if (cfg.ctas_per_sm == 0 || cfg.ctas_per_sm > 12)
+        return k_fused_thread;
+      if (cfg.ctas_per_sm > 8)
+        return k_fused_thread_r40;
+      if (cfg.ctas_per_sm > 5)
+        return k_fused_thread_r64;
+      return k_fused_thread_r96;
+    }
+
+    int ThreadBlocksPerSm(const micmb_solver& s)
+    {
+      int per_sm = 0;
+      MICMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ThreadKernelFor(s.fused), kThreadsPerBlock, 0));
+      if (s.fused.variant == 2 && s.fused.ctas_per_sm > 0)
+        per_sm = std::min(per_sm, s.fused.ctas_per_sm);
+      return per_sm;
     }
   }  // namespace
 
   int64_t FusedThreadResidentCells(const micmb_solver& s)
   {
-    int per_sm = 0;
-    MICMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused_thread, kThreadsPerBlock, 0));
-    if (s.fused.variant == 2 && s.fused.ctas_per_sm > 0)
-      per_sm = std::min(per_sm, s.fused.ctas_per_sm);
-    return (int64_t)std::max(per_sm, 1) * s.sm_count * kThreadsPerBlock;
+    return (int64_t)std::max(ThreadBlocksPerSm(s), 1) * s.sm_count * kThreadsPerBlock;
   }
 
   int64_t FusedThreadWorkspaceDoubles(const micmb_solver& s, int64_t n_cells)
@@ -292,20 +333,18 @@ namespace micmb
   {
     const auto& m = *s.mech;
     const ThreadLayout T = MakeThreadLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz);
-    int per_sm = 0;
-    MICMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused_thread, kThreadsPerBlock, 0));
+    const ThreadKernel kernel = ThreadKernelFor(s.fused);
+    const int per_sm = ThreadBlocksPerSm(s);
     if (per_sm < 1)
       return false;
-    if (s.fused.ctas_per_sm > 0)
-      per_sm = std::min(per_sm, s.fused.ctas_per_sm);
     int64_t grid = (int64_t)per_sm * s.sm_count;
     grid = std::max<int64_t>(1, std::min<int64_t>(grid, (A_in.n_cells + kThreadsPerBlock - 1) / kThreadsPerBlock));
     const int64_t doubles = grid * kThreadsPerBlock * (int64_t)T.per_slot;
     if (!st.thread_ws.p || st.thread_ws.bytes < (size_t)doubles * sizeof(double))
       st.thread_ws = DeviceMemory((size_t)doubles * sizeof(double));
     const StepBounds B = step_bounds(s.params, dt);
-    k_fused_thread<<<(unsigned)grid, kThreadsPerBlock, 0, st.stream>>>(s.dev, s.params, B, A_in,
-                                                                        st.thread_ws.as<double>(), T);
+    kernel<<<(unsigned)grid, kThreadsPerBlock, 0, st.stream>>>(s.dev, s.params, B, A_in, st.thread_ws.as<double>(),
+                                                               T);
     MICMB_CUDA(cudaGetLastError());
     return true;
   }

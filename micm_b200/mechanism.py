@@ -171,6 +171,62 @@ class Mechanism:
         return np.asarray(self.absolute_tolerance, dtype=np.float64)
 
 
+_KIND_BY_NAME = {"arrhenius": ARRHENIUS, "troe": TROE, "ternary_chemical_activation": TERNARY_CHEMICAL_ACTIVATION,
+                 "branched": BRANCHED, "tunneling": TUNNELING, "taylor_series": TAYLOR_SERIES,
+                 "reversible": REVERSIBLE, "user_defined": USER_DEFINED, "surface": SURFACE}
+
+
+def mechanism_from_dict(d: dict) -> Mechanism:
+    """A mechanism from its JSON description:
+
+    ``species``: names in gas-phase order (the state's system order);
+    ``parameterized``: ``[{"name", "coefficients": [c0, c_T, c_P, c_rho]}]``
+    (third bodies and other parameterized reactants, value c0 + c_T T + c_P P +
+    c_rho rho as micm's ParameterizedFunction, parameterized_function.hpp:26-49);
+    ``reactions``: ``[{"kind", "params", "reactants": [names], "products":
+    [[name, yield]], "label"?}]`` in input order, ``params`` as the rate
+    helpers of this module take them; optional ``absolute_tolerance`` (one
+    value or one per species; micm's builder default 1e-3 otherwise) and
+    ``relative_tolerance``."""
+    species = list(d["species"])
+    index = {n: i for i, n in enumerate(species)}
+    params = d.get("parameterized", [])
+    pindex = {p["name"]: i for i, p in enumerate(params)}
+    atol = d.get("absolute_tolerance")
+    if atol is not None:
+        atol = np.broadcast_to(np.asarray(atol, dtype=np.float64), (len(species),)).copy()
+    m = Mechanism(species=species, reactions=[], name=d.get("name", "mechanism"),
+                  parameterized=[tuple(float(c) for c in p["coefficients"]) for p in params],
+                  absolute_tolerance=atol, relative_tolerance=float(d.get("relative_tolerance", 1e-6)))
+
+    def reactant(name):
+        if name in index:
+            return index[name]
+        if name in pindex:
+            return -(pindex[name] + 1)
+        raise ValueError(f"unknown reactant '{name}'")
+
+    for rx in d["reactions"]:
+        kind = _KIND_BY_NAME[rx["kind"]]
+        products = []
+        for name, y in rx["products"]:
+            if name in pindex:
+                continue        # a parameterized product is no state variable (process_set.hpp:299-303)
+            if name not in index:
+                raise ValueError(f"unknown product '{name}'")
+            products.append((index[name], float(y)))
+        m.reactions.append(Reaction(kind, [float(v) for v in rx["params"]],
+                                    [reactant(n) for n in rx["reactants"]], products, rx.get("label")))
+    return m
+
+
+def load_mechanism_json(path: str) -> Mechanism:
+    """mechanism_from_dict of a JSON file."""
+    import json
+    with open(path) as f:
+        return mechanism_from_dict(json.load(f))
+
+
 def ideal_air_density(pressure, temperature):
     """Conditions::CalculateIdealAirDensity (include/micm/system/conditions.hpp:20-23)."""
     return np.asarray(pressure) / (GAS_CONSTANT * np.asarray(temperature))

@@ -116,7 +116,8 @@ def test_fused_lu_in_global_memory(cuda_device):
                                     dict(variant=0, cells_per_cta=1), dict(variant=0, ctas_per_sm=2),
                                     dict(variant=0, lu_in_shared=0, cells_per_cta=10),
                                     dict(variant=0, lu_in_shared=0, cells_per_cta=12, ring_slots=2),
-                                    dict(variant=2), dict(variant=2, ctas_per_sm=1)])
+                                    dict(variant=2), dict(variant=2, ctas_per_sm=1),
+                                    dict(variant=2, ctas_per_sm=8), dict(variant=2, ctas_per_sm=12)])
 def test_fused_variants_bitwise(cuda_device, config):
     """Every fused configuration computes exactly what the plain kernels compute."""
     m = synthetic.synthetic_mechanism(210, 440, seed=2101)

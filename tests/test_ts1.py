@@ -1,0 +1,69 @@
+"""micm's TS1 benchmark mechanism (test/benchmark/ts1_mechanism.hpp) as
+ingested from the fixture micm itself wrote (tests/golden/make_ts1.py): the
+numbering equals micm's state, and the checkers reproduce micm's results on it."""
+import numpy as np
+import pytest
+
+import oracle
+from micm_b200 import ts1
+from micm_b200.solver import CompiledMechanism
+
+GOLDEN = np.load(ts1.FIXTURE.replace("ts1_mechanism.json", "ts1_micm.npz"))
+
+
+def _golden_inputs(mech, cols):
+    y_sys = GOLDEN["initial_variables"][:, cols]
+    return dict(temperature=GOLDEN["temperature"], pressure=GOLDEN["pressure"], air_density=GOLDEN["air_density"],
+                concentrations=np.ascontiguousarray(y_sys),
+                custom_params=np.ascontiguousarray(GOLDEN["custom_parameters"]))
+
+
+def test_numbering_equals_micm_state():
+    mech = ts1.mechanism()
+    cm = CompiledMechanism(mech)
+    cols = ts1.micm_columns()
+    assert mech.n_species == 209 and mech.n_reactions == 547
+    np.testing.assert_array_equal(cm.species_columns, [cols["species"][s] for s in mech.species])
+    # custom parameters: label order is micm's column order
+    labels = mech.custom_param_labels()
+    np.testing.assert_array_equal([cols["custom_parameters"][l] for l in labels], np.arange(len(labels)))
+    # LU statistics micm reports for TS1 (2,381 filled nonzeros, 6,986 updates, 1,244 multipliers)
+    assert cm.info["jacobian_nnz"] == 2381
+    assert cm.info["lu_updates"] == 6986
+    assert cm.info["lu_lower"] == 1244
+
+
+def test_inputs_follow_the_benchmark_state():
+    mech = ts1.mechanism()
+    inp = ts1.inputs(3)
+    cols = CompiledMechanism(mech).species_columns
+    np.testing.assert_array_equal(inp["concentrations"][0], GOLDEN["initial_variables"][0, cols])
+    np.testing.assert_array_equal(inp["custom_params"][0], GOLDEN["custom_parameters"][0])
+    assert inp["temperature"][0] == GOLDEN["temperature"][0]
+    varied = ts1.inputs(16, seed=3)
+    assert np.all(varied["concentrations"] >= 0) and varied["temperature"].std() > 1.0
+
+
+@pytest.mark.skipif(not oracle.restatement_available(), reason="oracle not built")
+def test_restatement_rate_constants_equal_micm():
+    mech = ts1.mechanism()
+    R = oracle.Restatement(mech, tableau_kind=ts1.TABLEAU)
+    inp = _golden_inputs(mech, R.species_columns)
+    k = R.rate_constants(inp["temperature"], inp["pressure"], inp["air_density"], inp["custom_params"])
+    # both in micm's rate-constant columns (reactions after micm's type sort)
+    np.testing.assert_allclose(k, GOLDEN["rate_constants"], rtol=1e-14, atol=0)
+
+
+@pytest.mark.skipif(not oracle.reference_available(), reason="oracle/_ref not built")
+def test_flattened_mechanism_reproduces_micm_from_its_header():
+    """micm built from the flattened description (oracle/_ref) gives what micm
+    built from its own header gave: 10 global Solve(30 s) on 4 varied cells."""
+    mech = ts1.mechanism()
+    ref = oracle.Reference(mech, tableau=ts1.TABLEAU)
+    inp = _golden_inputs(mech, ref.species_columns)
+    for s in range(len(GOLDEN["variables"])):
+        y, stats = ref.solve_global(inp, float(GOLDEN["dt"]))
+        np.testing.assert_array_equal(ref.y_to_columns(y), GOLDEN["variables"][s])
+        assert stats[0]["accepted"] == GOLDEN["stats"][s, 0]
+        assert stats[0]["number_of_steps"] == GOLDEN["stats"][s, 2]
+        inp = dict(inp, concentrations=y)
