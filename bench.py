@@ -357,6 +357,11 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    # one explicit stream for the whole run: the state's kernels, the restore
+    # copies and the timing events must share it (the legacy default stream's
+    # handle is 0, which the library reads as "the state's own stream")
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     dist = None
     if world > 1:
         import datetime
@@ -380,7 +385,6 @@ def main():
         tuned = solver.get_fused_config()
     else:
         tuned = solver.autotune(cfg["dt"], state)              # cells-per-CTA, LU staging, ring depth, variant
-    stream = torch.cuda.current_stream()
     check(lib().micmb_state_set_stream(state.handle, ctypes.c_void_p(stream.cuda_stream)))
     y0_host = to_vector_layout(state.variables, L)
     y_dev = torch.from_numpy(y0_host).cuda()
