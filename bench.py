@@ -492,6 +492,19 @@ def main():
                               "frac": plain_gbs / peak_gbs,
                               "note": "algorithmic bytes of the per-stage kernels over the solve's wall time "
                                       "(launches and host synchronisation included)"}}
+        # the same kernels with micm's CUDA-path semantics: one step size for
+        # all cells from the error norm over all cells (a different step
+        # sequence, so not bit-comparable with the per-cell solves)
+        pview.copy_(p0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        gres = solver.solve(cfg["dt"], pstate, method="plain", step_control="global")
+        torch.cuda.synchronize()
+        gt = time.perf_counter() - t0
+        plain["global_step_size"] = {"value": pc * world / gt, "unit": UNIT, "ms_per_step": 1000 * gt,
+                                     "attempts": gres.stats["number_of_steps"], "accepted": gres.stats["accepted"],
+                                     "converged": bool(gres.converged),
+                                     "fused_over_this": value / (pc * world / gt)}
 
     # the solve states are released before the adjoint timing, which sizes its
     # checkpoint chunks from the free device memory
