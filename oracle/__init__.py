@@ -69,6 +69,9 @@ def _load_ref():
                                           _f64p, _f64p, _i64p]
         lib.mref_solve_per_cell.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, _f64p, _f64p, _f64p,
                                             _f64p, _f64p, _i64p, C.c_int]
+        if hasattr(lib, "mref_solve_groups_v128"):
+            lib.mref_solve_groups_v128.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, _f64p, _f64p,
+                                                   _f64p, _f64p, _f64p, _i64p, C.c_int]
         _ref = lib
     return _ref
 
@@ -184,6 +187,25 @@ class Reference:
             self.handle, n, float(dt), int(n_solves), _p(inputs["temperature"]), _p(inputs["pressure"]),
             _p(inputs["air_density"]), _p(params), _p(y), _p(stats, C.c_int64)))
         return self.y_from_columns(y), _stats_rows(stats)
+
+    def solve_groups_v128(self, inputs: Dict[str, np.ndarray], dt: float, group: int = 1024, n_solves: int = 1,
+                          threads: int = 0):
+        """micm with vector ordering L = 128: one State (one step size) per group
+        of `group` cells, groups over host threads.  Returns (y_final [n,S]
+        system order, stats rows per group)."""
+        if not hasattr(self.lib, "mref_solve_groups_v128"):
+            raise RuntimeError("oracle/_ref/libmicm_ref.so predates mref_solve_groups_v128; rebuild it")
+        y = self.y_to_columns(inputs["concentrations"])
+        n = len(y)
+        stats = np.zeros((max(-(-n // group), 1), 10), np.int64)
+        params = np.ascontiguousarray(inputs["custom_params"] if inputs["custom_params"].size
+                                      else np.zeros((n, 1)))
+        threads = threads or (os.cpu_count() or 1)
+        self._check(self.lib.mref_solve_groups_v128(
+            self.handle, n, int(group), float(dt), int(n_solves), _p(inputs["temperature"]),
+            _p(inputs["pressure"]), _p(inputs["air_density"]), _p(params), _p(y), _p(stats, C.c_int64),
+            int(threads)))
+        return self.y_from_columns(y), stats
 
     def solve_per_cell(self, inputs: Dict[str, np.ndarray], dt: float, n_solves: int = 1,
                        threads: int = 0):

@@ -211,6 +211,7 @@ namespace
     double rtol = 1e-6;
     bool reorder = true;
     std::unique_ptr<SolverL<1>> solver1;
+    std::unique_ptr<SolverL<128>> solver128;  // built on first use (mref_solve_groups_v128)
     std::vector<int> species_column;  // system species -> state column
     std::vector<int> param_column;    // input reaction -> custom param column or -1
     int n_params = 0;
@@ -529,6 +530,79 @@ extern "C"
     for (int c = 0; c < n; ++c)
       for (int j = 0; j < S; ++j)
         y_inout[(size_t)c * S + j] = state.variables_[c][j];
+    return 0;
+    GUARD_END
+  }
+
+  // micm's vector ordering with L = 128 (micm_bench's fastest CPU layout,
+  // test/benchmark/bench_harness.hpp VectorDense<128> / VectorSparse<128>):
+  // cells in consecutive groups of `group` cells, one State per group with one
+  // step size for the group, groups taken by n_threads host threads (one State
+  // per thread at a time, test/tutorial/test_openmp.cpp:115-122).  For cells
+  // that share their inputs this is the same solve as per-cell control.
+  // stats_out [group][10] accumulates over solves.
+  int mref_solve_groups_v128(void* p, int n, int group, double dt, int n_solves, const double* T, const double* P,
+                             const double* rho, const double* params, double* y_inout, int64_t* stats_out,
+                             int n_threads)
+  {
+    GUARD_BEGIN
+    auto* h = static_cast<Handle*>(p);
+    const int S = h->built.n_species;
+    if (group < 1)
+      throw std::runtime_error("group must be at least 1");
+    if (!h->solver128)
+      h->solver128 = std::make_unique<SolverL<128>>(MakeSolver<128>(*h));
+    if (n_threads < 1)
+      n_threads = 1;
+    const int n_groups = (n + group - 1) / group;
+    std::atomic<int> next{ 0 };
+    std::string failure;
+    auto work = [&]()
+    {
+      try
+      {
+        for (;;)
+        {
+          const int g = next.fetch_add(1);
+          if (g >= n_groups)
+            break;
+          const int c0 = g * group, count = std::min(group, n - c0);
+          auto state = h->solver128->GetState(count);
+          state.SetRelativeTolerance(h->rtol);
+          for (int c = 0; c < count; ++c)
+            LoadCell(state, c, h->n_params, S, T, P, rho, params, y_inout, c0 + c);
+          int64_t acc[10] = { 0 };
+          for (int i = 0; i < n_solves; ++i)
+          {
+            h->solver128->UpdateStateParameters(state);
+            auto r = h->solver128->Solve(dt, state);
+            int64_t one[10];
+            StatsOut(r, one);
+            for (int q = 0; q < 7; ++q)
+              acc[q] += one[q];
+            acc[7] = one[7];
+            acc[8] = one[8];
+          }
+          for (int c = 0; c < count; ++c)
+            for (int j = 0; j < S; ++j)
+              y_inout[(size_t)(c0 + c) * S + j] = state.variables_[c][j];
+          if (stats_out)
+            std::memcpy(stats_out + 10 * (size_t)g, acc, sizeof(acc));
+        }
+      }
+      catch (const std::exception& e)
+      {
+        failure = e.what();
+      }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < n_threads; ++t)
+      pool.emplace_back(work);
+    work();
+    for (auto& t : pool)
+      t.join();
+    if (!failure.empty())
+      throw std::runtime_error(failure);
     return 0;
     GUARD_END
   }

@@ -67,3 +67,20 @@ def test_flattened_mechanism_reproduces_micm_from_its_header():
         assert stats[0]["accepted"] == GOLDEN["stats"][s, 0]
         assert stats[0]["number_of_steps"] == GOLDEN["stats"][s, 2]
         inp = dict(inp, concentrations=y)
+
+
+@pytest.mark.skipif(not oracle.reference_available(), reason="oracle/_ref not built")
+def test_vector128_groups_solve_identical_cells_like_per_cell():
+    """The CPU baseline's micm_bench layout (vector ordering L = 128, one State
+    per 128 cells) takes the same steps as per-cell States on identical cells;
+    values agree within the solve's own absolute tolerance (1e-3, micm's
+    default, which micm_bench uses)."""
+    mech = ts1.mechanism()
+    ref = oracle.Reference(mech, tableau=ts1.TABLEAU)
+    inp = ts1.inputs(256)
+    y1, s1 = ref.solve_per_cell(inp, ts1.DT)
+    y2, s2 = ref.solve_groups_v128(inp, ts1.DT, group=128)
+    assert len(s2) == 2
+    for g in s2:
+        assert g[2] == s1[0, 2] and g[3] == s1[0, 3]      # number_of_steps, accepted
+    np.testing.assert_allclose(y2, y1, rtol=1e-6, atol=1e-3)
