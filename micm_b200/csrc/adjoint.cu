@@ -594,8 +594,7 @@ namespace micmb
         // ---- the accepted step's factor, stages and stage inputs ----
         const double alpha = 1.0 / (H * P.gamma0);
         jacobian_rates<1>(M, kk, y, scr, 0);
-        jacobian_gather<1>(M, scr, LU, alpha, true, 0);
-        lu_decompose<1>(M.lu_s, M.diag_row_of, LU, inv, 0);
+        lu_decompose_gathered(M, M.lu_s, M.diag_row_of, scr, alpha, LU, inv);  // -J + alpha I, then LU
         if (A.ckpt_k)
         {
           // stages stored by the forward pass; stage inputs rebuilt from them

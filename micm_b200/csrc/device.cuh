@@ -310,6 +310,40 @@ namespace micmb
     }
   }
 
+  // jacobian_gather (add_alpha) followed by lu_decompose on a serial schedule
+  // (every entry is one item, visited once, after the items it reads): each
+  // item starts from the value jacobian_gather would store for its entry --
+  // the gathered sum, then + alpha on the diagonal -- instead of reading it
+  // back, so the Jacobian never makes a round trip through memory.  Same
+  // operations in the same order as the two passes.
+  template<class DV, class AV, class IV>
+  __device__ __forceinline__ void lu_decompose_gathered(const DevMech& M, const DevSchedule& sch,
+                                                        const int32_t* diag_row, DV drate, double alpha, AV A, IV inv)
+  {
+    for (int32_t l = 0; l < sch.n_levels; ++l)
+    {
+      const int32_t end = sch.level_start[l + 1];
+      for (int32_t it = sch.level_start[l]; it < end; ++it)
+      {
+        const int32_t e = sch.target[it];
+        double v = 0.0;
+        for (int32_t t = M.j_start[e]; t < M.j_start[e + 1]; ++t)
+          v += M.j_coef[t] * drate[M.j_info[t]];
+        const int32_t dr = diag_row[e];
+        if (dr >= 0)
+          v += alpha;
+        for (int32_t t = sch.term_start[it]; t < sch.term_start[it + 1]; ++t)
+          v -= A[sch.ta[t]] * A[sch.tb[t]];
+        const int32_t aux = sch.aux[it];
+        if (aux >= 0)
+          v *= inv[diag_row[aux]];
+        A[e] = v;
+        if (aux != -2 && dr >= 0)
+          inv[dr] = 1.0 / v;
+      }
+    }
+  }
+
   // L y = b (unit diagonal), in place
   template<int NL, class AV, class XV>
   __device__ __forceinline__ void solve_lower(const DevSchedule& sch, AV A, XV x, int lane)

@@ -166,8 +166,7 @@ namespace micmb
         const double H = c.H;
         const double alpha = 1.0 / (H * P.gamma0);
         jacobian_rates<1>(M, kk, Y, scr, 0);
-        jacobian_gather<1>(M, scr, LU, alpha, true, 0);
-        lu_decompose<1>(M.lu_s, M.diag_row_of, LU, inv, 0);
+        lu_decompose_gathered(M, M.lu_s, M.diag_row_of, scr, alpha, LU, inv);  // -J + alpha I, then LU
         bool fc_is_src = false;
         for (int32_t st = 0; st < P.stages; ++st)
         {
