@@ -10,6 +10,7 @@ exceed the 126 MB L2, so no flush is needed between steps.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
     python bench.py --workload c600     # 600 species / 1,500 reactions, 262,144 cells
     python bench.py --workload ts1      # micm's TS1 benchmark mechanism, 1,048,576 cells, dt = 30 s
+    python bench.py --workload chapman  # micm_bench's default mechanism (Chapman), 1,048,576 cells
 
 N > 1 runs under torchrun: each rank solves its own 1M-cell shard (weak
 scaling; cells are independent, no collective on the data path).
@@ -49,6 +50,12 @@ WORKLOADS = {
                  l2="inputs exceed L2 (1.3 GB state + 3.1 GB rate constants); no flush",
                  adjoint=("c600", 262144, 160),
                  profile="k_fused_thread_c600_65536cells.md"),
+    "chapman": dict(cells=1048576, cpu_sample=262144,
+                    text="micm's Chapman benchmark mechanism (9 species, 7 reactions) on {cells} cells per GPU, "
+                         "micm_bench's initial state on every cell, 3-stage Rosenbrock, dt=30 s, fused persistent "
+                         "kernel",
+                    l2="inputs exceed L2 (75 MB state + 59 MB rate constants + 25 MB parameters); no flush",
+                    adjoint=None, profile="k_fused_thread_chapman_1M.md"),
     "ts1": dict(cells=1048576, cpu_sample=65536,
                 text="micm's TS1 benchmark mechanism (209 species, 547 reactions) on {cells} cells per GPU, "
                      "micm_bench's initial state on every cell, 3-stage Rosenbrock, dt=30 s, fused persistent kernel",
@@ -148,11 +155,11 @@ def job_throughput(cells_per_rank: int, world: int, steps: int, seconds: float) 
 
 def workload(name: str, cells: int, rank: int = 0):
     from micm_b200 import synthetic
-    if name == "ts1":
-        # micm_bench's TS1 case: the same initial state on every cell
-        from micm_b200 import ts1
-        cfg = dict(stages=ts1.TABLEAU, dt=ts1.DT, seed=0, inputs={})
-        return cfg, ts1.mechanism(), ts1.inputs(cells)
+    if name in ("ts1", "chapman"):
+        # micm_bench's cases: the benchmark's initial state on every cell
+        from micm_b200 import micm_bench
+        cfg = dict(stages=micm_bench.TABLEAU, dt=micm_bench.DT, seed=0, inputs={})
+        return cfg, micm_bench.mechanism(name), micm_bench.inputs(name, cells)
     cfg = synthetic.CONFIGS[name]
     mech = cfg["mech"]()
     inputs = synthetic.cell_inputs(mech, cells, cfg["seed"] + 1000 * rank, **cfg["inputs"])
@@ -213,7 +220,7 @@ def run_reference_arm(args):
     threads = os.cpu_count() or 1
     n = args.cpu_sample
     # identical cells (micm_bench's TS1 case): micm's vector-128 layout; else one 1-cell State per cell
-    uniform = args.workload == "ts1"
+    uniform = args.workload in ("ts1", "chapman")
     layout = ("vector ordering L=128, one State per 128 cells" if uniform else "1-cell micm States")
     times = []
     for i in range(args.warmup + args.steps):
@@ -565,7 +572,7 @@ def main():
 
     cpu = None
     if rank == 0 and not args.no_cpu:
-        cpu = cpu_reference(mech, cfg, inputs, args.cpu_sample, uniform=args.workload == "ts1")
+        cpu = cpu_reference(mech, cfg, inputs, args.cpu_sample, uniform=args.workload in ("ts1", "chapman"))
 
     if rank == 0:
         info = solver.compiled.info

@@ -1,5 +1,5 @@
 """micm's TS1 benchmark mechanism (test/benchmark/ts1_mechanism.hpp) as
-ingested from the fixture micm itself wrote (tests/golden/make_ts1.py): the
+ingested from the fixture micm itself wrote (tests/golden/make_micm_bench.py): the
 numbering equals micm's state, and the checkers reproduce micm's results on it."""
 import numpy as np
 import pytest
