@@ -595,6 +595,23 @@ namespace micm
       {
         return m_.y_dim_;
       }
+      // a whole row at once, as micm's VectorMatrix row proxy allows
+      // (state.variables_[cell] = {...} in micm_bench's InitState)
+      Row& operator=(const std::vector<T>& values)
+      {
+        if (values.size() != m_.y_dim_)
+          throw MicmException("MICM Matrix", 1, "Matrix row size mismatch in assignment from vector");
+        for (Index c = 0; c < m_.y_dim_; ++c)
+          (*this)[c] = values[c];
+        return *this;
+      }
+      operator std::vector<T>() const
+      {
+        std::vector<T> out(m_.y_dim_);
+        for (Index c = 0; c < m_.y_dim_; ++c)
+          out[c] = m_.data_[(row_ / L) * L * m_.y_dim_ + c * L + row_ % L];
+        return out;
+      }
     };
     class ConstRow
     {
@@ -610,6 +627,17 @@ namespace micm
       const T& operator[](Index col) const
       {
         return m_.data_[(row_ / L) * L * m_.y_dim_ + col * L + row_ % L];
+      }
+      Index Size() const
+      {
+        return m_.y_dim_;
+      }
+      operator std::vector<T>() const
+      {
+        std::vector<T> out(m_.y_dim_);
+        for (Index c = 0; c < m_.y_dim_; ++c)
+          out[c] = (*this)[c];
+        return out;
       }
     };
     VectorMatrix() = default;

@@ -48,3 +48,22 @@ def test_cpp_readme_example_on_gpu(cuda_device, readme_binary, method):
     r = subprocess.run([readme_binary, method], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     assert _rows(r.stdout) == [re.sub(r"\s+", " ", l) for l in README_TABLE]
+
+
+REFERENCE_BENCHMARK = os.path.join(os.environ.get("MICM_REFERENCE", "/root/reference"), "test", "benchmark")
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REFERENCE_BENCHMARK, "ts1_mechanism.hpp")),
+                    reason="micm's benchmark sources are not present")
+def test_micm_benchmark_mechanisms_build_unchanged(tmp_path):
+    """micm's own benchmark mechanisms (TS1, Chapman: test/benchmark/*_mechanism.hpp)
+    compile unchanged against this library's C++ API (include/micm/GPU.hpp,
+    CPU.hpp, util/property_keys.hpp serve micm's include names), link to
+    libmicmb.so and run up to the device (exit 3 without one)."""
+    out = str(tmp_path / "micm_bench_mechanisms")
+    subprocess.run(["g++", "-std=c++20", "-O1", "-I" + os.path.join(ROOT, "include"), "-I" + REFERENCE_BENCHMARK,
+                    os.path.join(ROOT, "tests", "cpp", "micm_bench_mechanisms.cpp"), "-o", out, "-L" + LIB_DIR,
+                    "-lmicmb", "-Wl,-rpath," + LIB_DIR], check=True)
+    if not _has_gpu():
+        r = subprocess.run([out], capture_output=True, text=True)
+        assert r.returncode == 3 and "no CUDA device" in r.stderr
