@@ -85,3 +85,99 @@ def micm_columns(name: str, path: Optional[str] = None) -> Dict[str, Dict[str, i
 def golden(name: str):
     """micm's results on the fixture's 4-cell state (tests/golden/<name>_micm.npz)."""
     return np.load(os.path.join(GOLDEN, f"{name}_micm.npz"))
+
+
+# ---------------------------------------------------------------------------
+# micm_bench's command line (test/benchmark/micm_bench.cpp,
+# test/benchmark/bench_harness.hpp), so scripts that drive micm's benchmark
+# can drive this library:
+#
+#   python -m micm_b200.micm_bench [num_cells] [num_steps] [dt_seconds] [backend] [matrix]
+#                                  [lu_type] [lu_algorithm] [mechanism]
+#
+# Same defaults, same "list" and error messages, same result line.  Backends:
+# "gpu" is micm's CUDA path (the plain per-stage kernels, one step size for
+# all cells); "gpu-fused" is this library's fused kernel with per-cell step
+# control.  Matrix "vector1|2|4|8|128" is the state's vector length; the LU
+# is the in-place Mozart one.
+# ---------------------------------------------------------------------------
+VECTOR_WIDTHS = (1, 2, 4, 8, 128)
+BACKENDS = {"gpu": ("plain", "global"), "gpu-fused": ("fused", "per_cell")}
+USAGE = " [num_cells] [num_steps] [dt_seconds] [backend] [matrix] [lu_type] [lu_algorithm] [mechanism]"
+
+
+def bench_keys():
+    return sorted(f"{m}/{b}/vector{L}/in-place/mozart" for m in NAMES for b in BACKENDS for L in VECTOR_WIDTHS)
+
+
+def run_case(mechanism_name: str, backend: str, vector_length: int, num_cells: int, num_steps: int,
+             dt: float) -> float:
+    """bench_harness.hpp RunCase + TimeSolve: build, GetState, the benchmark's
+    initial state, UpdateStateParameters once, one converged warm-up Solve,
+    num_steps timed Solve(dt) calls on the same state, one converged check
+    Solve.  Returns the elapsed milliseconds of the timed calls."""
+    import time
+    from .solver import Solver
+    method, step_control = BACKENDS[backend]
+    solver = Solver(mechanism(mechanism_name), TABLEAU, vector_length=vector_length)
+    state = solver.get_state(num_cells)
+    state.set_inputs(inputs(mechanism_name, num_cells))
+    state.sync_inputs_to_device()
+    solver.update_state_parameters(state)
+
+    def require_converged(result, when):
+        if not result.converged:
+            raise RuntimeError(f"the {when} solve did not converge ({result.state}) at dt={dt}; "
+                               "reduce dt or correct the initial conditions")
+
+    require_converged(solver.solve(dt, state, method=method, step_control=step_control), "warm-up")
+    t0 = time.perf_counter()
+    for _ in range(num_steps):
+        solver.solve(dt, state, method=method, step_control=step_control)
+    elapsed_ms = (time.perf_counter() - t0) * 1e3
+    require_converged(solver.solve(dt, state, method=method, step_control=step_control), "post-loop")
+    return elapsed_ms
+
+
+def main(argv=None) -> int:
+    import sys
+    argv = list(sys.argv if argv is None else argv)
+    prog = argv[0] if argv else "micm_bench"
+    args = argv[1:]
+    if args and args[0] == "list":
+        for key in bench_keys():
+            print(key)
+        return 0
+    try:
+        num_cells = int(args[0]) if len(args) > 0 else 10000
+        num_steps = int(args[1]) if len(args) > 1 else 100
+        dt = float(args[2]) if len(args) > 2 else 30.0
+        if num_cells < 0 or num_steps < 0:
+            raise ValueError("negative count")
+    except ValueError as e:
+        print(f"Could not read the arguments: {e}")
+        print(f"Usage: {prog}{USAGE}")
+        return 1
+    backend = args[3] if len(args) > 3 else "cpu"
+    matrix = args[4] if len(args) > 4 else "standard"
+    lu_matrix = args[5] if len(args) > 5 else "in-place"
+    lu = args[6] if len(args) > 6 else "mozart"
+    mech = args[7] if len(args) > 7 else "chapman"
+    key = f"{mech}/{backend}/{matrix}/{lu_matrix}/{lu}"
+    if key not in bench_keys():
+        print(f"Invalid option combination: {key}")
+        print(f"Run '{prog} list' to print every valid combination.")
+        return 1
+    try:
+        elapsed_ms = run_case(mech, backend, int(matrix[len("vector"):]), num_cells, num_steps, dt)
+    except Exception as e:  # noqa: BLE001 -- micm_bench reports any failure this way
+        print(f"Benchmark failed: {e}")
+        return 1
+    per_step = elapsed_ms / num_steps if num_steps else float("nan")
+    print(f"mechanism={mech} backend={backend} matrix_type={matrix} lu={lu}/{lu_matrix} cells={num_cells} "
+          f"steps={num_steps} dt={dt:g} elapsed_ms={elapsed_ms:.3f} ms_per_step={per_step:.3f}")
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
