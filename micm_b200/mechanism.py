@@ -186,8 +186,9 @@ def mechanism_from_dict(d: dict) -> Mechanism:
     ``reactions``: ``[{"kind", "params", "reactants": [names], "products":
     [[name, yield]], "label"?}]`` in input order, ``params`` as the rate
     helpers of this module take them; optional ``absolute_tolerance`` (one
-    value or one per species; micm's builder default 1e-3 otherwise) and
-    ``relative_tolerance``."""
+    value or one per species; micm's builder default 1e-3 otherwise),
+    ``relative_tolerance`` and ``reorder_state`` (micm's SetReorderState,
+    default true)."""
     species = list(d["species"])
     index = {n: i for i, n in enumerate(species)}
     params = d.get("parameterized", [])
@@ -197,7 +198,8 @@ def mechanism_from_dict(d: dict) -> Mechanism:
         atol = np.broadcast_to(np.asarray(atol, dtype=np.float64), (len(species),)).copy()
     m = Mechanism(species=species, reactions=[], name=d.get("name", "mechanism"),
                   parameterized=[tuple(float(c) for c in p["coefficients"]) for p in params],
-                  absolute_tolerance=atol, relative_tolerance=float(d.get("relative_tolerance", 1e-6)))
+                  absolute_tolerance=atol, relative_tolerance=float(d.get("relative_tolerance", 1e-6)),
+                  reorder_state=bool(d.get("reorder_state", True)))
 
     def reactant(name):
         if name in index:
@@ -218,6 +220,43 @@ def mechanism_from_dict(d: dict) -> Mechanism:
         m.reactions.append(Reaction(kind, [float(v) for v in rx["params"]],
                                     [reactant(n) for n in rx["reactants"]], products, rx.get("label")))
     return m
+
+
+_NAME_BY_KIND = {v: k for k, v in _KIND_BY_NAME.items()}
+
+
+def mechanism_to_dict(m: Mechanism, parameterized_names: Optional[Sequence[str]] = None) -> dict:
+    """The JSON description mechanism_from_dict reads (parameterized reactants
+    are named param0, param1, ... unless names are given)."""
+    pnames = list(parameterized_names) if parameterized_names else [f"param{i}" for i in range(len(m.parameterized))]
+
+    def reactant(i):
+        return m.species[i] if i >= 0 else pnames[-i - 1]
+
+    reactions = []
+    for rx in m.reactions:
+        d = {"kind": _NAME_BY_KIND[rx.kind], "params": [float(v) for v in rx.params],
+             "reactants": [reactant(i) for i in rx.reactants],
+             "products": [[m.species[s], float(y)] for s, y in rx.products]}
+        if rx.label is not None:
+            d["label"] = rx.label
+        reactions.append(d)
+    out = {"name": m.name, "species": list(m.species),
+           "parameterized": [{"name": n, "coefficients": [float(c) for c in coef]}
+                             for n, coef in zip(pnames, m.parameterized)],
+           "reactions": reactions, "relative_tolerance": float(m.relative_tolerance)}
+    if m.absolute_tolerance is not None:
+        out["absolute_tolerance"] = [float(v) for v in m.absolute_tolerance]
+    if not m.reorder_state:
+        out["reorder_state"] = False
+    return out
+
+
+def save_mechanism_json(m: Mechanism, path: str):
+    """mechanism_to_dict written to a JSON file."""
+    import json
+    with open(path, "w") as f:
+        json.dump(mechanism_to_dict(m), f, indent=1)
 
 
 def load_mechanism_json(path: str) -> Mechanism:

@@ -84,3 +84,16 @@ def test_vector128_groups_solve_identical_cells_like_per_cell():
     for g in s2:
         assert g[2] == s1[0, 2] and g[3] == s1[0, 3]      # number_of_steps, accepted
     np.testing.assert_allclose(y2, y1, rtol=1e-6, atol=1e-3)
+
+
+def test_json_description_round_trips():
+    """mechanism_to_dict / mechanism_from_dict keep every field micm's numbering and the kernels use."""
+    from micm_b200.mechanism import mechanism_from_dict, mechanism_to_dict
+    from mechanisms import all_rate_types
+    for m in (ts1.mechanism(), all_rate_types()):
+        back = mechanism_from_dict(mechanism_to_dict(m))
+        np.testing.assert_array_equal(CompiledMechanism(back).species_columns, CompiledMechanism(m).species_columns)
+        for key, a in m.flat().items():
+            np.testing.assert_array_equal(np.asarray(back.flat()[key]), np.asarray(a), err_msg=key)
+        assert back.custom_param_labels() == m.custom_param_labels()
+        np.testing.assert_array_equal(back.atol(), m.atol())
