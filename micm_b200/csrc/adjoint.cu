@@ -2,11 +2,12 @@
 // per-cell fused solve (no counterpart in micm).
 //
 // The forward solve (SolveFused with checkpointing) stores, for every accepted
-// step n of every cell, the starting state y_n and the step size H_n.  This
-// kernel then walks each cell's steps backwards.  For step n it recomputes
-// F(y_n), alpha I - J(y_n), the LU factor and the stages K_s exactly as the
-// forward pass did (same warp routines, so the same bits), and applies the
-// transposed step with the step size held fixed:
+// step n of every cell, the starting state y_n, the step size H_n and (where
+// memory allows) the stage vectors K_s.  The backward sweep, one cell per
+// thread, then walks each cell's steps backwards.  For step n it rebuilds
+// alpha I - J(y_n) and its LU factor, takes the stored stages or recomputes
+// them exactly as the forward pass did (same routines, so the same bits), and
+// applies the transposed step with the step size held fixed:
 //
 //   y_{n+1} = y_n + sum_s m_s K_s,   M K_s = F(Y_s) + sum_{j<s} (c_sj / H) K_j,
 //   M = 1/(H gamma_0) I - J(y_n),    Y_s = y_n + sum_{j<s} a_sj K_j
@@ -29,17 +30,11 @@ namespace micmb
 {
   namespace
   {
-    constexpr int kWarp = 32;
     constexpr int kMaxAdjStages = 6;
 
     __device__ __forceinline__ size_t cell_base(int64_t c, int32_t L, int32_t ncol)
     {
       return (size_t)(c / L) * (size_t)L * (size_t)ncol + (size_t)(c % L);
-    }
-
-    __host__ __device__ inline int32_t RoundUp2(int32_t v)
-    {
-      return (v + 1) & ~1;
     }
 
     struct AdjArgs
@@ -56,284 +51,11 @@ namespace micmb
       const int32_t* n_ckpt;         // [cell]
       double* ybar0;                 // vector layout [S]
       double* kbar;                  // [cell][R]
-      double* lu_global;             // per-warp LU slots (nullptr: LU in shared memory)
-      int64_t lu_slot_stride;
       int32_t* next_cell;
       const int32_t* order;          // cells in decreasing step count (thread kernel), or null
     };
 
-    struct AdjLayout
-    {
-      int32_t VS, KS, SC, LUS, per_warp;  // doubles
-    };
-
-    __host__ __device__ inline AdjLayout MakeAdjLayout(int32_t S, int32_t R, int32_t stages, int32_t n_info,
-                                                       int32_t nnz, bool lu_shared)
-    {
-      AdjLayout l;
-      l.VS = RoundUp2(S + 1);
-      l.KS = RoundUp2(R > 0 ? R : 1);
-      l.SC = RoundUp2((R > n_info ? R : n_info) + 1);
-      l.LUS = lu_shared ? RoundUp2(nnz + 1) : 0;
-      // y, F0, Fc, inv, yb, tmp + stage inputs, stages, Kbar, Gbar, Rbar
-      l.per_warp = l.VS * (6 + 5 * stages) + 2 * l.KS + l.SC + l.LUS;
-      return l;
-    }
-
-    // nu_r . v  (products with their yields, then reactants), as the oracle's nu_dot
-    __device__ __forceinline__ double nu_dot(const DevMech& M, int32_t r, const double* v)
-    {
-      double s = 0.0;
-      for (int32_t i = M.prod_start[r]; i < M.prod_start[r + 1]; ++i)
-        s += M.prod_yield[i] * v[M.prod_ids[i]];
-      for (int32_t i = M.react_start[r]; i < M.react_start[r + 1]; ++i)
-        s -= v[M.react_ids[i]];
-      return s;
-    }
-
-    // product of the reactant concentrations of r skipping occurrences a and b (-1: none)
-    __device__ __forceinline__ double prod_except(const DevMech& M, int32_t r, const double* y, int32_t a, int32_t b)
-    {
-      double v = 1.0;
-      for (int32_t i = M.react_start[r]; i < M.react_start[r + 1]; ++i)
-        if (i != a && i != b)
-          v *= y[M.react_ids[i]];
-      return v;
-    }
-
-    // yb += J(y)^T g ; kb[r] += (nu_r . g) w_r(y).  Lanes own reactions; the
-    // species sums take shared-memory atomics.
-    __device__ void vjp_f(const DevMech& M, const double* kk, const double* y, const double* g, double* yb,
-                          double* kb, int lane)
-    {
-      for (int32_t r = lane; r < M.R; r += kWarp)
-      {
-        const double c = nu_dot(M, r, g);
-        if (c == 0.0)
-          continue;
-        kb[r] += c * (kk[r] * prod_except(M, r, y, -1, -1));
-        for (int32_t i = M.react_start[r]; i < M.react_start[r + 1]; ++i)
-          atomicAdd(yb + M.react_ids[i], c * kk[r] * prod_except(M, r, y, i, -1));
-      }
-    }
-
-    // second-order term of M's dependence on y: for rho = nu_r . Rbar and the
-    // direction K, yb += rho H_r K and kb[r] += rho (grad w_r . K)
-    __device__ void jacobian_term(const DevMech& M, const double* kk, const double* y, const double* Rb,
-                                  const double* Kv, double* yb, double* kb, int lane)
-    {
-      for (int32_t r = lane; r < M.R; r += kWarp)
-      {
-        const double rho = nu_dot(M, r, Rb);
-        if (rho == 0.0)
-          continue;
-        const int32_t r0 = M.react_start[r], r1 = M.react_start[r + 1];
-        double gk = 0.0;
-        for (int32_t i = r0; i < r1; ++i)
-          gk += kk[r] * prod_except(M, r, y, i, -1) * Kv[M.react_ids[i]];
-        kb[r] += rho * gk;
-        for (int32_t i = r0; i < r1; ++i)
-          for (int32_t j = r0; j < r1; ++j)
-            if (i != j)
-              atomicAdd(yb + M.react_ids[j], rho * kk[r] * prod_except(M, r, y, i, j) * Kv[M.react_ids[i]]);
-      }
-    }
-
-    __global__ void __launch_bounds__(256) k_adjoint(DevMech M, DevParams P, AdjArgs A, AdjLayout W)
-    {
-      extern __shared__ __align__(16) double smem[];
-      const int warp = threadIdx.x >> 5;
-      const int lane = threadIdx.x & 31;
-      const int warps = blockDim.x >> 5;
-      const int32_t S = M.S, R = M.R, L = A.L, ns = P.stages, VS = W.VS;
-      double* base = smem + (size_t)warp * W.per_warp;
-      double* y = base;
-      double* F0 = y + VS;
-      double* Fc = F0 + VS;
-      double* inv = Fc + VS;
-      double* yb = inv + VS;
-      double* tmp = yb + VS;
-      double* Ys = tmp + VS;                 // [ns][VS]
-      double* K = Ys + (size_t)ns * VS;      // [ns][VS]
-      double* Kb = K + (size_t)ns * VS;      // [ns][VS]
-      double* Gb = Kb + (size_t)ns * VS;     // [ns][VS]
-      double* Rb = Gb + (size_t)ns * VS;     // [ns][VS]
-      double* kk = Rb + (size_t)ns * VS;
-      double* kb = kk + W.KS;
-      double* scr = kb + W.KS;
-      double* LU = W.LUS ? scr + W.SC : A.lu_global + ((size_t)blockIdx.x * warps + warp) * (size_t)A.lu_slot_stride;
-      if (lane == 0)
-      {
-        for (int32_t st = 0; st < ns; ++st)
-        {
-          K[(size_t)st * VS + S] = 0.0;
-          Rb[(size_t)st * VS + S] = 0.0;
-        }
-        scr[M.scratch_zero] = 0.0;
-        LU[M.nnz] = 0.0;
-      }
-      __syncwarp();
-
-      for (;;)
-      {
-        int32_t cell = 0;
-        if (lane == 0)
-          cell = atomicAdd(A.next_cell, 1);
-        cell = __shfl_sync(0xffffffffu, cell, 0);
-        if (cell >= A.n_cells)
-          break;
-        const size_t by = cell_base(cell, L, S);
-        const size_t bk = cell_base(cell, L, R);
-        for (int32_t r = lane; r < R; r += kWarp)
-        {
-          kk[r] = A.rate_constants[bk + (size_t)r * L];
-          kb[r] = 0.0;
-        }
-        const int32_t n_ck = A.n_ckpt[cell];
-        if (n_ck <= 0)
-          for (int32_t i = lane; i < S; i += kWarp)
-            yb[i] = (A.y0[by + (size_t)i * L] < 0.0) ? 0.0 : A.ybar_final[by + (size_t)i * L];
-        __syncwarp();
-
-        for (int32_t n = n_ck - 1; n >= 0; --n)
-        {
-          const double* yc = A.ckpt_y + ((size_t)cell * A.max_ckpt + n) * S;
-          const double H = A.ckpt_h[(size_t)cell * A.max_ckpt + n];
-          for (int32_t i = lane; i < S; i += kWarp)
-            y[i] = yc[i];
-          __syncwarp();
-          // ---- recompute the accepted step (same routines and order as the forward) ----
-          reaction_rates<kWarp>(M, Unit{ kk }, Unit{ y }, Unit{ scr }, lane);
-          __syncwarp();
-          warp_gather(M.w_forcing, scr, F0, 0.0, lane);
-          __syncwarp();
-          const double alpha = 1.0 / (H * P.gamma0);
-          jacobian_rates<kWarp>(M, Unit{ kk }, Unit{ y }, Unit{ scr }, lane);
-          __syncwarp();
-          warp_gather(M.w_jacobian, scr, LU, alpha, lane);
-          __syncwarp();
-          warp_lu(M.w_lu, LU, inv, lane);
-          const double* Fsrc = F0;
-          for (int32_t st = 0; st < ns; ++st)
-          {
-            const int32_t sc = st * (st - 1) / 2;
-            double* Yst = Ys + (size_t)st * VS;
-            if (st > 0 && P.new_f[st])
-            {
-              for (int32_t i = lane; i < S; i += kWarp)
-              {
-                double v = y[i];
-                for (int32_t j = 0; j < st; ++j)
-                  v += P.a[sc + j] * K[(size_t)j * VS + i];
-                Yst[i] = v;
-              }
-              __syncwarp();
-              reaction_rates<kWarp>(M, Unit{ kk }, Unit{ Yst }, Unit{ scr }, lane);
-              __syncwarp();
-              warp_gather(M.w_forcing, scr, Fc, 0.0, lane);
-              __syncwarp();
-              Fsrc = Fc;
-            }
-            else
-              for (int32_t i = lane; i < S; i += kWarp)
-                Yst[i] = y[i];
-            double* Ks = K + (size_t)st * VS;
-            for (int32_t i = lane; i < S; i += kWarp)
-            {
-              double v = Fsrc[i];
-              for (int32_t j = 0; j < st; ++j)
-              {
-                const double c_over_h = P.c[sc + j] / H;
-                v += c_over_h * K[(size_t)j * VS + i];
-              }
-              Ks[i] = v;
-            }
-            __syncwarp();
-            warp_solve(M.w_fwd, LU, Ks, lane);
-            warp_solve(M.w_bwd, LU, Ks, lane);
-          }
-          if (n == n_ck - 1)
-          {
-            // derivative of the final clamp max(y, 0) at the unclamped result
-            for (int32_t i = lane; i < S; i += kWarp)
-            {
-              double v = y[i];
-              for (int32_t st = 0; st < ns; ++st)
-                v += P.m[st] * K[(size_t)st * VS + i];
-              yb[i] = (v < 0.0) ? 0.0 : A.ybar_final[by + (size_t)i * L];
-            }
-            __syncwarp();
-          }
-          // ---- reverse sweep ----
-          for (int32_t i = lane; i < S; i += kWarp)
-          {
-            const double g = yb[i];
-            for (int32_t st = 0; st < ns; ++st)
-            {
-              Kb[(size_t)st * VS + i] = P.m[st] * g;
-              Gb[(size_t)st * VS + i] = 0.0;
-            }
-          }
-          __syncwarp();
-          for (int32_t st = ns - 1; st >= 0; --st)
-          {
-            const int32_t sc = st * (st - 1) / 2;
-            double* rb = Rb + (size_t)st * VS;
-            for (int32_t i = lane; i < S; i += kWarp)
-              rb[i] = Kb[(size_t)st * VS + i];
-            __syncwarp();
-            warp_solve(M.w_fwd_t, LU, rb, lane);  // U^T w = Kbar
-            warp_solve(M.w_bwd_t, LU, rb, lane);  // L^T z = w
-            for (int32_t i = lane; i < S; i += kWarp)
-            {
-              const double v = rb[i];
-              Gb[(size_t)st * VS + i] += v;
-              for (int32_t j = 0; j < st; ++j)
-              {
-                const double c_over_h = P.c[sc + j] / H;
-                Kb[(size_t)j * VS + i] += c_over_h * v;
-              }
-            }
-            __syncwarp();
-            if (st == 0)
-              continue;
-            if (P.new_f[st])
-            {
-              for (int32_t i = lane; i < S; i += kWarp)
-                tmp[i] = 0.0;
-              __syncwarp();
-              vjp_f(M, kk, Ys + (size_t)st * VS, Gb + (size_t)st * VS, tmp, kb, lane);
-              __syncwarp();
-              for (int32_t i = lane; i < S; i += kWarp)
-              {
-                const double t = tmp[i];
-                yb[i] += t;
-                for (int32_t j = 0; j < st; ++j)
-                  Kb[(size_t)j * VS + i] += P.a[sc + j] * t;
-              }
-            }
-            else
-              for (int32_t i = lane; i < S; i += kWarp)
-                Gb[(size_t)(st - 1) * VS + i] += Gb[(size_t)st * VS + i];
-            __syncwarp();
-          }
-          vjp_f(M, kk, y, Gb, yb, kb, lane);
-          __syncwarp();
-          for (int32_t st = 0; st < ns; ++st)
-          {
-            jacobian_term(M, kk, y, Rb + (size_t)st * VS, K + (size_t)st * VS, yb, kb, lane);
-            __syncwarp();
-          }
-        }
-        for (int32_t i = lane; i < S; i += kWarp)
-          A.ybar0[by + (size_t)i * L] = yb[i];
-        for (int32_t r = lane; r < R; r += kWarp)
-          A.kbar[(size_t)cell * R + r] = kb[r];
-        __syncwarp();
-      }
-    }
-
-    // ---- one cell per thread: the same recurrences over private working sets ----
+    // ---- one cell per thread, private working sets in global memory ----
 
     // entry offsets of a thread's working set (each entry is 32 doubles, one per lane)
     struct AdjThreadLayout
@@ -903,56 +625,6 @@ namespace micmb
 
   void LaunchAdjoint(micmb_solver& s, micmb_state& st, int32_t max_ckpt, int64_t begin, int64_t count)
   {
-    const auto& m = *s.mech;
-    if (s.fused.variant != 1)
-    {
-      LaunchAdjointThread(s, st, max_ckpt, begin, count);
-      return;
-    }
-    if (!s.dev.has_warp)
-      throw Error(MICMB_ERR_UNSUPPORTED, "mechanism exceeds the fused kernel's 16-bit table positions");
-    if (s.params.stages > kMaxAdjStages)
-      throw Error(MICMB_ERR_UNSUPPORTED, "too many stages for the adjoint kernel");
-    bool lu_shared = true;
-    AdjLayout W = MakeAdjLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz, true);
-    int warps = (int)std::min<size_t>(8, s.smem_optin / ((size_t)W.per_warp * sizeof(double)));
-    if (warps < 1)
-    {
-      lu_shared = false;
-      W = MakeAdjLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz, false);
-      warps = (int)std::min<size_t>(8, s.smem_optin / ((size_t)W.per_warp * sizeof(double)));
-    }
-    if (warps < 1)
-      throw Error(MICMB_ERR_UNSUPPORTED, "mechanism too large for the adjoint kernel's shared-memory working set");
-    const size_t smem = (size_t)W.per_warp * sizeof(double) * warps;
-    MICMB_CUDA(cudaFuncSetAttribute(k_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    MICMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adjoint, warps * kWarp, smem));
-    if (per_sm < 1)
-      throw Error(MICMB_ERR_UNSUPPORTED, "adjoint kernel cannot be resident");
-    const int64_t n = count;
-    int64_t grid = (int64_t)per_sm * s.sm_count;
-    grid = std::max<int64_t>(1, std::min<int64_t>(grid, (n + warps - 1) / warps));
-
-    AdjArgs A = ChunkArgs(s, st, max_ckpt, begin, count);
-    A.ckpt_k = nullptr;  // the warp kernel recomputes the stages
-    if (!lu_shared)
-    {
-      const int64_t slots = grid * warps;
-      const int64_t stride = ((int64_t)m.nnz + 1 + 31) & ~31ll;
-      if (st.lu_slot_count < slots * stride || !st.lu_slots.p)
-      {
-        st.lu_slots = DeviceMemory(sizeof(double) * (size_t)(slots * stride));
-        st.lu_slot_count = slots * stride;
-      }
-      A.lu_global = st.lu_slots.as<double>();
-      A.lu_slot_stride = stride;
-    }
-    MICMB_CUDA(cudaMemsetAsync(A.next_cell, 0, 8, st.stream));
-    if (n > 0)
-    {
-      k_adjoint<<<(unsigned)grid, warps * kWarp, smem, st.stream>>>(s.dev, s.params, A, W);
-      MICMB_CUDA(cudaGetLastError());
-    }
+    LaunchAdjointThread(s, st, max_ckpt, begin, count);
   }
 }  // namespace micmb
