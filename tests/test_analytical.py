@@ -159,3 +159,76 @@ def test_gpu_matches_closed_form(cuda_device, family, method, step_control):
         assert res.converged
         st.sync_outputs_to_host()
         np.testing.assert_allclose(st.concentrations(), closed_form(family, inp, float(step)), rtol=0, atol=tol)
+
+
+# ---------------------------------------------------------------------------
+# The "super stiff but analytical" variants (analytical_policy.hpp
+# TestSimpleStiffSystem :278-408 with TestAnalyticalStiffTroe :479-572 and the
+# other Stiff* families): A split into A1 and A2 that convert into each other
+# at 4e10 and 3.6e10 s-1, both decaying to B with k1; A = A1 + A2 follows the
+# same closed form.  Tolerances are micm's, per family and tableau
+# (test/integration/test_analytical_rosenbrock.cpp:356-569).
+# ---------------------------------------------------------------------------
+def _stiff_arrhenius_k2(T, P, rho):
+    return 1.2e-4 * math.exp(75 / T) * math.pow(T / 50, 1.6) * (1.0 + 0.5 * P)
+
+
+# family -> (rate A -> B (for A1 and A2), rate B -> C, custom parameters, k1, k2, {tableau: tolerance})
+STIFF_FAMILIES = {
+    "troe": (troe(k0_A=4.0e-11), troe(1.2e-3, 1.6, 3.0, 136.0, 5.0, 24.0, 0.9, 0.8), [],
+             _troe_k1, _troe_k2, {t: 1e-5 for t in (2, 3, 4, 40, 60)}),
+    "photolysis": (None, user_defined("photoB"), [2e-3, 2e-3, 3e-3],
+                   lambda T, P, rho: 2e-3, lambda T, P, rho: 3e-3, {t: 2e-5 for t in (2, 3, 4, 40, 60)}),
+    "ternary_chemical_activation": (ternary(k0_A=4.0e-5, kinf_A=1.0), ternary(1.2e-3, 1.6, 3.0, 136.0, 5.0, 24.0, 0.9, 0.8),
+                                    [], _ternary_k1, _ternary_k2, {t: 2e-3 for t in (2, 3, 4, 40, 60)}),
+    "tunneling": (tunneling(A=4.0e-3), tunneling(A=1.2e-4, B=167.0, C=1.0e8), [],
+                  lambda T, P, rho: 4.0e-3, lambda T, P, rho: 1.2e-4 * math.exp(-167 / T + 1.0e8 / math.pow(T, 3)),
+                  {t: 1e-4 for t in (2, 3, 4, 40, 60)}),
+    "arrhenius": (arrhenius(A=4.0e-3, C=50.0), arrhenius(A=1.2e-4, B=1.6, C=75.0, D=50.0, E=0.5), [],
+                  lambda T, P, rho: 4.0e-3 * math.exp(50 / T), _stiff_arrhenius_k2,
+                  {2: 1e-4, 3: 2e-5, 4: 2e-5, 40: 2e-5, 60: 1e-5}),
+    "branched": (branched(0, 1e-4, 204.3, 1.0e-3, 2), branched(1, 1e-4, 204.3, 1.0e-3, 2), [],
+                 lambda T, P, rho: _branched(T, rho, False), lambda T, P, rho: _branched(T, rho, True),
+                 {t: 2e-3 for t in (2, 3, 4, 40, 60)}),
+}
+
+
+def stiff_system(family):
+    r_ab, r_bc = STIFF_FAMILIES[family][:2]
+    m = Mechanism(species=["A1", "A2", "B", "C"], reactions=[], name=family + "_stiff")
+    if family == "photolysis":
+        m.add(user_defined("photoA1B"), [0], [(2, 1.0)])
+        m.add(user_defined("photoA2B"), [1], [(2, 1.0)])
+    else:
+        m.add(r_ab, [0], [(2, 1.0)])
+        m.add(r_ab, [1], [(2, 1.0)])
+    m.add(r_bc, [2], [(3, 1.0)])
+    m.add(arrhenius(A=4.0e10), [0], [(1, 1.0)])
+    m.add(arrhenius(A=0.9 * 4.0e10), [1], [(0, 1.0)])
+    return m
+
+
+@pytest.mark.skipif(not oracle.restatement_available(), reason="oracle not built")
+@pytest.mark.parametrize("tableau", [2, 3, 4, 40, 60])
+@pytest.mark.parametrize("family", sorted(STIFF_FAMILIES))
+def test_restatement_matches_stiff_closed_form(family, tableau):
+    k1f, k2f, tols = STIFF_FAMILIES[family][3:6]
+    R = oracle.Restatement(stiff_system(family), tableau_kind=tableau)
+    T, P = np.array(TEMPERATURES), np.array(PRESSURES)
+    rho = P / (GAS_CONSTANT * T)
+    params = np.tile(np.array(STIFF_FAMILIES[family][2], dtype=np.float64), (3, 1)).reshape(3, -1)
+    a0 = np.array([1.0 - i / 3.0 for i in range(3)])
+    y0 = np.stack([0.5 * a0, 0.5 * a0, np.zeros(3), np.zeros(3)], axis=1)
+    cur = dict(temperature=T, pressure=P, air_density=rho, concentrations=y0, custom_params=params)
+    for step in range(1, NSTEPS):
+        y, stats = R.solve_per_cell(cur, 1.0, threads=1)
+        assert np.all(stats[:, 7] == 2)
+        cur = dict(cur, concentrations=y)
+        model = np.stack([y[:, 0] + y[:, 1], y[:, 2], y[:, 3]], axis=1)
+        want = np.empty((3, 3))
+        for i in range(3):
+            k1, k2 = k1f(T[i], P[i], rho[i]), k2f(T[i], P[i], rho[i])
+            t = float(step)
+            want[i] = [a0[i] * math.exp(-k1 * t), a0[i] * (k1 / (k2 - k1)) * (math.exp(-k1 * t) - math.exp(-k2 * t)),
+                       a0[i] * (1.0 + (k1 * math.exp(-k2 * t) - k2 * math.exp(-k1 * t)) / (k2 - k1))]
+        np.testing.assert_allclose(model, want, rtol=0, atol=tols[tableau])
