@@ -232,3 +232,38 @@ def test_restatement_matches_stiff_closed_form(family, tableau):
             want[i] = [a0[i] * math.exp(-k1 * t), a0[i] * (k1 / (k2 - k1)) * (math.exp(-k1 * t) - math.exp(-k2 * t)),
                        a0[i] * (1.0 + (k1 * math.exp(-k2 * t) - k2 * math.exp(-k1 * t)) / (k2 - k1))]
         np.testing.assert_allclose(model, want, rtol=0, atol=tols[tableau])
+
+
+# ---------------------------------------------------------------------------
+# Surface reaction on an aerosol mode (test/integration/analytical_surface_rxn_policy.hpp:
+# foo -> bar + 0.4 baz on a lognormal mode, ten steps of 0.1 / k1, relative
+# tolerances per tableau from test_analytical_rosenbrock.cpp:574-578).
+# ---------------------------------------------------------------------------
+SURFACE_TOLERANCE = {2: 1e-2, 3: 1e-5, 4: 1e-6, 40: 1e-5, 60: 1e-7}
+
+
+@pytest.mark.skipif(not oracle.restatement_available(), reason="oracle not built")
+@pytest.mark.parametrize("tableau", [2, 3, 4, 40, 60])
+def test_restatement_matches_surface_closed_form(tableau):
+    from micm_b200.mechanism import surface
+    gmd, gsd, mw, dg, gamma = 1.0e-6, 0.1, 0.04607, 0.95e-5, 2.0e-2
+    T, P = 272.5, 101253.3
+    radius = gmd / 2.0 * math.exp(5.0 * math.log(gsd) * math.log(gsd) / 2.0)
+    number = 6.0 / (math.pi * math.pow(gmd, 3.0) * math.exp(9.0 / 2.0 * math.log(gsd) * math.log(gsd))) * \
+        (2.0e-3 / 1000.0 + 3.0e-3 / 1000.0)
+    m = Mechanism(species=["foo", "bar", "baz"], reactions=[], name="surface")
+    m.add(surface("foo", dg, mw, gamma), [0], [(1, 1.0), (2, 0.4)])
+    R = oracle.Restatement(m, tableau_kind=tableau)
+    speed = math.sqrt(8.0 * GAS_CONSTANT / (math.pi * mw) * T)
+    k1 = 4.0 * number * math.pi * radius * radius / (radius / dg + 4.0 / (speed * gamma))
+    inp = dict(temperature=np.array([T]), pressure=np.array([P]), air_density=np.array([P / (GAS_CONSTANT * T)]),
+               concentrations=np.array([[1.0, 0.0, 0.0]]), custom_params=np.array([[radius, number]]))
+    k = R.rate_constants(inp["temperature"], inp["pressure"], inp["air_density"], inp["custom_params"])
+    assert abs(k[0, 0] - k1) <= 1e-8
+    dt = 0.1 / k1
+    for i in range(1, 11):
+        y, stats = R.solve_per_cell(inp, dt, threads=1)
+        assert stats[0, 7] == 2
+        inp = dict(inp, concentrations=y)
+        foo = math.exp(-k1 * i * dt)
+        np.testing.assert_allclose(y[0], [foo, 1.0 - foo, 0.4 * (1.0 - foo)], rtol=SURFACE_TOLERANCE[tableau])
