@@ -1,5 +1,8 @@
-"""Robertson's stiff chemical kinetics problem as micm's integration test sets
-it up (test/integration/analytical_policy.hpp:1380-1536: A -> B (0.04),
+"""Classic stiff problems as micm's integration tests set them up, with the C
+restatement (and, for Robertson, the GPU) following micm itself at every
+output.
+
+Robertson's stiff chemical kinetics problem (test/integration/analytical_policy.hpp:1380-1536: A -> B (0.04),
 B + B -> B + C (3e7), B + C -> A + C (1e4), air density 1e6, relative
 tolerance 1e-10, absolute 1e-12, outputs at t = 1, 10, ..., 1e11).  micm's
 test checks micm against a published reference solution; here the C
@@ -76,3 +79,52 @@ def test_gpu_follows_micm(cuda_device, tableau, method, step_control):
         assert res.converged and res.stats["accepted"] == acc
         st.sync_outputs_to_host()
         np.testing.assert_allclose(st.concentrations()[0], y_micm, rtol=1e-6, atol=1e-30)
+
+
+# ---------------------------------------------------------------------------
+# E5 (analytical_policy.hpp TestAnalyticalE5 :2018-: A1 -> A2 + A3 (7.89e-10),
+# A2 + A3 -> A5 (1.13e9), A1 + A3 -> A4 (1.1e7), A4 -> A3 + A6 (1.13e3);
+# relative tolerance 1e-13, absolute 1e-17 (1e-7 for A1, A5, A6); outputs at
+# t = 10, 1e3, ..., 1e13).  micm's test checks micm against a published
+# reference solution; the restatement is checked against micm itself.
+# Tableaus that cover every output interval within micm's 1,000 steps per
+# Solve: 3-stage, 4-stage and both DA ones.
+# ---------------------------------------------------------------------------
+def e5():
+    atol = np.full(6, 1e-17)
+    atol[[0, 4, 5]] = 1e-7
+    m = Mechanism(species=["A1", "A2", "A3", "A4", "A5", "A6"], reactions=[], name="e5", reorder_state=False,
+                  absolute_tolerance=atol, relative_tolerance=1e-13)
+    m.add(user_defined("r1"), [0], [(1, 1.0), (2, 1.0)])
+    m.add(user_defined("r2"), [1, 2], [(4, 1.0)])
+    m.add(user_defined("r3"), [0, 2], [(3, 1.0)])
+    m.add(user_defined("r4"), [3], [(2, 1.0), (5, 1.0)])
+    return m
+
+
+def e5_inputs():
+    return dict(temperature=np.array([272.5]), pressure=np.array([101253.3]), air_density=np.array([1.0]),
+                concentrations=np.array([[1.76e-3, 0.0, 0.0, 0.0, 0.0, 0.0]]),
+                custom_params=np.array([[7.89e-10, 1.13e9, 1.1e7, 1.13e3]]))
+
+
+def e5_intervals():
+    t, target = 0.0, 10.0
+    for _ in range(7):
+        yield target - t
+        t, target = target, target * 100
+
+
+@pytest.mark.skipif(not oracle.restatement_available(), reason="oracle not built")
+@pytest.mark.parametrize("tableau", [3, 4, 40, 60])
+def test_e5_restatement_follows_micm(tableau):
+    ref = oracle.Reference(e5(), tableau=tableau)
+    R = oracle.Restatement(e5(), tableau_kind=tableau)
+    inp_ref, inp = e5_inputs(), e5_inputs()
+    for dt in e5_intervals():
+        y_micm, st_micm = ref.solve_global(inp_ref, dt)
+        assert st_micm[0]["state"] == 2 and st_micm[0]["final_time"] == dt
+        y, st = R.solve_per_cell(inp, dt, threads=1)
+        assert st[0, 3] == st_micm[0]["accepted"]
+        np.testing.assert_allclose(y, y_micm, rtol=1e-6, atol=1e-30)
+        inp_ref, inp = dict(inp_ref, concentrations=y_micm), dict(inp, concentrations=y)
