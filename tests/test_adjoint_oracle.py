@@ -70,3 +70,52 @@ def test_adjoint_matches_finite_differences(case, species):
         if sig.any():
             worst = max(worst, (np.abs(fd - gk[:, r]) / np.abs(gk[:, r]))[sig].max())
     assert worst < 1e-5
+
+
+def test_adjoint_on_micms_ts1_mechanism_matches_finite_differences():
+    """The same check on micm's TS1 benchmark mechanism (Troe, photolysis,
+    surface reactions, a third body), two varied cells, gradients of the final
+    O3 (absolute tolerance 1e-9, 3-stage Rosenbrock, dt = 30 s)."""
+    from micm_b200 import ts1
+    mech = ts1.mechanism(absolute_tolerance=1e-9)
+    inputs = ts1.inputs(2, seed=5)
+    R = oracle.Restatement(mech, tableau_kind=ts1.TABLEAU)
+    k = R._k(inputs)
+    h, steps = R.step_sizes_per_cell(inputs, ts1.DT, 1024, k)
+    y_final, _ = R.solve_per_cell(inputs, ts1.DT, k=k)
+    np.testing.assert_array_equal(R.replay_per_cell(inputs["concentrations"], k, h, steps), y_final)
+    o3 = mech.species.index("O3")
+    ybar = np.zeros_like(y_final)
+    ybar[:, o3] = 1.0
+    _, g0, gk = R.adjoint_per_cell(inputs, ts1.DT, ybar, k=k, max_steps=1024)
+
+    def out(y, kk=k):
+        return R.replay_per_cell(y, kk, h, steps)[:, o3]
+
+    rel_h, worst, checked = 1e-6, 0.0, 0
+    y0 = inputs["concentrations"]
+    imp = np.abs(g0) * np.abs(y0)
+    for j in range(mech.n_species):
+        e = rel_h * np.abs(y0[:, j])
+        sig = imp[:, j] > 1e-3 * imp.max(axis=1)
+        if not sig.any() or np.any(e[sig] == 0):
+            continue
+        yp, ym = y0.copy(), y0.copy()
+        yp[:, j] += e
+        ym[:, j] -= e
+        fd = (out(yp) - out(ym)) / (2 * np.where(e > 0, e, 1.0))
+        worst = max(worst, (np.abs(fd - g0[:, j]) / np.abs(g0[:, j]))[sig].max())
+        checked += 1
+    kimp = np.abs(gk)
+    for r in range(mech.n_reactions):
+        sig = kimp[:, r] > 1e-3 * kimp.max(axis=1)
+        if not sig.any():
+            continue
+        c = R.reaction_columns[r]
+        kp, km = k.copy(), k.copy()
+        kp[:, c] *= np.exp(rel_h)
+        km[:, c] *= np.exp(-rel_h)
+        fd = (out(y0, kp) - out(y0, km)) / (2 * rel_h)
+        worst = max(worst, (np.abs(fd - gk[:, r]) / np.abs(gk[:, r]))[sig].max())
+        checked += 1
+    assert checked > 10 and worst < 1e-5
