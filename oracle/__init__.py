@@ -69,6 +69,9 @@ def _load_ref():
                                           _f64p, _f64p, _i64p]
         lib.mref_solve_per_cell.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, _f64p, _f64p, _f64p,
                                             _f64p, _f64p, _i64p, C.c_int]
+        if hasattr(lib, "mref_backward_euler_per_cell"):
+            lib.mref_backward_euler_per_cell.argtypes = [C.c_void_p, C.c_int, C.c_double, _f64p, _f64p, _f64p,
+                                                         _f64p, _f64p, _i64p]
         if hasattr(lib, "mref_solve_groups_v128"):
             lib.mref_solve_groups_v128.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, _f64p, _f64p,
                                                    _f64p, _f64p, _f64p, _i64p, C.c_int]
@@ -207,6 +210,21 @@ class Reference:
             int(threads)))
         return self.y_from_columns(y), stats
 
+    def backward_euler_per_cell(self, inputs: Dict[str, np.ndarray], dt: float):
+        """micm's Backward Euler, a 1-cell State per cell, one Solve(dt) each:
+        (y_final [n,S] system order, stats rows per cell)."""
+        if not hasattr(self.lib, "mref_backward_euler_per_cell"):
+            raise RuntimeError("oracle/_ref/libmicm_ref.so predates mref_backward_euler_per_cell; rebuild it")
+        y = self.y_to_columns(inputs["concentrations"])
+        n = len(y)
+        stats = np.zeros((n, 10), np.int64)
+        params = np.ascontiguousarray(inputs["custom_params"] if inputs["custom_params"].size
+                                      else np.zeros((n, 1)))
+        self._check(self.lib.mref_backward_euler_per_cell(
+            self.handle, n, float(dt), _p(inputs["temperature"]), _p(inputs["pressure"]),
+            _p(inputs["air_density"]), _p(params), _p(y), _p(stats, C.c_int64)))
+        return self.y_from_columns(y), stats
+
     def solve_per_cell(self, inputs: Dict[str, np.ndarray], dt: float, n_solves: int = 1,
                        threads: int = 0):
         """A 1-cell State per cell; returns (y_final [n,S] system order, stats rows per cell)."""
@@ -244,6 +262,8 @@ def _load_oracle():
         lib.om_adjoint_per_cell.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, _f64p, _f64p,
                                             C.c_double, _f64p, _f64p, _f64p, _f64p, _f64p, C.c_int, C.c_int]
         lib.om_replay_per_cell.argtypes = [C.c_void_p, C.c_void_p, C.c_int, _f64p, _f64p, _i32p, C.c_int, _f64p]
+        lib.om_backward_euler_per_cell.argtypes = [C.c_void_p, C.c_int, C.c_double, _f64p, _f64p, C.c_double,
+                                                   _f64p, _i64p]
         lib.om_step_sizes_per_cell.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, _f64p, _f64p,
                                                C.c_double, _f64p, C.c_int, _f64p, _i32p]
         _om = lib
@@ -314,6 +334,21 @@ class Restatement:
         rc = self.lib.om_solve_per_cell(self.handle, C.byref(self.params), n, float(dt), _p(k),
                                         _p(self.atol_columns), self.mech.relative_tolerance, _p(y),
                                         _p(stats, C.c_int64), int(threads or os.cpu_count() or 1))
+        if rc:
+            raise RuntimeError(self.lib.om_last_error().decode())
+        return np.ascontiguousarray(y[:, self.species_columns]), stats
+
+    def backward_euler_per_cell(self, inputs, dt, k=None):
+        """Backward Euler (micm's algorithm and default parameters), a 1-cell
+        solve per cell: (y_final [n,S] system order, stats [n,10])."""
+        y = np.zeros_like(inputs["concentrations"])
+        y[:, self.species_columns] = inputs["concentrations"]
+        y = np.ascontiguousarray(y)
+        n = len(y)
+        k = self._k(inputs) if k is None else np.ascontiguousarray(k)
+        stats = np.zeros((n, 10), np.int64)
+        rc = self.lib.om_backward_euler_per_cell(self.handle, n, float(dt), _p(k), _p(self.atol_columns),
+                                                 self.mech.relative_tolerance, _p(y), _p(stats, C.c_int64))
         if rc:
             raise RuntimeError(self.lib.om_last_error().decode())
         return np.ascontiguousarray(y[:, self.species_columns]), stats

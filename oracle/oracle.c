@@ -1021,6 +1021,129 @@ int om_solve_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n,
   return run(&j, n_threads);
 }
 
+/* ---------------------------------------------------------------- */
+/* Backward Euler on one cell (backward_euler.inl:12-193: Newton     */
+/* iterations on forcing, -J + I/H, the in-place LU and a solve,     */
+/* clamped at zero; IsConverged :195-246; default parameters of      */
+/* backward_euler_solver_parameters.hpp: small 1e-40, 11 iterations, */
+/* step reductions 0.5, 0.5, 0.5, 0.5, 0.1)                          */
+/* ---------------------------------------------------------------- */
+#define OM_SOLVER_ACCEPTING_UNCONVERGED 8 /* micm's SolverState::AcceptingUnconvergedIntegration */
+
+static int backward_euler_cell(const om_mech* m, double dt, const double* k, const double* atol, double rtol,
+                               double* Yn1, double* Yn, double* f, double* J, int64_t* stats)
+{
+  const int S = m->S;
+  const double small = 1.0e-40;
+  const int max_iter = 11;
+  const double reductions[5] = { 0.5, 0.5, 0.5, 0.5, 0.1 };
+  int64_t st[7] = { 0 }; /* function_calls, jacobian_updates, number_of_steps, accepted, rejected,
+                            decompositions, solves */
+  double H = dt, t = 0.0;
+  int n_ok = 0, n_fail = 0, state = MICMB_SOLVER_NOT_YET_CALLED;
+  memcpy(Yn, Yn1, sizeof(double) * S);
+  while (t < dt)
+  {
+    state = MICMB_SOLVER_RUNNING;
+    int converged = 0, iterations = 0;
+    do
+    {
+      st[2]++;
+      forcing(m, k, Yn1, f);
+      st[0]++;
+      neg_jacobian(m, k, Yn1, J);
+      st[1]++;
+      for (int i = 0; i < S; ++i)
+        J[m->pos[(size_t)i * S + i]] += 1 / H;
+      decompose(m, J);
+      st[5]++;
+      for (int i = 0; i < S; ++i)
+        f[i] -= (Yn1[i] - Yn[i]) / H;
+      lu_solve(m, J, f);
+      st[6]++;
+      for (int i = 0; i < S; ++i)
+      {
+        const double v = Yn1[i] + f[i];
+        Yn1[i] = (0.0 > v) ? 0.0 : v;
+      }
+      if (iterations++ == 0)
+        continue;
+      converged = 1;
+      for (int i = 0; i < S; ++i)
+      {
+        const double r = f[i];
+        if (!isfinite(r))
+          converged = 0;
+        else if (fabs(r) > small && fabs(r) > atol[i] && fabs(r) > rtol * fabs(Yn1[i]))
+          converged = 0;
+      }
+    } while (!converged && iterations < max_iter);
+    if (!converged)
+    {
+      st[4]++;
+      n_ok = 0;
+      if (n_fail >= 5)
+      {
+        t += H;
+        state = OM_SOLVER_ACCEPTING_UNCONVERGED;
+        int any_nan = 0, any_inf = 0;
+        for (int i = 0; i < S; ++i)
+        {
+          any_nan = any_nan || isnan(Yn1[i]);
+          any_inf = any_inf || isinf(Yn1[i]);
+        }
+        if (any_nan)
+          state = MICMB_SOLVER_NAN_DETECTED;
+        else if (any_inf)
+          state = MICMB_SOLVER_INF_DETECTED;
+        break;
+      }
+      memcpy(Yn1, Yn, sizeof(double) * S);
+      H *= reductions[n_fail++];
+    }
+    else
+    {
+      st[3]++;
+      state = MICMB_SOLVER_CONVERGED;
+      t += H;
+      memcpy(Yn, Yn1, sizeof(double) * S);
+      if (++n_ok >= 2)
+      {
+        n_ok = 0;
+        H *= 2.0;
+      }
+    }
+    H = dmin(H, dt - t);
+  }
+  if (stats)
+  {
+    for (int q = 0; q < 7; ++q)
+      stats[q] = st[q];
+    stats[7] = state;
+    memcpy(&stats[8], &t, sizeof(double));
+    stats[9] = 0;
+  }
+  return state;
+}
+
+/* Backward Euler per cell (a 1-cell State per cell), one Solve(dt) each.
+ * y [cell][column] in/out; stats_out [cell][10] as om_solve_per_cell's. */
+int om_backward_euler_per_cell(const om_mech* m, int n, double dt, const double* k, const double* atol, double rtol,
+                               double* y, int64_t* stats_out)
+{
+  const int S = m->S;
+  double* Yn = xcalloc(S, sizeof(double));
+  double* f = xcalloc(S, sizeof(double));
+  double* J = xcalloc(m->nnz, sizeof(double));
+  for (int c = 0; c < n; ++c)
+    backward_euler_cell(m, dt, k + (size_t)c * m->R, atol, rtol, y + (size_t)c * S, Yn, f, J,
+                        stats_out ? stats_out + (size_t)c * 10 : NULL);
+  free(Yn);
+  free(f);
+  free(J);
+  return 0;
+}
+
 /* One Rosenbrock step of size H from Y (no error estimate), Y <- Y + sum m_s K_s;
  * the stage recurrences of adjoint_cell's recomputation. */
 static void fixed_step(const om_mech* m, const micmb_rosenbrock_params* p, const double* k, double H, double* Y,

@@ -62,6 +62,10 @@ int om_adjoint_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int 
 int om_replay_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n, const double* k, const double* h,
                        const int32_t* n_steps, int max_steps, double* y);
 /* Accepted step sizes of a per-cell solve from y0 [cell][S]. */
+/* Backward Euler (micm's backward_euler.inl, default parameters), a 1-cell
+ * State per cell, one Solve(dt) each; y [cell][column] in/out, stats [cell][10]. */
+int om_backward_euler_per_cell(const om_mech* m, int n, double dt, const double* k, const double* atol, double rtol,
+                               double* y, int64_t* stats_out);
 int om_step_sizes_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n, double dt, const double* k,
                            const double* atol, double rtol, const double* y0, int max_steps, double* h,
                            int32_t* n_steps);

@@ -45,6 +45,13 @@ namespace
       micm::LuDecompositionMozartInPlace<SparseL<L>>>;
   template<std::size_t L>
   using SolverL = decltype(std::declval<BuilderL<L>>().Build());
+  // micm's Backward Euler on the same matrices and in-place Mozart LU
+  using BuilderBE = micm::CpuSolverBuilderInPlace<
+      micm::BackwardEulerSolverParameters,
+      DenseL<1>,
+      SparseL<1>,
+      micm::LuDecompositionMozartInPlace<SparseL<1>>>;
+  using SolverBE = decltype(std::declval<BuilderBE>().Build());
 
   thread_local std::string g_error;
 
@@ -603,6 +610,37 @@ extern "C"
       t.join();
     if (!failure.empty())
       throw std::runtime_error(failure);
+    return 0;
+    GUARD_END
+  }
+
+  // micm's Backward Euler (backward_euler.inl, default parameters), a 1-cell
+  // State per cell, one Solve(dt) each.  y_inout [cell][column]; stats_out
+  // [cell][10] as mref_solve_per_cell's.
+  int mref_backward_euler_per_cell(void* p, int n, double dt, const double* T, const double* P, const double* rho,
+                                   const double* params, double* y_inout, int64_t* stats_out)
+  {
+    GUARD_BEGIN
+    auto* h = static_cast<Handle*>(p);
+    const int S = h->built.n_species;
+    auto solver = BuilderBE(micm::BackwardEulerSolverParameters{})
+                      .SetSystem(h->built.system)
+                      .SetReactions(h->built.processes)
+                      .SetReorderState(h->reorder)
+                      .SetIgnoreUnusedSpecies(true)
+                      .Build();
+    auto state = solver.GetState(1);
+    state.SetRelativeTolerance(h->rtol);
+    for (int c = 0; c < n; ++c)
+    {
+      LoadCell(state, 0, h->n_params, S, T, P, rho, params, y_inout, c);
+      solver.UpdateStateParameters(state);
+      auto r = solver.Solve(dt, state);
+      for (int j = 0; j < S; ++j)
+        y_inout[(size_t)c * S + j] = state.variables_[0][j];
+      if (stats_out)
+        StatsOut(r, stats_out + 10 * (size_t)c);
+    }
     return 0;
     GUARD_END
   }
