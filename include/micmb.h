@@ -348,15 +348,39 @@ int micmb_normalized_error(micmb_solver* solver, micmb_state* state, double* glo
                            double* per_cell_out);
 
 /* The global value of micmb_normalized_error, computed without allocating
- * (no counterpart in micm).  Scratch is a fixed file-scope device array for at
- * most 65536 cells; larger states return MICMB_ERR_INVALID_ARGUMENT.  The
- * buffers read (variables, MICMB_BUF_SCRATCH_Y, MICMB_BUF_FORCING, absolute
- * tolerances) must already exist: upload them first.  Nothing in the scratch
- * needs to start at zero.  The first call on a device looks up the scratch
- * address (cudaGetSymbolAddress); make it before any stream capture.  There is
- * one scratch area per device: overlapping calls on the same device race on
- * it, so serialise them. */
+ * (no counterpart in micm).  For callers that cannot call cudaMalloc while they
+ * run: a host model that has handed the device's memory to its own pool
+ * allocator up front, or one whose error-control loop runs where a device
+ * allocation would stall or fail (an allocation synchronises the device and
+ * can fail once the device is full).  Scratch is a fixed file-scope device
+ * array for at most 65536 cells (512 KB, held on every device that loads the
+ * library until the process exits); larger states return
+ * MICMB_ERR_INVALID_ARGUMENT.  The buffers read (variables,
+ * MICMB_BUF_SCRATCH_Y, MICMB_BUF_FORCING, absolute tolerances) must already
+ * exist: upload them first.  Nothing in the scratch needs to start at zero:
+ * every slot a call reads, the same call wrote first.  The first call on a
+ * device looks up the scratch address (cudaGetSymbolAddress) and keeps it;
+ * make that first call before any stream capture, and make no call after a
+ * cudaDeviceReset in the same process (the kept address is then stale).
+ * There is one scratch area per device: calls that overlap on the same device
+ * (different streams or host threads) race on it, so serialise them. */
 int micmb_normalized_error_noalloc(micmb_solver* solver, micmb_state* state, double* global_out);
+
+/* ---- math check ---- */
+#define MICMB_MATH_EXP 0
+#define MICMB_MATH_LOG10 1
+#define MICMB_MATH_POW 2
+/* The correctly rounded exp, log10 and pow every kernel uses in place of the C
+ * library calls micm makes (std::exp / std::pow / std::log10 in
+ * include/micm/process/rate_constant/rate_constant_functions.hpp:52-136, and
+ * the step-size factor std::pow(error, 1 / order) in
+ * include/micm/solver/rosenbrock.inl:232-235), evaluated element-wise:
+ * out[i] = f(x[i]) or pow(x[i], y[i]).  on_device = 0 runs the host build of
+ * the same code on host arrays; 1 runs it in a kernel on device arrays (the
+ * current device, default stream, synchronised).  A diagnostic: it lets a
+ * caller check the device results against the host's bit for bit. */
+int micmb_math_eval(int32_t function, const double* x, const double* y, double* out, int64_t n,
+                    int32_t on_device);
 
 #ifdef __cplusplus
 }

@@ -68,6 +68,7 @@ def lib():
             "micmb_linear_solve": [vp, vp],
             "micmb_normalized_error": [vp, vp, f64p, f64p],
             "micmb_normalized_error_noalloc": [vp, vp, f64p],
+            "micmb_math_eval": [C.c_int32, vp, vp, vp, C.c_int64, C.c_int32],
         }
         for name, args in sig.items():
             fn = getattr(L, name)

@@ -288,32 +288,7 @@ namespace micmb
     template<class F>
     int Guard(F&& f)
     {
-      try
-      {
-        f();
-        g_last_error.clear();
-        return MICMB_OK;
-      }
-      catch (const Error& e)
-      {
-        g_last_error = e.what();
-        return e.code;
-      }
-      catch (const std::bad_alloc&)
-      {
-        g_last_error = "host allocation failed";
-        return MICMB_ERR_OUT_OF_MEMORY;
-      }
-      catch (const std::exception& e)
-      {
-        g_last_error = e.what();
-        return MICMB_ERR_INVALID_ARGUMENT;
-      }
-      catch (...)
-      {
-        g_last_error = "unknown error";
-        return MICMB_ERR_INTERNAL;
-      }
+      return GuardCall<MICMB_ERR_INVALID_ARGUMENT>(std::forward<F>(f));
     }
 
     void Need(bool ok, const char* what)

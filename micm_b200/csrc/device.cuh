@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/micmb.h"
+#include "crmath.cuh"
 
 namespace micmb
 {
@@ -123,14 +124,15 @@ namespace micmb
   }
 
   // ---------------------------------------------------------------------
-  // rate constants (rate_constant_functions.hpp:52-136)
+  // rate constants (rate_constant_functions.hpp:52-136), with the C library's
+  // correctly rounded exp, pow and log10 (crmath.cuh)
   // ---------------------------------------------------------------------
   __device__ __forceinline__ double falloff(const double* p, double T, double rho, double numerator_scale)
   {
-    const double k0 = p[0] * exp(p[2] / T) * pow(T / 300.0, p[1]);
-    const double kinf = p[3] * exp(p[5] / T) * pow(T / 300.0, p[4]);
+    const double k0 = p[0] * cr_exp(p[2] / T) * cr_pow(T / 300.0, p[1]);
+    const double kinf = p[3] * cr_exp(p[5] / T) * cr_pow(T / 300.0, p[4]);
     const double ratio = k0 * rho / kinf;
-    return k0 * numerator_scale / (1.0 + ratio) * pow(p[6], p[7] / (p[7] + pow(log10(ratio), 2.0)));
+    return k0 * numerator_scale / (1.0 + ratio) * cr_pow(p[6], p[7] / (p[7] + cr_pow(cr_log10(ratio), 2.0)));
   }
 
   // k for rate column r given the cell's conditions and custom-parameter column reader
@@ -142,29 +144,29 @@ namespace micmb
     double k;
     switch (M.rate_kind[r])
     {
-      case MICMB_RATE_ARRHENIUS: k = p[0] * exp(p[2] / T) * pow(T / p[3], p[1]) * (1.0 + p[4] * Pr); break;
+      case MICMB_RATE_ARRHENIUS: k = p[0] * cr_exp(p[2] / T) * cr_pow(T / p[3], p[1]) * (1.0 + p[4] * Pr); break;
       case MICMB_RATE_TROE: k = falloff(p, T, rho, rho); break;
       case MICMB_RATE_TERNARY_CHEMICAL_ACTIVATION: k = falloff(p, T, rho, 1.0); break;
       case MICMB_RATE_BRANCHED:
       {
         const double a = p[5] * rho;
-        const double b = 0.43 * pow(T / 298.0, -8.0);
-        const double A_val = a / (1.0 + a / b) * pow(0.41, 1.0 / (1.0 + pow(log10(a / b), 2.0)));
-        const double pre = p[1] * exp(-p[2] / T);
+        const double b = 0.43 * cr_pow(T / 298.0, -8.0);
+        const double A_val = a / (1.0 + a / b) * cr_pow(0.41, 1.0 / (1.0 + cr_pow(cr_log10(a / b), 2.0)));
+        const double pre = p[1] * cr_exp(-p[2] / T);
         k = (p[0] == 0.0) ? pre * (p[6] / (p[6] + A_val)) : pre * (A_val / (A_val + p[6]));
         break;
       }
-      case MICMB_RATE_TUNNELING: k = p[0] * exp(-p[1] / T + p[2] / (T * T * T)); break;
+      case MICMB_RATE_TUNNELING: k = p[0] * cr_exp(-p[1] / T + p[2] / (T * T * T)); break;
       case MICMB_RATE_TAYLOR_SERIES:
       {
         double poly = 0.0, t_pow = 1.0;
         const int32_t n = (int32_t)p[5];
         for (int32_t j = 0; j < n; ++j, t_pow *= T)
           poly += p[6 + j] * t_pow;
-        k = poly * p[0] * exp(p[2] / T) * pow(T / p[3], p[1]) * (1.0 + p[4] * Pr);
+        k = poly * p[0] * cr_exp(p[2] / T) * cr_pow(T / p[3], p[1]) * (1.0 + p[4] * Pr);
         break;
       }
-      case MICMB_RATE_REVERSIBLE: k = p[0] * exp(p[1] / T) * p[2]; break;
+      case MICMB_RATE_REVERSIBLE: k = p[0] * cr_exp(p[1] / T) * p[2]; break;
       case MICMB_RATE_USER_DEFINED: k = param(M.rate_param_col[r]) * p[0]; break;
       case MICMB_RATE_SURFACE:
       {
@@ -514,10 +516,12 @@ namespace micmb
   }
 
   // ---------------------------------------------------------------------
-  // normalized error (rosenbrock.inl:353-402), lane-striped partial sums
-  // combined in butterfly order; the one-lane version reproduces the order.
+  // normalized error (rosenbrock.inl:353-402).  micm adds the scaled squares
+  // of one cell in species order with one accumulator (ReduceStrict,
+  // vector_matrix.hpp:858-866); every per-cell sum here is formed in that
+  // order, so a cell's error equals micm's bit for bit.
   // ---------------------------------------------------------------------
-  __device__ __forceinline__ double scaled_sq(double y, double ynew, double err, double atol, double rtol)
+  __host__ __device__ __forceinline__ double scaled_sq(double y, double ynew, double err, double atol, double rtol)
   {
     const double ay = fabs(y), an = fabs(ynew);
     const double ymax = ay > an ? ay : an;
@@ -525,72 +529,21 @@ namespace micmb
     return q * q;
   }
 
-  // Partial sum of lane `lane` of a 32-lane stripe over S species.
-  template<class YV, class NV, class EV>
-  __device__ __forceinline__ double error_partial(int32_t S, YV y, NV ynew, EV err, const double* atol, double rtol,
-                                                  int lane)
+  // Sequential sum of the 32-lane stripe values q (lane l holds the term of
+  // species base + l) added to acc in species order; every lane returns the
+  // same total.  `count` is the number of valid lanes of this stripe.
+  __device__ __forceinline__ double warp_seq_add(double acc, double q, int32_t count)
   {
-    double acc = 0.0;
-    for (int32_t s = lane; s < S; s += 32)
-      acc += scaled_sq(y[s], ynew[s], err[s], atol[s], rtol);
+    for (int l = 0; l < count; ++l)
+      acc += __shfl_sync(0xffffffffu, q, l);
     return acc;
   }
 
-  // warp butterfly sum (all lanes get the total)
-  __device__ __forceinline__ double warp_sum(double v)
+  // The scaled error (max(sqrt(sum / n), 1e-10)) from a sum of squares.
+  __host__ __device__ __forceinline__ double error_from_sum(double sum, double n)
   {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1)
-      v += __shfl_xor_sync(0xffffffffu, v, off);
-    return v;
-  }
-
-  // the same sum computed by one thread: partial[l] for l in 0..31, butterfly order
-  __device__ __forceinline__ double butterfly_sum_serial(double* part)
-  {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1)
-    {
-      double nxt[32];
-#pragma unroll
-      for (int l = 0; l < 32; ++l)
-        nxt[l] = part[l] + part[l ^ off];
-#pragma unroll
-      for (int l = 0; l < 32; ++l)
-        part[l] = nxt[l];
-    }
-    return part[0];
-  }
-
-  // 5-bit bit reversal (compile-time when t is)
-  __host__ __device__ constexpr int bitrev5(int t)
-  {
-    return ((t & 1) << 4) | ((t & 2) << 2) | (t & 4) | ((t & 8) >> 2) | ((t & 16) >> 4);
-  }
-
-  // The sum butterfly_sum_serial forms from part[l] = sum of term(i) over
-  // i = l, l + 32, ... < n (increasing i), without the 32 partial sums: the
-  // stripes are visited in the tree's leaf order (bit-reversed l), and a
-  // five-level stack joins them pairwise as a binary counter does, so every
-  // addition has the same operands as in the butterfly (x + y == y + x).
-  template<class F>
-  __device__ __forceinline__ double stripe_tree_sum(int32_t n, F term)
-  {
-    double stack[5];
-    double v = 0.0;
-#pragma unroll 1
-    for (int t = 0; t < 32; ++t)
-    {
-      v = 0.0;
-      for (int32_t i = bitrev5(t); i < n; i += 32)
-        v += term(i);
-      int level = 0;
-      for (; level < 5 && ((t >> level) & 1); ++level)
-        v = stack[level] + v;
-      if (level < 5)
-        stack[level] = v;
-    }
-    return v;
+    const double rms = sqrt(sum / n);
+    return (rms < 1.0e-10) ? 1.0e-10 : rms;
   }
 
   // ---------------------------------------------------------------------
@@ -665,8 +618,9 @@ namespace micmb
   // Accept/reject after the error norm. Returns 1 accepted, 0 rejected, -1 stopped (NaN/Inf).
   __host__ __device__ inline int ctl_after_error(CellCtl& c, const DevParams& p, const StepBounds& b, double error)
   {
-    // std::min(factor_max, std::max(factor_min, safety / pow(error, 1/order)))
-    const double x = p.safety_factor / pow(error, p.inv_order);
+    // std::min(factor_max, std::max(factor_min, safety / pow(error, 1/order))),
+    // with micm's (the C library's) correctly rounded pow
+    const double x = p.safety_factor / cr_pow(error, p.inv_order);
     const double lo = (p.factor_min < x) ? x : p.factor_min;
     const double fac = (lo < p.factor_max) ? lo : p.factor_max;
     double Hnew = c.H * fac;

@@ -16,22 +16,7 @@ namespace micmb
     template<class F>
     int GuardX(F&& f)
     {
-      try
-      {
-        f();
-        g_last_error.clear();
-        return MICMB_OK;
-      }
-      catch (const Error& e)
-      {
-        g_last_error = e.what();
-        return e.code;
-      }
-      catch (const std::exception& e)
-      {
-        g_last_error = e.what();
-        return MICMB_ERR_INTERNAL;
-      }
+      return GuardCall(std::forward<F>(f));
     }
 
     void NeedX(bool ok, const char* what)

@@ -174,23 +174,29 @@ namespace micmb
               warp_solve(M.w_fwd, LU, Ks, lane);
               warp_solve(M.w_bwd, LU, Ks, lane);
             }
-            double part = 0.0;
-            for (int32_t i = lane; i < S; i += kWarp)
+            // error norm in species order (micm's order): stripe by stripe, the
+            // lanes' terms added in lane order
+            double sum = 0.0;
+            for (int32_t base = 0; base < S; base += kWarp)
             {
-              double v = Y[i];
-              double e = 0.0;
-              for (int32_t st = 0; st < P.stages; ++st)
+              const int32_t i = base + lane;
+              double q = 0.0;
+              if (i < S)
               {
-                const double kv = K[(size_t)st * VS + i];
-                v += P.m[st] * kv;
-                e += P.e[st] * kv;
+                double v = Y[i];
+                double e = 0.0;
+                for (int32_t st = 0; st < P.stages; ++st)
+                {
+                  const double kv = K[(size_t)st * VS + i];
+                  v += P.m[st] * kv;
+                  e += P.e[st] * kv;
+                }
+                Yn[i] = v;
+                q = scaled_sq(Y[i], v, e, A.atol[i], A.rtol);
               }
-              Yn[i] = v;
-              part += scaled_sq(Y[i], v, e, A.atol[i], A.rtol);
+              sum = warp_seq_add(sum, q, (S - base < kWarp) ? S - base : kWarp);
             }
-            const double sum = warp_sum(part);
-            const double rms = sqrt(sum / (double)S);
-            const double error = (rms < 1.0e-10) ? 1.0e-10 : rms;
+            const double error = error_from_sum(sum, (double)S);
             count_attempt(c, P);
             const double h_used = c.H;
             const int res = ctl_after_error(c, P, B, error);

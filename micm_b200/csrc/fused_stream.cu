@@ -411,23 +411,29 @@ namespace micmb
         }
         if (act && !*abort_flag)
         {
-          double part = 0.0;
-          for (int32_t i = lane; i < S; i += kWarp)
+          // error norm in species order (micm's order): stripe by stripe, the
+          // lanes' terms added in lane order
+          double sum = 0.0;
+          for (int32_t base = 0; base < S; base += kWarp)
           {
-            double v = Y[i];
-            double e = 0.0;
-            for (int32_t st = 0; st < P.stages; ++st)
+            const int32_t i = base + lane;
+            double q = 0.0;
+            if (i < S)
             {
-              const double kv = K[(size_t)st * VS + i];
-              v += P.m[st] * kv;
-              e += P.e[st] * kv;
+              double v = Y[i];
+              double e = 0.0;
+              for (int32_t st = 0; st < P.stages; ++st)
+              {
+                const double kv = K[(size_t)st * VS + i];
+                v += P.m[st] * kv;
+                e += P.e[st] * kv;
+              }
+              Yn[i] = v;
+              q = scaled_sq(Y[i], v, e, A.atol[i], A.rtol);
             }
-            Yn[i] = v;
-            part += scaled_sq(Y[i], v, e, A.atol[i], A.rtol);
+            sum = warp_seq_add(sum, q, (S - base < kWarp) ? S - base : kWarp);
           }
-          const double sum = warp_sum(part);
-          const double rms = sqrt(sum / (double)S);
-          const double error = (rms < 1.0e-10) ? 1.0e-10 : rms;
+          const double error = error_from_sum(sum, (double)S);
           count_attempt(wc.c, P);
           const double h_used = wc.c.H;
           const int res = ctl_after_error(wc.c, P, B, error);

@@ -198,8 +198,10 @@ namespace micmb
           solve_lower<1>(M.fwd_s, LU, Ks, 0);
           solve_upper<1>(M.bwd_s, LU, Ks, 0);
         }
-        // Ynew, and the error norm summed in the 32-lane-stripe order of the warp kernels
-        const double sum = stripe_tree_sum(S, [&](int32_t i) {
+        // Ynew, and the error norm summed in species order (micm's order)
+        double sum = 0.0;
+        for (int32_t i = 0; i < S; ++i)
+        {
           double v = Y[i];
           double e = 0.0;
           for (int32_t st = 0; st < P.stages; ++st)
@@ -209,10 +211,9 @@ namespace micmb
             e += P.e[st] * kv;
           }
           Yn[i] = v;
-          return scaled_sq(Y[i], v, e, A.atol[i], A.rtol);
-        });
-        const double rms = sqrt(sum / (double)S);
-        const double error = (rms < 1.0e-10) ? 1.0e-10 : rms;
+          sum += scaled_sq(Y[i], v, e, A.atol[i], A.rtol);
+        }
+        const double error = error_from_sum(sum, (double)S);
         count_attempt(c, P);
         const double h_used = c.H;
         const int res = ctl_after_error(c, P, B, error);

@@ -7,7 +7,10 @@
 // it.  Nothing in the scratch has to start at zero: every slot a call reads is
 // written earlier in the same call.  There is one scratch area per device, so
 // two calls that overlap in time on the same device (different streams or
-// host threads) race on it; callers serialise them.
+// host threads) race on it; callers serialise them.  The cached address
+// belongs to the device's primary context: after cudaDeviceReset (or any
+// reset of that context) the array is gone and the cached address is stale,
+// so the entry point must not be called in a process after such a reset.
 #include "runtime.hpp"
 
 #include <cmath>
@@ -46,8 +49,8 @@ namespace micmb
       return (size_t)(c / L) * (size_t)L * (size_t)ncol + (size_t)(c % L);
     }
 
-    // per-cell sum of squared scaled errors, in the same 32-stripe order as the
-    // per-cell error of micmb_normalized_error
+    // per-cell sum of squared scaled errors in species order, as the per-cell
+    // error of micmb_normalized_error forms it
     __global__ void k_error_cells_fixed(int32_t S, const double* y, const double* ynew, const double* err,
                                         const double* atol, double rtol, int64_t n, int32_t L, double* cells)
     {
@@ -55,14 +58,10 @@ namespace micmb
       if (c >= n)
         return;
       const size_t bs = cell_base(c, L, S);
-      double part[32];
-#pragma unroll
-      for (int l = 0; l < 32; ++l)
-        part[l] = 0.0;
+      double sum = 0.0;
       for (int32_t i = 0; i < S; ++i)
-        part[i & 31] += scaled_sq(y[bs + (size_t)i * L], ynew[bs + (size_t)i * L], err[bs + (size_t)i * L], atol[i],
-                                  rtol);
-      cells[c] = butterfly_sum_serial(part);
+        sum += scaled_sq(y[bs + (size_t)i * L], ynew[bs + (size_t)i * L], err[bs + (size_t)i * L], atol[i], rtol);
+      cells[c] = sum;
     }
 
     // total over cells in cell order (the order micmb_normalized_error adds them in)
@@ -80,8 +79,7 @@ using namespace micmb;
 
 extern "C" int micmb_normalized_error_noalloc(micmb_solver* solver, micmb_state* state, double* global_out)
 {
-  try
-  {
+  return GuardCall([&] {
     if (!solver || !state || state->solver != solver || !global_out)
       throw Error(MICMB_ERR_INVALID_ARGUMENT, "state does not belong to this solver, or no output");
     micmb_state& st = *state;
@@ -106,14 +104,6 @@ extern "C" int micmb_normalized_error_noalloc(micmb_solver* solver, micmb_state*
     double sum = 0.0;
     MICMB_CUDA(cudaMemcpyAsync(&sum, scratch + kNoAllocMaxCells, sizeof(double), cudaMemcpyDeviceToHost, st.stream));
     MICMB_CUDA(cudaStreamSynchronize(st.stream));
-    const double rms = std::sqrt(sum / (double)(n * S > 0 ? n * S : 1));
-    *global_out = rms < 1.0e-10 ? 1.0e-10 : rms;
-    g_last_error.clear();
-    return MICMB_OK;
-  }
-  catch (const Error& e)
-  {
-    g_last_error = e.what();
-    return e.code;
-  }
+    *global_out = error_from_sum(sum, (double)(n * S > 0 ? n * S : 1));
+  });
 }

@@ -205,8 +205,8 @@ namespace micmb
       solve_upper<1>(M.bwd_s, J, Ks, 0);
     }
 
-    // Ynew = Y + sum m_s K_s ; Yerr = sum e_s K_s ; per-cell error partial sums
-    // in the 32-lane-stripe order of the fused kernel.  Returns the cell's sum.
+    // Ynew = Y + sum m_s K_s ; Yerr = sum e_s K_s ; the cell's sum of scaled
+    // squared errors in species order (micm's order).
     __device__ double finish_cell(const DevMech& M, const PlainArgs& a, const DevParams& P, int64_t c)
     {
       const int32_t L = a.L, S = M.S;
@@ -214,10 +214,7 @@ namespace micmb
       const size_t bk = cell_base(c, L, P.stages * S);
       Strided y{ a.y + bs, L };
       Strided yn{ a.ynew + bs, L };
-      double part[32];
-#pragma unroll
-      for (int l = 0; l < 32; ++l)
-        part[l] = 0.0;
+      double sum = 0.0;
       for (int32_t i = 0; i < S; ++i)
       {
         double v = y[i];
@@ -229,9 +226,9 @@ namespace micmb
           e += P.e[st] * kv;
         }
         yn[i] = v;
-        part[i & 31] += scaled_sq(y[i], v, e, a.atol[i], a.rtol);
+        sum += scaled_sq(y[i], v, e, a.atol[i], a.rtol);
       }
-      return butterfly_sum_serial(part);
+      return sum;
     }
 
     __device__ __forceinline__ void count_attempt(CellCtl& cc, const DevParams& P)
@@ -247,9 +244,7 @@ namespace micmb
       const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
       if (c >= a.n || !running(a, c))
         return;
-      const double sum = finish_cell(M, a, P, c);
-      const double rms = sqrt(sum / (double)M.S);
-      const double error = (rms < 1.0e-10) ? 1.0e-10 : rms;
+      const double error = error_from_sum(finish_cell(M, a, P, c), (double)M.S);
       CellCtl cc = a.ctl[c];
       count_attempt(cc, P);
       const int res = ctl_after_error(cc, P, b, error);
@@ -264,36 +259,52 @@ namespace micmb
       a.ctl[c] = cc;
     }
 
-    __global__ void k_finish_partial(DevMech M, PlainArgs a, DevParams P)
+    // Fixed-shape tree over the kBlock values of a block (thread 0 returns the total).
+    __device__ __forceinline__ double block_tree_sum(double v, double* red)
     {
-      const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-      if (c >= a.n || !running(a, c))
-        return;
-      a.err_cell[c] = finish_cell(M, a, P, c);
-    }
-
-    // global decision: deterministic reduction over cells, then micm's step control
-    __global__ void k_global_decide(PlainArgs a, DevParams P, StepBounds b, int32_t S, int32_t* last_accept)
-    {
-      __shared__ double red[1024];
-      if (a.status[0] != MICMB_SOLVER_RUNNING)
-        return;
-      double acc = 0.0;
-      for (int64_t c = threadIdx.x; c < a.n; c += blockDim.x)
-        acc += a.err_cell[c];
-      red[threadIdx.x] = acc;
+      red[threadIdx.x] = v;
       __syncthreads();
-      for (int w = blockDim.x / 2; w > 0; w >>= 1)
+      for (int w = kBlock / 2; w > 0; w >>= 1)
       {
         if ((int)threadIdx.x < w)
           red[threadIdx.x] += red[threadIdx.x + w];
         __syncthreads();
       }
+      return red[0];
+    }
+
+    // Global mode, first level: each cell's sum in species order, then one
+    // partial per block (fixed tree over its kBlock cells) in blk_err[block].
+    // A single cell's error therefore equals micm's bit for bit.
+    __global__ void k_finish_partial(DevMech M, PlainArgs a, DevParams P, double* blk_err)
+    {
+      __shared__ double red[kBlock];
+      const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+      if (a.status[0] != MICMB_SOLVER_RUNNING)
+        return;  // uniform over the grid in global mode
+      const double v = (c < a.n) ? finish_cell(M, a, P, c) : 0.0;
+      const double t = block_tree_sum(v, red);
+      if (threadIdx.x == 0)
+        blk_err[blockIdx.x] = t;
+    }
+
+    // Global decision: the block partials reduced in a fixed order by one
+    // block (each thread a strided sequential sum, then a fixed tree), then
+    // micm's step control.  Deterministic for a given cell count.
+    __global__ void k_global_decide(PlainArgs a, DevParams P, StepBounds b, int32_t S, const double* blk_err,
+                                    int64_t n_blk, int32_t* last_accept)
+    {
+      __shared__ double red[kBlock];
+      if (a.status[0] != MICMB_SOLVER_RUNNING)
+        return;
+      double acc = 0.0;
+      for (int64_t i = threadIdx.x; i < n_blk; i += kBlock)
+        acc += blk_err[i];
+      const double total = block_tree_sum(acc, red);
       if (threadIdx.x == 0)
       {
         const double N = (double)(a.n * (int64_t)S > 0 ? a.n * (int64_t)S : 1);
-        const double rms = sqrt(red[0] / N);
-        const double error = (rms < 1.0e-10) ? 1.0e-10 : rms;
+        const double error = error_from_sum(total, N);
         CellCtl cc = a.ctl[0];
         count_attempt(cc, P);
         const int res = ctl_after_error(cc, P, b, error);
@@ -482,8 +493,8 @@ namespace micmb
         }
         if (global)
         {
-          k_finish_partial<<<grid, kBlock, 0, stream>>>(s.dev, a, P);
-          k_global_decide<<<1, 1024, 0, stream>>>(a, P, b, m.S, last_accept);
+          k_finish_partial<<<grid, kBlock, 0, stream>>>(s.dev, a, P, a.err_cell);
+          k_global_decide<<<1, kBlock, 0, stream>>>(a, P, b, m.S, a.err_cell, (int64_t)grid, last_accept);
           k_global_apply<<<grid, kBlock, 0, stream>>>(s.dev, a, last_accept);
         }
         else
@@ -642,14 +653,11 @@ namespace micmb
         return;
       const int32_t L = a.L;
       const size_t bs = cell_base(c, L, M.S);
-      double part[32];
-#pragma unroll
-      for (int l = 0; l < 32; ++l)
-        part[l] = 0.0;
+      double sum = 0.0;
       for (int32_t i = 0; i < M.S; ++i)
-        part[i & 31] += scaled_sq(a.y[bs + (size_t)i * L], a.ynew[bs + (size_t)i * L], a.f0[bs + (size_t)i * L],
-                                  a.atol[i], a.rtol);
-      a.err_cell[c] = butterfly_sum_serial(part);
+        sum += scaled_sq(a.y[bs + (size_t)i * L], a.ynew[bs + (size_t)i * L], a.f0[bs + (size_t)i * L], a.atol[i],
+                         a.rtol);
+      a.err_cell[c] = sum;
     }
   }  // namespace
 

@@ -9,6 +9,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 struct micmb_mechanism
@@ -147,6 +148,40 @@ struct micmb_state
 namespace micmb
 {
   extern thread_local std::string g_last_error;  // micmb_last_error()
+
+  // Runs an entry point's body and turns every C++ exception into a status
+  // code and a micmb_last_error() message, so none crosses the C ABI
+  // (kStdCode: the status of a standard-library exception).
+  template<int kStdCode = MICMB_ERR_INTERNAL, class F>
+  int GuardCall(F&& f) noexcept
+  {
+    try
+    {
+      f();
+      g_last_error.clear();
+      return MICMB_OK;
+    }
+    catch (const Error& e)
+    {
+      g_last_error = e.what();
+      return e.code;
+    }
+    catch (const std::bad_alloc&)
+    {
+      g_last_error = "host allocation failed";
+      return MICMB_ERR_OUT_OF_MEMORY;
+    }
+    catch (const std::exception& e)
+    {
+      g_last_error = e.what();
+      return kStdCode;
+    }
+    catch (...)
+    {
+      g_last_error = "unknown error";
+      return MICMB_ERR_INTERNAL;
+    }
+  }
   void EnsurePlainBuffers(micmb_state& st);
   // plain path: one kernel per stage; returns after the whole solve
   void SolvePlain(micmb_solver& s, micmb_state& st, double dt, int32_t step_control, micmb_solver_stats* stats,
