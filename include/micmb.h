@@ -53,6 +53,7 @@ extern "C" {
 #define MICMB_SOLVER_REPEATEDLY_SINGULAR_MATRIX 5
 #define MICMB_SOLVER_NAN_DETECTED 6
 #define MICMB_SOLVER_INF_DETECTED 7
+#define MICMB_SOLVER_ACCEPTING_UNCONVERGED 8 /* Backward Euler: AcceptingUnconvergedIntegration */
 
 /* ------------------------------------------------------------------ */
 /* mechanism description                                               */
@@ -365,6 +366,33 @@ int micmb_normalized_error(micmb_solver* solver, micmb_state* state, double* glo
  * There is one scratch area per device: calls that overlap on the same device
  * (different streams or host threads) race on it, so serialise them. */
 int micmb_normalized_error_noalloc(micmb_solver* solver, micmb_state* state, double* global_out);
+
+/* ---- Backward Euler (micm's second integrator) ---- */
+/* micm::BackwardEulerSolverParameters
+ * (include/micm/solver/backward_euler_solver_parameters.hpp:17-29). */
+typedef struct micmb_backward_euler_params {
+  double small;                    /* residuals below this count as converged (1e-40) */
+  double h_start;                  /* first step size; 0 = the whole time step */
+  int32_t max_number_of_steps;     /* Newton iterations per attempt (11) */
+  int32_t n_time_step_reductions;  /* entries of time_step_reductions in use (5, at most 8) */
+  double time_step_reductions[8];  /* H factor after the k-th failed attempt ({0.5, 0.5, 0.5, 0.5, 0.1}) */
+} micmb_backward_euler_params;
+/* micm's defaults (the CAM-Chem set). */
+int micmb_backward_euler_params_default(micmb_backward_euler_params* out);
+/* Backward Euler Solve(time_step, state) over every cell, then the clamp at
+ * zero; replaces AbstractBackwardEuler::Solve
+ * (include/micm/solver/backward_euler.inl:10-186, IsConverged :188-246) and
+ * Solver::PostSolveClamp.  params may be NULL (micm's defaults).
+ * step_control MICMB_STEP_GLOBAL follows micm's multi-cell State exactly: one
+ * step size and one convergence test over all cells (device-side control, one
+ * launch group per Newton iteration).  MICMB_STEP_PER_CELL solves each cell as
+ * micm solves a 1-cell State (one persistent kernel, one cell per thread,
+ * cells taken from an atomic queue).  stats are summed over cells (global:
+ * the single control's); per_cell_status / per_cell_accepted as micmb_solve. */
+int micmb_solve_backward_euler(micmb_solver* solver, micmb_state* state, double dt,
+                               const micmb_backward_euler_params* params, int32_t step_control,
+                               micmb_solver_stats* stats, int32_t* per_cell_status,
+                               int32_t* per_cell_accepted);
 
 /* ---- math check ---- */
 #define MICMB_MATH_EXP 0

@@ -114,3 +114,14 @@ def _nonempty(a, key, dtype):
     if a[key].size == 0:
         a[key] = np.zeros(1, dtype=dtype)
     return a[key]
+
+
+class BackwardEulerParams(C.Structure):
+    """micm::BackwardEulerSolverParameters (backward_euler_solver_parameters.hpp:17-29)."""
+    _fields_ = [
+        ("small", C.c_double),
+        ("h_start", C.c_double),
+        ("max_number_of_steps", C.c_int32),
+        ("n_time_step_reductions", C.c_int32),
+        ("time_step_reductions", C.c_double * 8),
+    ]

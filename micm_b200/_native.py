@@ -8,7 +8,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 
-from ._abi import FusedConfig, MechanismDesc, MechanismInfo, RosenbrockParams, SolverStats
+from ._abi import BackwardEulerParams, FusedConfig, MechanismDesc, MechanismInfo, RosenbrockParams, SolverStats
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmicmb.so")
@@ -69,6 +69,9 @@ def lib():
             "micmb_normalized_error": [vp, vp, f64p, f64p],
             "micmb_normalized_error_noalloc": [vp, vp, f64p],
             "micmb_math_eval": [C.c_int32, vp, vp, vp, C.c_int64, C.c_int32],
+            "micmb_backward_euler_params_default": [C.POINTER(BackwardEulerParams)],
+            "micmb_solve_backward_euler": [vp, vp, C.c_double, C.POINTER(BackwardEulerParams), C.c_int32,
+                                           C.POINTER(SolverStats), i32p, i32p],
         }
         for name, args in sig.items():
             fn = getattr(L, name)

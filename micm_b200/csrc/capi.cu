@@ -830,6 +830,32 @@ extern "C"
     });
   }
 
+  int micmb_backward_euler_params_default(micmb_backward_euler_params* out)
+  {
+    return Guard([&] {
+      Need(out != nullptr, "no output");
+      DefaultBackwardEulerParams(out);
+    });
+  }
+
+  int micmb_solve_backward_euler(micmb_solver* solver, micmb_state* state, double dt,
+                                 const micmb_backward_euler_params* params, int32_t step_control,
+                                 micmb_solver_stats* stats, int32_t* per_cell_status, int32_t* per_cell_accepted)
+  {
+    return Guard([&] {
+      Need(solver && state && state->solver == solver, "state does not belong to this solver");
+      Need(dt > 0 && std::isfinite(dt), "time step must be positive and finite");
+      Need(step_control == MICMB_STEP_GLOBAL || step_control == MICMB_STEP_PER_CELL, "unknown step control");
+      SetDevice(*solver);
+      micmb_backward_euler_params p;
+      if (params)
+        p = *params;
+      else
+        DefaultBackwardEulerParams(&p);
+      SolveBackwardEuler(*solver, *state, dt, p, step_control, stats, per_cell_status, per_cell_accepted);
+    });
+  }
+
   int micmb_set_adjoint_memory_limit(micmb_solver* solver, int64_t bytes)
   {
     return Guard([&] {

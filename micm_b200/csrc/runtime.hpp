@@ -135,6 +135,7 @@ struct micmb_state
   micmb_fused_config graph_config{};
   // adjoint working set (allocated on first use)
   micmb::DeviceMemory adj_y0, adj_ybar, adj_ckpt_y, adj_ckpt_h, adj_ckpt_k, adj_kbar_cells, adj_kbar;
+  micmb::DeviceMemory be_ctl;     // Backward Euler global control block
   micmb::DeviceMemory adj_order;  // backward sweep: cells by decreasing step count, then bins
   int64_t adj_ckpt_capacity = 0;  // doubles in adj_ckpt_y
   double dt_for_launch = 0.0;
@@ -216,4 +217,9 @@ namespace micmb
   // cells the one-cell-per-thread forward keeps resident at once
   int64_t FusedThreadResidentCells(const micmb_solver& s);
   int FusedWarpsPerCta(const micmb_solver& s, const micmb_fused_config& cfg);
+  // Backward Euler (global: micm's multi-cell State; per cell: one persistent kernel)
+  void DefaultBackwardEulerParams(micmb_backward_euler_params* p);
+  void SolveBackwardEuler(micmb_solver& s, micmb_state& st, double dt, const micmb_backward_euler_params& params,
+                          int32_t step_control, micmb_solver_stats* stats, int32_t* per_cell_status,
+                          int32_t* per_cell_accepted);
 }  // namespace micmb

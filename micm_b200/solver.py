@@ -23,7 +23,7 @@ from typing import Dict, Optional, Union
 import numpy as np
 
 from . import _native
-from ._abi import DescHolder, FusedConfig, MechanismInfo, RosenbrockParams, SolverStats
+from ._abi import BackwardEulerParams, DescHolder, FusedConfig, MechanismInfo, RosenbrockParams, SolverStats
 from ._native import check, lib
 from .mechanism import Mechanism, from_vector_layout, padded_cells, to_vector_layout
 
@@ -194,6 +194,29 @@ class Solver:
                                 _i32(pac) if per_cell else None))
         return SolverResult(stats.state, stats.as_dict(), pst[:n] if per_cell else None,
                             pac[:n] if per_cell else None)
+
+    def solve_backward_euler(self, dt: float, state: "State", step_control: str = "global",
+                             params: Optional[BackwardEulerParams] = None, per_cell: bool = False) -> SolverResult:
+        """micm's Backward Euler Solve (backward_euler.inl:10-186) on the GPU.  "global": one
+        step size and convergence test for all cells (micm's multi-cell State); "per_cell": each
+        cell as a 1-cell State.  params: micm's defaults when None."""
+        stats = SolverStats()
+        n = state.n_cells
+        pst = np.zeros(max(n, 1), np.int32) if per_cell else None
+        pac = np.zeros(max(n, 1), np.int32) if per_cell else None
+        check(lib().micmb_solve_backward_euler(self.handle, state.handle, float(dt),
+                                               C.byref(params) if params is not None else None,
+                                               STEP_CONTROL[step_control], C.byref(stats),
+                                               _i32(pst) if per_cell else None, _i32(pac) if per_cell else None))
+        return SolverResult(stats.state, stats.as_dict(), pst[:n] if per_cell else None,
+                            pac[:n] if per_cell else None)
+
+    @staticmethod
+    def backward_euler_params() -> BackwardEulerParams:
+        """micm's default Backward Euler parameters (a ctypes struct the caller may edit)."""
+        p = BackwardEulerParams()
+        check(lib().micmb_backward_euler_params_default(C.byref(p)))
+        return p
 
     def autotune(self, dt: float, state: "State", cache_path: Optional[str] = None) -> Dict[str, int]:
         """Time the fused configurations on this state and keep the fastest."""

@@ -69,6 +69,9 @@ def _load_ref():
                                           _f64p, _f64p, _i64p]
         lib.mref_solve_per_cell.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, _f64p, _f64p, _f64p,
                                             _f64p, _f64p, _i64p, C.c_int]
+        if hasattr(lib, "mref_backward_euler_global"):
+            lib.mref_backward_euler_global.argtypes = [C.c_void_p, C.c_int, C.c_double, _f64p, _f64p, _f64p,
+                                                       _f64p, _f64p, _i64p]
         if hasattr(lib, "mref_backward_euler_per_cell"):
             lib.mref_backward_euler_per_cell.argtypes = [C.c_void_p, C.c_int, C.c_double, _f64p, _f64p, _f64p,
                                                          _f64p, _f64p, _i64p]
@@ -225,6 +228,21 @@ class Reference:
             _p(inputs["air_density"]), _p(params), _p(y), _p(stats, C.c_int64)))
         return self.y_from_columns(y), stats
 
+    def backward_euler_global(self, inputs: Dict[str, np.ndarray], dt: float):
+        """micm's Backward Euler on one n-cell State, one Solve(dt):
+        (y_final [n,S] system order, stats row [10])."""
+        if not hasattr(self.lib, "mref_backward_euler_global"):
+            raise RuntimeError("oracle/_ref/libmicm_ref.so predates mref_backward_euler_global; rebuild it")
+        y = self.y_to_columns(inputs["concentrations"])
+        n = len(y)
+        stats = np.zeros(10, np.int64)
+        params = np.ascontiguousarray(inputs["custom_params"] if inputs["custom_params"].size
+                                      else np.zeros((n, 1)))
+        self._check(self.lib.mref_backward_euler_global(
+            self.handle, n, float(dt), _p(inputs["temperature"]), _p(inputs["pressure"]),
+            _p(inputs["air_density"]), _p(params), _p(y), _p(stats, C.c_int64)))
+        return self.y_from_columns(y), stats
+
     def solve_per_cell(self, inputs: Dict[str, np.ndarray], dt: float, n_solves: int = 1,
                        threads: int = 0):
         """A 1-cell State per cell; returns (y_final [n,S] system order, stats rows per cell)."""
@@ -262,6 +280,8 @@ def _load_oracle():
         lib.om_adjoint_per_cell.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, _f64p, _f64p,
                                             C.c_double, _f64p, _f64p, _f64p, _f64p, _f64p, C.c_int, C.c_int]
         lib.om_replay_per_cell.argtypes = [C.c_void_p, C.c_void_p, C.c_int, _f64p, _f64p, _i32p, C.c_int, _f64p]
+        lib.om_backward_euler_global.argtypes = [C.c_void_p, C.c_int, C.c_double, _f64p, _f64p, C.c_double,
+                                                 _f64p, _i64p]
         lib.om_backward_euler_per_cell.argtypes = [C.c_void_p, C.c_int, C.c_double, _f64p, _f64p, C.c_double,
                                                    _f64p, _i64p]
         lib.om_step_sizes_per_cell.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, _f64p, _f64p,
@@ -349,6 +369,21 @@ class Restatement:
         stats = np.zeros((n, 10), np.int64)
         rc = self.lib.om_backward_euler_per_cell(self.handle, n, float(dt), _p(k), _p(self.atol_columns),
                                                  self.mech.relative_tolerance, _p(y), _p(stats, C.c_int64))
+        if rc:
+            raise RuntimeError(self.lib.om_last_error().decode())
+        return np.ascontiguousarray(y[:, self.species_columns]), stats
+
+    def backward_euler_global(self, inputs, dt, k=None):
+        """Backward Euler on one n-cell State (micm's multi-cell semantics):
+        (y_final [n,S] system order, stats [10])."""
+        y = np.zeros_like(inputs["concentrations"])
+        y[:, self.species_columns] = inputs["concentrations"]
+        y = np.ascontiguousarray(y)
+        n = len(y)
+        k = self._k(inputs) if k is None else np.ascontiguousarray(k)
+        stats = np.zeros(10, np.int64)
+        rc = self.lib.om_backward_euler_global(self.handle, n, float(dt), _p(k), _p(self.atol_columns),
+                                               self.mech.relative_tolerance, _p(y), _p(stats, C.c_int64))
         if rc:
             raise RuntimeError(self.lib.om_last_error().decode())
         return np.ascontiguousarray(y[:, self.species_columns]), stats

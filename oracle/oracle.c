@@ -1144,6 +1144,119 @@ int om_backward_euler_per_cell(const om_mech* m, int n, double dt, const double*
   return 0;
 }
 
+/* Backward Euler on one n-cell State (micm's multi-cell semantics,
+ * backward_euler.inl:10-186): one step size, and an attempt converges only
+ * when every cell's test passes (IsConverged :188-246, a logical AND over
+ * cells and species).  y [cell][column] in/out, k [cell][R]; stats_out [10]
+ * as one row of om_solve_per_cell's. */
+int om_backward_euler_global(const om_mech* m, int n, double dt, const double* k, const double* atol, double rtol,
+                             double* y, int64_t* stats_out)
+{
+  const int S = m->S;
+  const double small = 1.0e-40;
+  const int max_iter = 11;
+  const double reductions[5] = { 0.5, 0.5, 0.5, 0.5, 0.1 };
+  double* Yn = xcalloc((size_t)n * S, sizeof(double));
+  double* f = xcalloc((size_t)n * S, sizeof(double));
+  double* J = xcalloc((size_t)m->nnz, sizeof(double));
+  int64_t st[7] = { 0 };
+  double H = dt, t = 0.0;
+  int n_ok = 0, n_fail = 0, state = MICMB_SOLVER_NOT_YET_CALLED;
+  memcpy(Yn, y, sizeof(double) * (size_t)n * S);
+  while (t < dt)
+  {
+    state = MICMB_SOLVER_RUNNING;
+    int converged = 0, iterations = 0;
+    do
+    {
+      st[2]++;
+      st[0]++;
+      st[1]++;
+      st[5]++;
+      st[6]++;
+      for (int c = 0; c < n; ++c)
+      {
+        double* Yc = y + (size_t)c * S;
+        double* fc = f + (size_t)c * S;
+        const double* Ync = Yn + (size_t)c * S;
+        forcing(m, k + (size_t)c * m->R, Yc, fc);
+        neg_jacobian(m, k + (size_t)c * m->R, Yc, J);
+        for (int i = 0; i < S; ++i)
+          J[m->pos[(size_t)i * S + i]] += 1 / H;
+        decompose(m, J);
+        for (int i = 0; i < S; ++i)
+          fc[i] -= (Yc[i] - Ync[i]) / H;
+        lu_solve(m, J, fc);
+        for (int i = 0; i < S; ++i)
+        {
+          const double v = Yc[i] + fc[i];
+          Yc[i] = (0.0 > v) ? 0.0 : v;
+        }
+      }
+      if (iterations++ == 0)
+        continue;
+      converged = 1;
+      for (size_t e = 0; e < (size_t)n * S; ++e)
+      {
+        const double r = f[e];
+        const int i = (int)(e % (size_t)S);
+        if (!isfinite(r))
+          converged = 0;
+        else if (fabs(r) > small && fabs(r) > atol[i] && fabs(r) > rtol * fabs(y[e]))
+          converged = 0;
+      }
+    } while (!converged && iterations < max_iter);
+    if (!converged)
+    {
+      st[4]++;
+      n_ok = 0;
+      if (n_fail >= 5)
+      {
+        t += H;
+        state = OM_SOLVER_ACCEPTING_UNCONVERGED;
+        int any_nan = 0, any_inf = 0;
+        for (size_t e = 0; e < (size_t)n * S; ++e)
+        {
+          any_nan = any_nan || isnan(y[e]);
+          any_inf = any_inf || isinf(y[e]);
+        }
+        if (any_nan)
+          state = MICMB_SOLVER_NAN_DETECTED;
+        else if (any_inf)
+          state = MICMB_SOLVER_INF_DETECTED;
+        break;
+      }
+      memcpy(y, Yn, sizeof(double) * (size_t)n * S);
+      H *= reductions[n_fail++];
+    }
+    else
+    {
+      st[3]++;
+      state = MICMB_SOLVER_CONVERGED;
+      t += H;
+      memcpy(Yn, y, sizeof(double) * (size_t)n * S);
+      if (++n_ok >= 2)
+      {
+        n_ok = 0;
+        H *= 2.0;
+      }
+    }
+    H = dmin(H, dt - t);
+  }
+  if (stats_out)
+  {
+    for (int q = 0; q < 7; ++q)
+      stats_out[q] = st[q];
+    stats_out[7] = state;
+    memcpy(&stats_out[8], &t, sizeof(double));
+    stats_out[9] = 0;
+  }
+  free(Yn);
+  free(f);
+  free(J);
+  return 0;
+}
+
 /* One Rosenbrock step of size H from Y (no error estimate), Y <- Y + sum m_s K_s;
  * the stage recurrences of adjoint_cell's recomputation. */
 static void fixed_step(const om_mech* m, const micmb_rosenbrock_params* p, const double* k, double H, double* Y,

@@ -66,6 +66,10 @@ int om_replay_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n
  * State per cell, one Solve(dt) each; y [cell][column] in/out, stats [cell][10]. */
 int om_backward_euler_per_cell(const om_mech* m, int n, double dt, const double* k, const double* atol, double rtol,
                                double* y, int64_t* stats_out);
+/* Backward Euler on one n-cell State (one step size, one convergence test over
+ * all cells), micm's multi-cell semantics; stats_out [10]. */
+int om_backward_euler_global(const om_mech* m, int n, double dt, const double* k, const double* atol, double rtol,
+                             double* y, int64_t* stats_out);
 int om_step_sizes_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n, double dt, const double* k,
                            const double* atol, double rtol, const double* y0, int max_steps, double* h,
                            int32_t* n_steps);

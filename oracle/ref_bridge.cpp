@@ -645,6 +645,36 @@ extern "C"
     GUARD_END
   }
 
+  // micm's Backward Euler on one n-cell State (one step size and one
+  // convergence test for all cells), one Solve(dt).  y_inout [cell][column];
+  // stats_out [10] as one row of mref_solve_per_cell's.
+  int mref_backward_euler_global(void* p, int n, double dt, const double* T, const double* P, const double* rho,
+                                 const double* params, double* y_inout, int64_t* stats_out)
+  {
+    GUARD_BEGIN
+    auto* h = static_cast<Handle*>(p);
+    const int S = h->built.n_species;
+    auto solver = BuilderBE(micm::BackwardEulerSolverParameters{})
+                      .SetSystem(h->built.system)
+                      .SetReactions(h->built.processes)
+                      .SetReorderState(h->reorder)
+                      .SetIgnoreUnusedSpecies(true)
+                      .Build();
+    auto state = solver.GetState(n);
+    state.SetRelativeTolerance(h->rtol);
+    for (int c = 0; c < n; ++c)
+      LoadCell(state, c, h->n_params, S, T, P, rho, params, y_inout, c);
+    solver.UpdateStateParameters(state);
+    auto r = solver.Solve(dt, state);
+    for (int c = 0; c < n; ++c)
+      for (int j = 0; j < S; ++j)
+        y_inout[(size_t)c * S + j] = state.variables_[c][j];
+    if (stats_out)
+      StatsOut(r, stats_out);
+    return 0;
+    GUARD_END
+  }
+
   // Per-cell step control: a 1-cell State per cell (the reference's own idiom
   // for independent cells, test/tutorial/test_openmp.cpp:115-122), cells split
   // over n_threads host threads.  stats_out [cell][10] accumulates over solves

@@ -20,7 +20,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        sys.exit(f"usage: python {os.path.basename(__file__)} <micm source tree>")
+    ref = sys.argv[1]
     for solver in ("rosenbrock", "backward_euler"):
         path = os.path.join(ref, "test", "regression", "expected_results", f"{solver}_wall_loss.csv")
         with open(path) as f:

@@ -49,7 +49,9 @@ def write(name, doc):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        sys.exit(f"usage: python {os.path.basename(__file__)} <micm source tree>")
+    ref = sys.argv[1]
     out_dir = os.path.join(ROOT, "oracle", "_ref")
     os.makedirs(out_dir, exist_ok=True)
     exe = os.path.join(out_dir, "micm_bench_dump")

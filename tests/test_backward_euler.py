@@ -58,3 +58,15 @@ def test_equals_micms_backward_euler(name, make_mech, make_inputs, dt):
         assert stats[:, 4].max() >= 3 and stats[:, 3].max() >= 5     # rejections and several accepted steps
     if name == "ts1_unconverged":
         assert np.all(stats[:, 7] == 8)                                # AcceptingUnconvergedIntegration
+
+
+@pytest.mark.skipif(not oracle.reference_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("name,make_mech,make_inputs,dt", CASES, ids=[c[0] for c in CASES])
+def test_global_equals_micms_multi_cell_backward_euler(name, make_mech, make_inputs, dt):
+    """micm's n-cell State (one step size, one convergence test over all cells)."""
+    mech = make_mech()
+    inp = make_inputs(mech)
+    y, stats = oracle.Restatement(mech, tableau_kind=3).backward_euler_global(inp, dt)
+    y_micm, stats_micm = oracle.Reference(mech, tableau=3).backward_euler_global(inp, dt)
+    np.testing.assert_array_equal(y, y_micm)
+    np.testing.assert_array_equal(stats[:9], stats_micm[:9])
