@@ -169,42 +169,76 @@ def workload(name: str, cells: int, rank: int = 0):
 def cpu_reference(mech, cfg, inputs, sample: int, uniform: bool = False):
     """micm's own CPU solver (oracle/_ref) over a bounded sample of the workload.
 
+    The baseline figure is micm built for speed (libmicm_ref_fast.so: -O3,
+    AVX2, multiply-add contraction); the bit-exact parity build (no
+    contraction) is timed beside it, and its results are returned for the
+    parity check of the GPU's results on the same cells.
+
     Cells that share their inputs (micm_bench's TS1 case) are timed in micm's
     fastest CPU layout, vector ordering with L = 128 (one State and step size
     per 128 cells), which solves them exactly as per-cell control does.  Cells
     with their own inputs need one step size each, so the baseline is one
     1-cell State per cell (micm's idiom for independent cells); the grouped
     layout is reported beside it for a smaller sample, as it solves a
-    different problem there (each group steps at its hardest cell's pace)."""
+    different problem there (each group steps at its hardest cell's pace).
+
+    Returns (baseline dict, parity build's final concentrations, its per-cell
+    accepted-step counts), or (None, None, None) without the reference."""
     import oracle
     if not oracle.reference_available():
-        return None
+        return None, None, None
+    fast = oracle.reference_available(fast=True)
     n = min(sample, len(inputs["temperature"]))
     sub = {k: v[:n] for k, v in inputs.items()}
-    ref = oracle.Reference(mech, tableau=cfg["stages"])
     threads = os.cpu_count() or 1
     layout_v128 = (f"micm CpuSolverBuilderInPlace with vector ordering L=128 (in-place Mozart LU), one State "
                    f"per 128 cells over {threads} host threads")
-    if uniform:
+    layout_cell = (f"one 1-cell micm State per cell over {threads} host threads, micm CpuSolverBuilderInPlace "
+                   "(vector ordering L=1, in-place Mozart LU)")
+    build_fast = "micm built -O3 -march=x86-64-v3 (FMA contraction on)"
+    build_exact = "micm built -O3 -march=x86-64-v3 -ffp-contract=off (the bit-exact parity build)"
+
+    def timed(fast_build):
+        ref = oracle.Reference(mech, tableau=cfg["stages"], fast=fast_build)
         t0 = time.perf_counter()
-        ref.solve_groups_v128(sub, cfg["dt"], group=128, threads=threads)
-        t = time.perf_counter() - t0
-        return {"value": n / t, "unit": UNIT, "cores": threads, "kind": "reference",
-                "sample": f"{n} cells of the workload, {layout_v128}, {t:.1f} s"}
-    t0 = time.perf_counter()
-    ref.solve_per_cell(sub, cfg["dt"], threads=threads)
-    t = time.perf_counter() - t0
-    out = {"value": n / t, "unit": UNIT, "cores": threads, "kind": "reference",
-           "sample": f"{n} cells of the workload, one 1-cell micm State per cell over {threads} host threads, "
-                     f"micm CpuSolverBuilderInPlace (vector ordering L=1, in-place Mozart LU), {t:.1f} s"}
-    ng = min(n, 16384)
-    t0 = time.perf_counter()
-    ref.solve_groups_v128({k: v[:ng] for k, v in inputs.items()}, cfg["dt"], group=128, threads=threads)
-    tg = time.perf_counter() - t0
-    out["vector128_groups"] = {"value": ng / tg, "unit": UNIT,
-                               "sample": f"{ng} cells, {layout_v128}, {tg:.1f} s; one step size per group, "
-                                         "so not the per-cell solve"}
-    return out
+        if uniform:
+            y, st = ref.solve_groups_v128(sub, cfg["dt"], group=128, threads=threads)
+        else:
+            y, st = ref.solve_per_cell(sub, cfg["dt"], threads=threads)
+        return time.perf_counter() - t0, y, st
+
+    t_exact, y_ref, st_ref = timed(False)
+    t_base, build = (timed(True)[0], build_fast) if fast else (t_exact, build_exact)
+    layout = layout_v128 if uniform else layout_cell
+    out = {"value": n / t_base, "unit": UNIT, "cores": threads, "kind": "reference",
+           "sample": f"{n} cells of the workload, {layout}, {build}, {t_base:.1f} s",
+           "parity_build": {"value": n / t_exact, "unit": UNIT, "sample": f"same cells, {build_exact}, "
+                                                                          f"{t_exact:.1f} s"}}
+    if not uniform:
+        ng = min(n, 16384)
+        ref = oracle.Reference(mech, tableau=cfg["stages"], fast=fast)
+        t0 = time.perf_counter()
+        ref.solve_groups_v128({k: v[:ng] for k, v in inputs.items()}, cfg["dt"], group=128, threads=threads)
+        tg = time.perf_counter() - t0
+        out["vector128_groups"] = {"value": ng / tg, "unit": UNIT,
+                                   "sample": f"{ng} cells, {layout_v128}, {build if fast else build_exact}, "
+                                             f"{tg:.1f} s; one step size per group, so not the per-cell solve"}
+    return out, y_ref, np.asarray(st_ref)[:, 3]
+
+
+def parity_summary(y_gpu, acc_gpu, y_ref, acc_ref, rtol=1e-6, atol=1e-12):
+    """The GPU's final concentrations and accepted-step counts against micm's on
+    the same cells: the north-star criterion (every species within rtol / atol,
+    identical step counts in at least 99.9 % of cells)."""
+    d = np.abs(y_gpu - y_ref)
+    bound = atol + rtol * np.abs(y_ref)
+    sig = np.abs(y_ref) >= atol
+    return {"cells": int(len(y_ref)), "rtol": rtol, "atol": atol,
+            "frac_cells_within_rtol_atol": float(np.mean(np.all(d <= bound, axis=1))),
+            "max_err_over_bound": float(np.max(d / bound)),
+            "max_rel_err": float(np.max(d[sig] / np.abs(y_ref[sig]))) if sig.any() else 0.0,
+            "frac_identical_accepted": float(np.mean(np.asarray(acc_gpu) == np.asarray(acc_ref))),
+            "frac_bitwise_identical_cells": float(np.mean(np.all(y_gpu == y_ref, axis=1)))}
 
 
 def run_reference_arm(args):
@@ -216,7 +250,10 @@ def run_reference_arm(args):
     if not oracle.reference_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmicm_ref.so was not built"}))
         return
-    ref = oracle.Reference(mech, tableau=cfg["stages"])
+    fast = oracle.reference_available(fast=True)
+    ref = oracle.Reference(mech, tableau=cfg["stages"], fast=fast)
+    build = ("micm built -O3 -march=x86-64-v3 (FMA contraction on)" if fast
+             else "micm built -O3 -march=x86-64-v3 -ffp-contract=off")
     threads = os.cpu_count() or 1
     n = args.cpu_sample
     # identical cells (micm_bench's TS1 case): micm's vector-128 layout; else one 1-cell State per cell
@@ -243,7 +280,7 @@ def run_reference_arm(args):
                                    + f"; each step a {n}-cell sample on the host",
                        "cells_per_step": n},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
-                             "sample": f"{n} cells per step, {layout} over {threads} threads"},
+                             "sample": f"{n} cells per step, {layout} over {threads} threads, {build}"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -474,7 +511,37 @@ def main():
         torch.cuda.synchronize()
     ms = start.elapsed_time(end)
     kernel_ms = sum(a.elapsed_time(b) for a, b in events)
-    ms, kernel_ms = max_over_ranks([ms, kernel_ms], dist, "cuda")
+
+    # the same steps replayed from a CUDA graph (UpdateStateParameters + the
+    # fused Solve captured once per state and time step, micmb_solve_graph)
+    y_view.copy_(y_dev)
+    solver.solve_graph(cfg["dt"], state, 1)                   # capture (and one run)
+    graph_events = []
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        y_view.copy_(y_dev)
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        solver.solve_graph(cfg["dt"], state, 1)
+        g1.record(stream)
+        graph_events.append((g0, g1))
+    torch.cuda.synchronize()
+    graph_ms = sum(a.elapsed_time(b) for a, b in graph_events)
+    ms, kernel_ms, graph_ms = max_over_ranks([ms, kernel_ms, graph_ms], dist, "cuda")
+
+    # parity at the metric's scale: the fused solve's results on the cells the
+    # CPU baseline solves (the first cpu_sample cells of this shard)
+    n_par = min(args.cpu_sample, args.cells) if (rank == 0 and not args.no_cpu) else 0
+    gpu_par = None
+    if n_par:
+        from micm_b200.mechanism import from_vector_layout, padded_cells
+        y_view.copy_(y_dev)
+        rpar = solver.solve(cfg["dt"], state, method="fused", step_control="per_cell", per_cell=True)
+        torch.cuda.synchronize()
+        n_pad = padded_cells(n_par, L)
+        yv = y_view[: n_pad * mech.n_species].cpu().numpy()
+        y_cols = from_vector_layout(yv, n_par, mech.n_species, L)
+        gpu_par = (y_cols[:, solver.compiled.species_columns], rpar.per_cell_accepted[:n_par].copy())
     value = job_throughput(args.cells, world, args.steps, ms / 1000.0)
     attempts_per_cell = totals["number_of_steps"] / (args.cells * args.steps)
     accepted_per_cell = totals["accepted"] / (args.cells * args.steps)
@@ -570,9 +637,15 @@ def main():
         same = W["adjoint"][0] == args.workload            # same mechanism: keep the configuration tuned above
         adj = adjoint_ratio(torch, rank, *W["adjoint"], fused_config=tuned if same else None)
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and not args.no_cpu:
-        cpu = cpu_reference(mech, cfg, inputs, args.cpu_sample, uniform=args.workload in ("ts1", "chapman"))
+        cpu, y_ref, acc_ref = cpu_reference(mech, cfg, inputs, args.cpu_sample,
+                                            uniform=args.workload in ("ts1", "chapman"))
+        if cpu is not None and gpu_par is not None:
+            parity = parity_summary(gpu_par[0], gpu_par[1], y_ref, acc_ref)
+            parity["reference"] = ("micm (oracle/_ref parity build) on the same cells, "
+                                   + ("micm_bench's vector-128 layout" if args.workload in ("ts1", "chapman")
+                                      else "one 1-cell State per cell"))
 
     if rank == 0:
         info = solver.compiled.info
@@ -601,6 +674,12 @@ def main():
                                   "frac": flops / kernel_s / 1e12 / fp64_peak(), "flops_per_launch": flops,
                                   "peak_source": "nominal (SMs x 64 FMA/clk x 2 x max SM clock)"}},
             "gpu_launches": args.steps,
+            "graph": {"value": job_throughput(args.cells, world, args.steps, graph_ms / 1000.0), "unit": UNIT,
+                      "ms_per_step": graph_ms / args.steps,
+                      "note": "each step one replay of a CUDA graph holding UpdateStateParameters and the fused "
+                              "Solve (micmb_solve_graph), after the same device copy of the initial "
+                              "concentrations; rate constants are recomputed inside every replay"},
+            "parity": parity,
             "plain": plain,
             "adjoint": adj,
             "cpu_baseline": cpu,

@@ -25,6 +25,8 @@ from micm_b200.mechanism import Mechanism
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libmicm_ref.so")
+# micm built for speed (FMA contraction, AVX2): the CPU baseline, not a parity checker
+REF_LIB_FAST = os.path.join(HERE, "_ref", "libmicm_ref_fast.so")
 ORACLE_LIB = os.path.join(HERE, "liboracle.so")
 
 _f64p = C.POINTER(C.c_double)
@@ -39,17 +41,16 @@ def _p(a, t=C.c_double):
     return a.ctypes.data_as(C.POINTER(t))
 
 
-_ref = None
+_ref = {}
 
 
-def reference_available() -> bool:
-    return os.path.exists(REF_LIB)
+def reference_available(fast: bool = False) -> bool:
+    return os.path.exists(REF_LIB_FAST if fast else REF_LIB)
 
 
-def _load_ref():
-    global _ref
-    if _ref is None:
-        lib = C.CDLL(REF_LIB)
+def _load_ref(fast: bool = False):
+    if fast not in _ref:
+        lib = C.CDLL(REF_LIB_FAST if fast else REF_LIB)
         lib.mref_last_error.restype = C.c_char_p
         lib.mref_create.restype = C.c_void_p
         lib.mref_create.argtypes = [C.c_void_p, _f64p, C.c_double, C.c_int]
@@ -78,8 +79,8 @@ def _load_ref():
         if hasattr(lib, "mref_solve_groups_v128"):
             lib.mref_solve_groups_v128.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int, _f64p, _f64p,
                                                    _f64p, _f64p, _f64p, _i64p, C.c_int]
-        _ref = lib
-    return _ref
+        _ref[fast] = lib
+    return _ref[fast]
 
 
 def _stats_rows(raw: np.ndarray):
@@ -92,10 +93,12 @@ def _stats_rows(raw: np.ndarray):
 
 
 class Reference:
-    """micm's own CPU Rosenbrock (in-place Mozart LU, vector ordering)."""
+    """micm's own CPU Rosenbrock (in-place Mozart LU, vector ordering).
+    fast=True loads the build for speed (the CPU baseline) instead of the
+    bit-exact parity build."""
 
-    def __init__(self, mech: Mechanism, tableau: int = 3):
-        self.lib = _load_ref()
+    def __init__(self, mech: Mechanism, tableau: int = 3, fast: bool = False):
+        self.lib = _load_ref(fast)
         self.mech = mech
         self._desc = DescHolder(mech.flat())
         atol = np.ascontiguousarray(mech.atol())
@@ -280,6 +283,10 @@ def _load_oracle():
         lib.om_adjoint_per_cell.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, _f64p, _f64p,
                                             C.c_double, _f64p, _f64p, _f64p, _f64p, _f64p, C.c_int, C.c_int]
         lib.om_replay_per_cell.argtypes = [C.c_void_p, C.c_void_p, C.c_int, _f64p, _f64p, _i32p, C.c_int, _f64p]
+        lib.om_set_correctly_rounded.argtypes = [C.c_void_p, C.c_int]
+        lib.om_set_correctly_rounded.restype = None
+        lib.om_math_eval.argtypes = [C.c_void_p, C.c_int, _f64p, _f64p, _f64p, C.c_int64]
+        lib.om_math_eval.restype = None
         lib.om_backward_euler_global.argtypes = [C.c_void_p, C.c_int, C.c_double, _f64p, _f64p, C.c_double,
                                                  _f64p, _i64p]
         lib.om_backward_euler_per_cell.argtypes = [C.c_void_p, C.c_int, C.c_double, _f64p, _f64p, C.c_double,
@@ -306,13 +313,17 @@ def tableau(kind: int):
 class Restatement:
     """oracle.c: plain-C restatement of micm's Rosenbrock path + discrete adjoint."""
 
-    def __init__(self, mech: Mechanism, tableau_kind: int = 3, params=None):
+    def __init__(self, mech: Mechanism, tableau_kind: int = 3, params=None, correctly_rounded: bool = False):
+        """correctly_rounded: exp, pow and log10 of the rate constants and the
+        step-size factor correctly rounded (quad precision) instead of the C
+        library's (micm's)."""
         self.lib = _load_oracle()
         self.mech = mech
         self._desc = DescHolder(mech.flat())
         self.handle = self.lib.om_create(C.byref(self._desc.desc))
         if not self.handle:
             raise RuntimeError("om_create: " + self.lib.om_last_error().decode())
+        self.lib.om_set_correctly_rounded(self.handle, 1 if correctly_rounded else 0)
         self.S, self.R = mech.n_species, mech.n_reactions
         self.params = params if params is not None else tableau(tableau_kind)
         self.species_columns = np.zeros(self.S, np.int32)
@@ -327,6 +338,14 @@ class Restatement:
         self.lib.om_jacobian_pattern(self.handle, _p(self.rows, C.c_int32), _p(self.cols, C.c_int32))
         self.atol_columns = np.zeros(self.S)
         self.atol_columns[self.species_columns] = mech.atol()
+
+    def math_eval(self, fn: int, x, y=None):
+        """exp (0), log10 (1) or pow (2) element-wise in this handle's mode."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.ascontiguousarray(x if y is None else y, dtype=np.float64)
+        out = np.empty_like(x)
+        self.lib.om_math_eval(self.handle, int(fn), _p(x), _p(y), _p(out), len(x))
+        return out
 
     def __del__(self):
         if getattr(self, "handle", None):

@@ -8,6 +8,7 @@
 #include "oracle.h"
 
 #include <math.h>
+#include <quadmath.h>
 #include <pthread.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -37,6 +38,7 @@ struct om_mech
   int *info_ind, *info_rxn, *info_ds, *info_dep;
   int* pos; /* [S*S] storage position or -1 */
   int *nz_row, *nz_col;
+  int cr; /* 0: the C library's exp/pow/log10 (micm's); 1: correctly rounded (quad precision) */
 };
 
 #define NA 6.02214076e23
@@ -375,12 +377,44 @@ void om_jacobian_pattern(const om_mech* m, int32_t* rows, int32_t* cols)
 /* ---------------------------------------------------------------- */
 /* rate constants (rate_constant_functions.hpp:52-136)               */
 /* ---------------------------------------------------------------- */
-static double falloff(const double* p, double T, double rho, double scale)
+/* The transcendental functions of the rate constants and the step-size
+ * factor: the C library's (what micm calls), or correctly rounded results
+ * (evaluated in quad precision by libquadmath, then rounded once to double;
+ * wrong only when the exact value lies within about 2^-60 ulp of a rounding
+ * boundary).  The second mode is an independent check of the GPU library's
+ * own correctly rounded functions. */
+static double o_exp(const om_mech* m, double x)
 {
-  double k0 = p[0] * exp(p[2] / T) * pow(T / 300.0, p[1]);
-  double kinf = p[3] * exp(p[5] / T) * pow(T / 300.0, p[4]);
+  return m->cr ? (double)expq((__float128)x) : exp(x);
+}
+static double o_pow(const om_mech* m, double x, double y)
+{
+  return m->cr ? (double)powq((__float128)x, (__float128)y) : pow(x, y);
+}
+static double o_log10(const om_mech* m, double x)
+{
+  return m->cr ? (double)log10q((__float128)x) : log10(x);
+}
+
+void om_set_correctly_rounded(om_mech* m, int on)
+{
+  m->cr = on ? 1 : 0;
+}
+
+/* exp (fn 0), log10 (1) or pow (2) with the mode's functions, element-wise
+ * (for tests of both modes) */
+void om_math_eval(const om_mech* m, int fn, const double* x, const double* y, double* out, int64_t n)
+{
+  for (int64_t i = 0; i < n; ++i)
+    out[i] = fn == 0 ? o_exp(m, x[i]) : (fn == 1 ? o_log10(m, x[i]) : o_pow(m, x[i], y[i]));
+}
+
+static double falloff(const om_mech* m, const double* p, double T, double rho, double scale)
+{
+  double k0 = p[0] * o_exp(m, p[2] / T) * o_pow(m, T / 300.0, p[1]);
+  double kinf = p[3] * o_exp(m, p[5] / T) * o_pow(m, T / 300.0, p[4]);
   double ratio = k0 * rho / kinf;
-  return k0 * scale / (1.0 + ratio) * pow(p[6], p[7] / (p[7] + pow(log10(ratio), 2.0)));
+  return k0 * scale / (1.0 + ratio) * o_pow(m, p[6], p[7] / (p[7] + o_pow(m, o_log10(m, ratio), 2.0)));
 }
 
 static double rate_constant(const om_mech* m, int r, double T, double Pr, double rho, const double* prm)
@@ -389,29 +423,29 @@ static double rate_constant(const om_mech* m, int r, double T, double Pr, double
   double k = 0.0;
   switch (m->kind[r])
   {
-    case MICMB_RATE_ARRHENIUS: k = p[0] * exp(p[2] / T) * pow(T / p[3], p[1]) * (1.0 + p[4] * Pr); break;
-    case MICMB_RATE_TROE: k = falloff(p, T, rho, rho); break;
-    case MICMB_RATE_TERNARY_CHEMICAL_ACTIVATION: k = falloff(p, T, rho, 1.0); break;
+    case MICMB_RATE_ARRHENIUS: k = p[0] * o_exp(m, p[2] / T) * o_pow(m, T / p[3], p[1]) * (1.0 + p[4] * Pr); break;
+    case MICMB_RATE_TROE: k = falloff(m, p, T, rho, rho); break;
+    case MICMB_RATE_TERNARY_CHEMICAL_ACTIVATION: k = falloff(m, p, T, rho, 1.0); break;
     case MICMB_RATE_BRANCHED:
     {
       double a = p[5] * rho;
-      double b = 0.43 * pow(T / 298.0, -8.0);
-      double A_val = a / (1.0 + a / b) * pow(0.41, 1.0 / (1.0 + pow(log10(a / b), 2.0)));
-      double pre = p[1] * exp(-p[2] / T);
+      double b = 0.43 * o_pow(m, T / 298.0, -8.0);
+      double A_val = a / (1.0 + a / b) * o_pow(m, 0.41, 1.0 / (1.0 + o_pow(m, o_log10(m, a / b), 2.0)));
+      double pre = p[1] * o_exp(m, -p[2] / T);
       k = (p[0] == 0.0) ? pre * (p[6] / (p[6] + A_val)) : pre * (A_val / (A_val + p[6]));
       break;
     }
-    case MICMB_RATE_TUNNELING: k = p[0] * exp(-p[1] / T + p[2] / (T * T * T)); break;
+    case MICMB_RATE_TUNNELING: k = p[0] * o_exp(m, -p[1] / T + p[2] / (T * T * T)); break;
     case MICMB_RATE_TAYLOR_SERIES:
     {
       double poly = 0.0, tp = 1.0;
       int n = (int)p[5];
       for (int j = 0; j < n; ++j, tp *= T)
         poly += p[6 + j] * tp;
-      k = poly * p[0] * exp(p[2] / T) * pow(T / p[3], p[1]) * (1.0 + p[4] * Pr);
+      k = poly * p[0] * o_exp(m, p[2] / T) * o_pow(m, T / p[3], p[1]) * (1.0 + p[4] * Pr);
       break;
     }
-    case MICMB_RATE_REVERSIBLE: k = p[0] * exp(p[1] / T) * p[2]; break;
+    case MICMB_RATE_REVERSIBLE: k = p[0] * o_exp(m, p[1] / T) * p[2]; break;
     case MICMB_RATE_USER_DEFINED: k = prm[m->pcol[r]] * p[0]; break;
     case MICMB_RATE_SURFACE:
     {
@@ -686,7 +720,7 @@ static int rosenbrock_cell(const om_mech* m, const micmb_rosenbrock_params* p, d
       }
       double error = dmax(sqrt(sum / (double)(S > 0 ? S : 1)), 1.0e-10);
       double fac = dmin(p->factor_max,
-                        dmax(p->factor_min, p->safety_factor / pow(error, 1 / p->estimator_of_local_order)));
+                        dmax(p->factor_min, p->safety_factor / o_pow(m, error, 1 / p->estimator_of_local_order)));
       double Hnew = H * fac;
       nst++;
       if (isnan(error))

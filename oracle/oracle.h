@@ -64,6 +64,12 @@ int om_replay_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n
 /* Accepted step sizes of a per-cell solve from y0 [cell][S]. */
 /* Backward Euler (micm's backward_euler.inl, default parameters), a 1-cell
  * State per cell, one Solve(dt) each; y [cell][column] in/out, stats [cell][10]. */
+/* 0 (default): exp, pow and log10 of the rate constants and the step-size
+ * factor from the C library, as micm calls them; 1: correctly rounded (quad
+ * precision).  om_math_eval evaluates exp (0), log10 (1) or pow (2)
+ * element-wise in the handle's mode. */
+void om_set_correctly_rounded(om_mech* m, int on);
+void om_math_eval(const om_mech* m, int fn, const double* x, const double* y, double* out, int64_t n);
 int om_backward_euler_per_cell(const om_mech* m, int n, double dt, const double* k, const double* atol, double rtol,
                                double* y, int64_t* stats_out);
 /* Backward Euler on one n-cell State (one step size, one convergence test over

@@ -80,6 +80,20 @@ def test_agrees_with_glibc_except_where_glibc_misrounds():
     assert np.mean(got == libc) >= 0.995
 
 
+def test_agrees_with_the_oracles_quad_precision_functions():
+    """Two independent correctly rounded implementations (this library's
+    double-double code, the oracle's libquadmath evaluation) agree on every
+    sample."""
+    import oracle
+    from micm_b200 import synthetic
+    if not oracle.restatement_available():
+        pytest.skip("oracle not built")
+    R = oracle.Restatement(synthetic.readme_mechanism(), 3, correctly_rounded=True)
+    x_exp, x_log, x_pow, y_pow = _samples(seed=14, n=20000)
+    for fn, x, y in ((EXP, x_exp, None), (LOG10, x_log, None), (POW, x_pow, y_pow)):
+        assert np.array_equal(_host(fn, x, y), R.math_eval(fn, x, y)), fn
+
+
 def test_special_arguments():
     assert list(_host(POW, [2.0, 9.0, -3.0, 0.0, 5.0], [0.5, 0.5, 2.0, 0.25, 0.0])) == [math.sqrt(2.0), 3.0, 9.0, 0.0, 1.0]
     assert list(_host(LOG10, [1.0, 10.0, 1e-300, 1e300])) == [0.0, 1.0, -300.0, 300.0]

@@ -153,3 +153,32 @@ def test_autograd_function(cuda_device):
     g0_cols, gk, _ = solver.solve_adjoint(cfg["dt"], st, g)
     np.testing.assert_array_equal(y0.grad.cpu().numpy(), g0_cols[:, cols])
     np.testing.assert_array_equal(logs.grad.cpu().numpy(), gk)
+
+
+def test_adjoint_configuration_spot_check(cuda_device):
+    """The adjoint configuration (60 species, 120 reactions, dt = 3600 s) at
+    8,192 cells: the GPU's dL/dy0 on a seeded sample of 64 cells, and the
+    per-cell rate-parameter gradients of those cells (through a loss that
+    touches only them), against the FP64 CPU adjoint oracle."""
+    n, n_check = 8192, 64
+    cfg, mech, inputs, solver, st = _setup("c60_adjoint", n, 43)
+    k = np.ascontiguousarray(st.rate_constants())
+    rng = np.random.default_rng(9)
+    pick = np.sort(rng.choice(n, n_check, replace=False))
+    cols = solver.compiled.species_columns
+    ybar_sys = np.zeros((n, mech.n_species))
+    ybar_sys[pick] = rng.normal(size=(n_check, mech.n_species))
+    ybar_cols = np.zeros_like(ybar_sys)
+    ybar_cols[:, cols] = ybar_sys
+    g0_cols, gk, res = solver.solve_adjoint(cfg["dt"], st, ybar_cols, max_checkpoints=400)
+    assert res.converged
+    g0 = g0_cols[:, cols]
+    sub = {key: v[pick] for key, v in inputs.items()}
+    R = oracle.Restatement(mech, tableau_kind=cfg["stages"])
+    _, g0_ref, gk_ref = R.adjoint_per_cell(sub, cfg["dt"], ybar_sys[pick], k=k[pick], max_steps=400)
+    scale = np.abs(g0_ref).max(axis=1, keepdims=True)
+    sig = _significant(g0_ref, scale)
+    assert (np.abs(g0[pick] - g0_ref)[sig] / np.abs(g0_ref)[sig]).max() < 1e-8
+    assert np.all(g0[np.setdiff1d(np.arange(n), pick)] == 0.0)
+    gk_ref_sum = gk_ref.sum(axis=0)
+    np.testing.assert_allclose(gk, gk_ref_sum, rtol=1e-8, atol=1e-9 * np.abs(gk_ref_sum).max())
