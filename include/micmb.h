@@ -367,6 +367,24 @@ int micmb_normalized_error(micmb_solver* solver, micmb_state* state, double* glo
  * (different streams or host threads) race on it, so serialise them. */
 int micmb_normalized_error_noalloc(micmb_solver* solver, micmb_state* state, double* global_out);
 
+/* ---- global step control over several GPUs (one process per GPU) ---- */
+/* All-gather of one double per rank: recv[r] = rank r's send[0], in rank
+ * order (device pointers), queued on `stream` (a cudaStream_t) after the work
+ * already queued there.  Called on the host once per step attempt while a
+ * solve queues its kernels; it must not wait for the stream.  Returns 0 on
+ * success. */
+typedef int (*micmb_allgather_fn)(const double* send, double* recv, int32_t world, void* stream, void* user);
+/* Makes MICMB_STEP_GLOBAL plain solves of this state one shard of a job over
+ * `world` ranks: per step attempt the shard's sum of scaled squared errors
+ * goes through `fn`, every rank adds the gathered sums in rank order and
+ * divides by total_cells * n_species, so every rank takes the same step-size
+ * decisions -- micm's global NormalizedError (include/micm/solver/
+ * rosenbrock.inl:353-402) over the whole job, one 8-byte exchange per
+ * attempt.  Every rank must call micmb_solve the same number of times with
+ * the same dt.  fn = NULL restores the single-GPU solve. */
+int micmb_state_set_global_exchange(micmb_state* state, micmb_allgather_fn fn, void* user, int32_t world,
+                                    int64_t total_cells);
+
 /* ---- Backward Euler (micm's second integrator) ---- */
 /* micm::BackwardEulerSolverParameters
  * (include/micm/solver/backward_euler_solver_parameters.hpp:17-29). */

@@ -26,6 +26,10 @@ class MicmbError(RuntimeError):
         self.code = code
 
 
+# int allgather(const double* send, double* recv, int32_t world, void* stream, void* user)
+ALLGATHER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p)
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -69,6 +73,7 @@ def lib():
             "micmb_normalized_error": [vp, vp, f64p, f64p],
             "micmb_normalized_error_noalloc": [vp, vp, f64p],
             "micmb_math_eval": [C.c_int32, vp, vp, vp, C.c_int64, C.c_int32],
+            "micmb_state_set_global_exchange": [vp, ALLGATHER_FN, vp, C.c_int32, C.c_int64],
             "micmb_backward_euler_params_default": [C.POINTER(BackwardEulerParams)],
             "micmb_solve_backward_euler": [vp, vp, C.c_double, C.POINTER(BackwardEulerParams), C.c_int32,
                                            C.POINTER(SolverStats), i32p, i32p],

@@ -830,6 +830,31 @@ extern "C"
     });
   }
 
+  int micmb_state_set_global_exchange(micmb_state* state, micmb_allgather_fn fn, void* user, int32_t world,
+                                      int64_t total_cells)
+  {
+    return Guard([&] {
+      Need(state != nullptr, "no state");
+      if (!fn)
+      {
+        state->gx_fn = nullptr;
+        state->gx_user = nullptr;
+        state->gx_world = 1;
+        state->gx_total_cells = 0;
+        return;
+      }
+      Need(world >= 1 && world <= 65536, "world must be 1..65536");
+      Need(total_cells >= state->n_cells, "total_cells must count every rank's cells");
+      SetDevice(*state->solver);
+      if (!state->gx_buf.p || state->gx_buf.bytes < sizeof(double) * (size_t)(1 + world))
+        state->gx_buf = DeviceMemory(sizeof(double) * (size_t)(1 + world));
+      state->gx_fn = fn;
+      state->gx_user = user;
+      state->gx_world = world;
+      state->gx_total_cells = total_cells;
+    });
+  }
+
   int micmb_backward_euler_params_default(micmb_backward_euler_params* out)
   {
     return Guard([&] {

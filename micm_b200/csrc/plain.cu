@@ -288,30 +288,63 @@ namespace micmb
         blk_err[blockIdx.x] = t;
     }
 
-    // Global decision: the block partials reduced in a fixed order by one
-    // block (each thread a strided sequential sum, then a fixed tree), then
-    // micm's step control.  Deterministic for a given cell count.
+    // The block partials reduced in a fixed order by one block: each thread a
+    // strided sequential sum, then a fixed tree.  Deterministic for a given
+    // cell count.
+    __device__ __forceinline__ double reduce_blocks(const double* blk_err, int64_t n_blk, double* red)
+    {
+      double acc = 0.0;
+      for (int64_t i = threadIdx.x; i < n_blk; i += kBlock)
+        acc += blk_err[i];
+      return block_tree_sum(acc, red);
+    }
+
+    // micm's step control from the job's sum of squared scaled errors
+    __device__ __forceinline__ void global_decide(const PlainArgs& a, const DevParams& P, const StepBounds& b,
+                                                  double total, double n_values, int32_t* last_accept)
+    {
+      const double error = error_from_sum(total, n_values > 0.0 ? n_values : 1.0);
+      CellCtl cc = a.ctl[0];
+      count_attempt(cc, P);
+      const int res = ctl_after_error(cc, P, b, error);
+      *last_accept = (res == 1);
+      a.status[0] = cc.state;
+      a.ctl[0] = cc;
+    }
+
+    // Global decision on one GPU: all cells' partials, then the step control.
     __global__ void k_global_decide(PlainArgs a, DevParams P, StepBounds b, int32_t S, const double* blk_err,
                                     int64_t n_blk, int32_t* last_accept)
     {
       __shared__ double red[kBlock];
       if (a.status[0] != MICMB_SOLVER_RUNNING)
         return;
-      double acc = 0.0;
-      for (int64_t i = threadIdx.x; i < n_blk; i += kBlock)
-        acc += blk_err[i];
-      const double total = block_tree_sum(acc, red);
+      const double total = reduce_blocks(blk_err, n_blk, red);
       if (threadIdx.x == 0)
-      {
-        const double N = (double)(a.n * (int64_t)S > 0 ? a.n * (int64_t)S : 1);
-        const double error = error_from_sum(total, N);
-        CellCtl cc = a.ctl[0];
-        count_attempt(cc, P);
-        const int res = ctl_after_error(cc, P, b, error);
-        *last_accept = (res == 1);
-        a.status[0] = cc.state;
-        a.ctl[0] = cc;
-      }
+        global_decide(a, P, b, total, (double)(a.n * (int64_t)S), last_accept);
+    }
+
+    // Several ranks, first half: this shard's sum (the same reduction), for the exchange.
+    __global__ void k_shard_sum(PlainArgs a, const double* blk_err, int64_t n_blk, double* shard_sum)
+    {
+      __shared__ double red[kBlock];
+      if (a.status[0] != MICMB_SOLVER_RUNNING)
+        return;
+      const double total = reduce_blocks(blk_err, n_blk, red);
+      if (threadIdx.x == 0)
+        *shard_sum = total;
+    }
+
+    // Several ranks, second half: the gathered shard sums added in rank order.
+    __global__ void k_global_decide_gathered(PlainArgs a, DevParams P, StepBounds b, const double* gathered,
+                                             int32_t world, double n_values, int32_t* last_accept)
+    {
+      if (a.status[0] != MICMB_SOLVER_RUNNING)
+        return;
+      double total = 0.0;
+      for (int32_t r = 0; r < world; ++r)
+        total += gathered[r];
+      global_decide(a, P, b, total, n_values, last_accept);
     }
 
     __global__ void k_global_apply(DevMech M, PlainArgs a, const int32_t* last_accept)
@@ -494,7 +527,18 @@ namespace micmb
         if (global)
         {
           k_finish_partial<<<grid, kBlock, 0, stream>>>(s.dev, a, P, a.err_cell);
-          k_global_decide<<<1, kBlock, 0, stream>>>(a, P, b, m.S, a.err_cell, (int64_t)grid, last_accept);
+          if (st.gx_fn)
+          {
+            double* gx = st.gx_buf.as<double>();
+            k_shard_sum<<<1, kBlock, 0, stream>>>(a, a.err_cell, (int64_t)grid, gx);
+            MICMB_CUDA(cudaGetLastError());
+            if (st.gx_fn(gx, gx + 1, st.gx_world, stream, st.gx_user) != 0)
+              throw Error(MICMB_ERR_INTERNAL, "global step control: the all-gather of the error sums failed");
+            k_global_decide_gathered<<<1, 1, 0, stream>>>(a, P, b, gx + 1, st.gx_world,
+                                                          (double)st.gx_total_cells * (double)m.S, last_accept);
+          }
+          else
+            k_global_decide<<<1, kBlock, 0, stream>>>(a, P, b, m.S, a.err_cell, (int64_t)grid, last_accept);
           k_global_apply<<<grid, kBlock, 0, stream>>>(s.dev, a, last_accept);
         }
         else

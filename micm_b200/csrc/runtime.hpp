@@ -136,6 +136,12 @@ struct micmb_state
   // adjoint working set (allocated on first use)
   micmb::DeviceMemory adj_y0, adj_ybar, adj_ckpt_y, adj_ckpt_h, adj_ckpt_k, adj_kbar_cells, adj_kbar;
   micmb::DeviceMemory be_ctl;     // Backward Euler global control block
+  // global step control over several ranks (micmb_state_set_global_exchange)
+  micmb_allgather_fn gx_fn = nullptr;
+  void* gx_user = nullptr;
+  int32_t gx_world = 1;
+  int64_t gx_total_cells = 0;
+  micmb::DeviceMemory gx_buf;     // [0]: this shard's sum; [1, 1 + world): the gathered sums
   micmb::DeviceMemory adj_order;  // backward sweep: cells by decreasing step count, then bins
   int64_t adj_ckpt_capacity = 0;  // doubles in adj_ckpt_y
   double dt_for_launch = 0.0;

@@ -304,6 +304,25 @@ class State:
         if self.P:
             self.set_custom_rate_parameters(inputs["custom_params"])
 
+    def set_global_exchange(self, allgather, world: int, total_cells: int):
+        """Make global-step-control solves of this state one shard of a job over
+        `world` ranks.  allgather(send_ptr, recv_ptr, world, stream_ptr) -> int
+        queues, on the CUDA stream, an all-gather of one double per rank from
+        device address send_ptr into recv_ptr[0:world] in rank order.  None
+        restores the single-GPU solve."""
+        from ._native import ALLGATHER_FN
+        if allgather is None:
+            self._gx = None
+            check(lib().micmb_state_set_global_exchange(self.handle, ALLGATHER_FN(), None, 1, 0))
+            return
+        def trampoline(send, recv, w, stream, _user):
+            try:
+                return int(allgather(send, recv, w, stream) or 0)
+            except Exception:  # an exception must not cross the C ABI
+                return -1
+        self._gx = ALLGATHER_FN(trampoline)  # kept alive as long as the state
+        check(lib().micmb_state_set_global_exchange(self.handle, self._gx, None, int(world), int(total_cells)))
+
     def upload(self, buffer: int, host_vector_layout: np.ndarray):
         a = np.ascontiguousarray(host_vector_layout, dtype=np.float64)
         check(lib().micmb_state_upload(self.handle, buffer, _f64(a)))

@@ -264,6 +264,10 @@ class Reference:
 _om = None
 
 
+# double exchange(double shard_sum, void* user): the job's sum of the shards' error sums
+EXCHANGE_FN = C.CFUNCTYPE(C.c_double, C.c_double, C.c_void_p)
+
+
 def _load_oracle():
     global _om
     if _om is None:
@@ -283,6 +287,8 @@ def _load_oracle():
         lib.om_adjoint_per_cell.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, _f64p, _f64p,
                                             C.c_double, _f64p, _f64p, _f64p, _f64p, _f64p, C.c_int, C.c_int]
         lib.om_replay_per_cell.argtypes = [C.c_void_p, C.c_void_p, C.c_int, _f64p, _f64p, _i32p, C.c_int, _f64p]
+        lib.om_solve_global.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, _f64p, _f64p, C.c_double,
+                                        _f64p, _i64p, C.c_int, _i32p, EXCHANGE_FN, C.c_void_p, C.c_int64]
         lib.om_set_correctly_rounded.argtypes = [C.c_void_p, C.c_int]
         lib.om_set_correctly_rounded.restype = None
         lib.om_math_eval.argtypes = [C.c_void_p, C.c_int, _f64p, _f64p, _f64p, C.c_int64]
@@ -388,6 +394,29 @@ class Restatement:
         stats = np.zeros((n, 10), np.int64)
         rc = self.lib.om_backward_euler_per_cell(self.handle, n, float(dt), _p(k), _p(self.atol_columns),
                                                  self.mech.relative_tolerance, _p(y), _p(stats, C.c_int64))
+        if rc:
+            raise RuntimeError(self.lib.om_last_error().decode())
+        return np.ascontiguousarray(y[:, self.species_columns]), stats
+
+    def solve_global(self, inputs, dt, k=None, shards=None, exchange=None, total_cells=0):
+        """Global step control (one step size for all cells), the error sum in
+        the fixed order a GPU reproduces.  shards: cell counts of consecutive
+        shards (default one); exchange(shard_sum) -> job sum makes the cells
+        this rank's shard of a job over total_cells.  (y_final [n,S] system
+        order, stats [10])."""
+        y = np.zeros_like(inputs["concentrations"])
+        y[:, self.species_columns] = inputs["concentrations"]
+        y = np.ascontiguousarray(y)
+        n = len(y)
+        k = self._k(inputs) if k is None else np.ascontiguousarray(k)
+        stats = np.zeros(10, np.int64)
+        sizes = [n] if shards is None else list(shards)
+        assert sum(sizes) == n
+        starts = np.ascontiguousarray(np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32))
+        cb = EXCHANGE_FN(lambda v, _u: float(exchange(v))) if exchange else EXCHANGE_FN()
+        rc = self.lib.om_solve_global(self.handle, C.byref(self.params), n, float(dt), _p(k), _p(self.atol_columns),
+                                      self.mech.relative_tolerance, _p(y), _p(stats, C.c_int64), len(sizes),
+                                      _p(starts, C.c_int32), cb, None, int(total_cells or n))
         if rc:
             raise RuntimeError(self.lib.om_last_error().decode())
         return np.ascontiguousarray(y[:, self.species_columns]), stats

@@ -1178,6 +1178,238 @@ int om_backward_euler_per_cell(const om_mech* m, int n, double dt, const double*
   return 0;
 }
 
+/* ---------------------------------------------------------------- */
+/* global step control (one step size for all cells), micm's          */
+/* AbstractRosenbrockSolver::Solve on a multi-cell State               */
+/* (rosenbrock.inl:12-304), with the error norm's sum over cells       */
+/* formed in a fixed order that a GPU reproduces: per cell in species  */
+/* order, per block of 256 cells a pairwise tree, per shard each of    */
+/* 256 lanes adds the blocks b = lane, lane + 256, ... in order and a  */
+/* tree joins the lanes, and the shards' sums are added in rank order. */
+/* micm itself adds all values with one accumulator, so the two agree  */
+/* to rounding (exactly for one cell).                                 */
+/* ---------------------------------------------------------------- */
+static double tree256(double* red)
+{
+  for (int w = 128; w > 0; w >>= 1)
+    for (int t = 0; t < w; ++t)
+      red[t] += red[t + w];
+  return red[0];
+}
+
+static double shard_error_sum(const double* cell_sum, int n)
+{
+  const int n_blk = (n + 255) / 256;
+  double* blk = xcalloc(n_blk > 0 ? n_blk : 1, sizeof(double));
+  double red[256];
+  for (int b = 0; b < n_blk; ++b)
+  {
+    for (int t = 0; t < 256; ++t)
+    {
+      const int c = b * 256 + t;
+      red[t] = c < n ? cell_sum[c] : 0.0;
+    }
+    blk[b] = tree256(red);
+  }
+  for (int t = 0; t < 256; ++t)
+  {
+    double acc = 0.0;
+    for (int b = t; b < n_blk; b += 256)
+      acc += blk[b];
+    red[t] = acc;
+  }
+  free(blk);
+  return tree256(red);
+}
+
+/* y [cell][column] in/out, k [cell][R]; stats_out [10] as one row of
+ * om_solve_per_cell's.  n_shards / shard_start: the cells split into shards
+ * (shard_start[0] = 0, shard_start[n_shards] = n), the job's sum is the
+ * shards' sums in shard order.  With `exchange` set, the n cells are this
+ * rank's shard only: exchange(this shard's sum, user) returns the job's sum,
+ * and total_cells counts every rank's cells. */
+int om_solve_global(const om_mech* m, const micmb_rosenbrock_params* p, int n, double dt, const double* k,
+                    const double* atol, double rtol, double* y, int64_t* stats_out, int n_shards,
+                    const int* shard_start, om_exchange_fn exchange, void* user, int64_t total_cells)
+{
+  const int S = m->S, ns = p->stages;
+  const size_t nS = (size_t)n * S;
+  double* F0 = xcalloc(nS + 1, sizeof(double));
+  double* Ynew = xcalloc(nS + 1, sizeof(double));
+  double* Yerr = xcalloc(nS + 1, sizeof(double));
+  double* K = xcalloc((size_t)ns * nS + 1, sizeof(double));
+  double* J = xcalloc((size_t)n * m->nnz + 1, sizeof(double));
+  double* cell_sum = xcalloc((size_t)n + 1, sizeof(double));
+  const double h_min = p->h_min == 0.0 ? 1.0e-15 * dt : p->h_min;
+  const double h_max = p->h_max == 0.0 ? dt : dmin(dt, p->h_max);
+  const double h_start = p->h_start == 0.0 ? 1.0e-6 * dt : dmin(h_max, p->h_start);
+  double H = dmin(dmax(h_min, fabs(h_start)), fabs(h_max));
+  double t = 0.0;
+  int reject_last = 0, reject_more = 0, state = MICMB_SOLVER_RUNNING;
+  int64_t fc = 0, ju = 0, nst = 0, acc = 0, rej = 0, dec = 0, sol = 0;
+  const double n_values = (double)(exchange ? total_cells : n) * (double)S;
+  while ((t - dt + p->round_off) <= 0 && state == MICMB_SOLVER_RUNNING)
+  {
+    if (nst > p->max_number_of_steps)
+    {
+      state = MICMB_SOLVER_CONVERGENCE_EXCEEDED_MAX_STEPS;
+      break;
+    }
+    if (((t + 0.1 * H) == t) || (H <= p->round_off))
+    {
+      state = MICMB_SOLVER_STEP_SIZE_TOO_SMALL;
+      break;
+    }
+    H = dmin(H, fabs(dt - t));
+    for (int c = 0; c < n; ++c)
+      forcing(m, k + (size_t)c * m->R, y + (size_t)c * S, F0 + (size_t)c * S);
+    fc++;
+    for (int c = 0; c < n; ++c)
+      neg_jacobian(m, k + (size_t)c * m->R, y + (size_t)c * S, J + (size_t)c * m->nnz);
+    ju++;
+    int accepted = 0;
+    while (!accepted)
+    {
+      const double alpha = 1.0 / (H * p->gamma[0]);
+      for (int c = 0; c < n; ++c)
+      {
+        double* Jc = J + (size_t)c * m->nnz;
+        for (int i = 0; i < S; ++i)
+          Jc[m->pos[(size_t)i * S + i]] += alpha;
+        decompose(m, Jc);
+      }
+      dec++;
+      for (int s = 0; s < ns; ++s)
+      {
+        const int sc = s * (s - 1) / 2;
+        for (int c = 0; c < n; ++c)
+        {
+          const double* Yc = y + (size_t)c * S;
+          double* Ks = K + ((size_t)s * n + c) * S;
+          double* Yn = Ynew + (size_t)c * S;
+          if (s == 0)
+            memcpy(Ks, F0 + (size_t)c * S, sizeof(double) * S);
+          else if (p->new_function_evaluation[s])
+          {
+            memcpy(Yn, Yc, sizeof(double) * S);
+            for (int j = 0; j < s; ++j)
+              for (int i = 0; i < S; ++i)
+                Yn[i] += p->a[sc + j] * K[((size_t)j * n + c) * S + i];
+            forcing(m, k + (size_t)c * m->R, Yn, Ks);
+          }
+          if (s + 1 < ns && !p->new_function_evaluation[s + 1])
+            memcpy(K + ((size_t)(s + 1) * n + c) * S, Ks, sizeof(double) * S);
+          for (int j = 0; j < s; ++j)
+          {
+            const double coh = p->c[sc + j] / H;
+            for (int i = 0; i < S; ++i)
+              Ks[i] += coh * K[((size_t)j * n + c) * S + i];
+          }
+          lu_solve(m, J + (size_t)c * m->nnz, Ks);
+        }
+        if (s > 0 && p->new_function_evaluation[s])
+          fc++;
+        sol++;
+      }
+      for (int c = 0; c < n; ++c)
+      {
+        const double* Yc = y + (size_t)c * S;
+        double* Yn = Ynew + (size_t)c * S;
+        double* Ye = Yerr + (size_t)c * S;
+        memcpy(Yn, Yc, sizeof(double) * S);
+        for (int s = 0; s < ns; ++s)
+          for (int i = 0; i < S; ++i)
+            Yn[i] += p->m[s] * K[((size_t)s * n + c) * S + i];
+        for (int i = 0; i < S; ++i)
+          Ye[i] = 0.0;
+        for (int s = 0; s < ns; ++s)
+          for (int i = 0; i < S; ++i)
+            Ye[i] += p->e[s] * K[((size_t)s * n + c) * S + i];
+        double sum = 0.0;
+        for (int i = 0; i < S; ++i)
+        {
+          const double ay = fabs(Yc[i]), an = fabs(Yn[i]);
+          const double ymax = ay > an ? ay : an;
+          const double q = Ye[i] / (atol[i] + rtol * ymax);
+          sum += q * q;
+        }
+        cell_sum[c] = sum;
+      }
+      double total = 0.0;
+      if (exchange)
+        total = exchange(shard_error_sum(cell_sum, n), user);
+      else
+        for (int r = 0; r < n_shards; ++r)
+          total += shard_error_sum(cell_sum + shard_start[r], shard_start[r + 1] - shard_start[r]);
+      const double error = dmax(sqrt(total / (n_values > 0.0 ? n_values : 1.0)), 1.0e-10);
+      const double fac = dmin(p->factor_max,
+                              dmax(p->factor_min, p->safety_factor / o_pow(m, error, 1 / p->estimator_of_local_order)));
+      double Hnew = H * fac;
+      nst++;
+      if (isnan(error))
+      {
+        state = MICMB_SOLVER_NAN_DETECTED;
+        break;
+      }
+      if (isinf(error))
+      {
+        state = MICMB_SOLVER_INF_DETECTED;
+        break;
+      }
+      if ((error < 1) || (H < h_min))
+      {
+        acc++;
+        t = t + H;
+        memcpy(y, Ynew, sizeof(double) * nS);
+        Hnew = dmax(h_min, dmin(Hnew, h_max));
+        if (reject_last)
+          Hnew = dmin(Hnew, H);
+        reject_last = 0;
+        reject_more = 0;
+        H = Hnew;
+        accepted = 1;
+      }
+      else
+      {
+        if (reject_more)
+          Hnew = H * p->rejection_factor_decrease;
+        reject_more = reject_last;
+        reject_last = 1;
+        H = Hnew;
+        if (acc >= 1)
+          rej++;
+        for (int c = 0; c < n; ++c)
+          neg_jacobian(m, k + (size_t)c * m->R, y + (size_t)c * S, J + (size_t)c * m->nnz);
+        ju++;
+      }
+    }
+  }
+  if (state == MICMB_SOLVER_RUNNING)
+    state = MICMB_SOLVER_CONVERGED;
+  for (size_t e = 0; e < nS; ++e)
+    y[e] = (y[e] < 0.0) ? 0.0 : y[e]; /* Solver::PostSolveClamp */
+  if (stats_out)
+  {
+    stats_out[0] = fc;
+    stats_out[1] = ju;
+    stats_out[2] = nst;
+    stats_out[3] = acc;
+    stats_out[4] = rej;
+    stats_out[5] = dec;
+    stats_out[6] = sol;
+    stats_out[7] = state;
+    memcpy(&stats_out[8], &t, sizeof(double));
+    stats_out[9] = 0;
+  }
+  free(F0);
+  free(Ynew);
+  free(Yerr);
+  free(K);
+  free(J);
+  free(cell_sum);
+  return 0;
+}
+
 /* Backward Euler on one n-cell State (micm's multi-cell semantics,
  * backward_euler.inl:10-186): one step size, and an attempt converges only
  * when every cell's test passes (IsConverged :188-246, a logical AND over

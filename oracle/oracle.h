@@ -64,6 +64,14 @@ int om_replay_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n
 /* Accepted step sizes of a per-cell solve from y0 [cell][S]. */
 /* Backward Euler (micm's backward_euler.inl, default parameters), a 1-cell
  * State per cell, one Solve(dt) each; y [cell][column] in/out, stats [cell][10]. */
+/* Global step control (one step size for all n cells) with the error sum in
+ * the fixed order a GPU reproduces (per cell, per 256-cell block tree, per
+ * shard, shards in order).  exchange != NULL: the cells are this rank's
+ * shard; exchange(shard sum, user) returns the job's sum over total_cells. */
+typedef double (*om_exchange_fn)(double shard_sum, void* user);
+int om_solve_global(const om_mech* m, const micmb_rosenbrock_params* p, int n, double dt, const double* k,
+                    const double* atol, double rtol, double* y, int64_t* stats_out, int n_shards,
+                    const int* shard_start, om_exchange_fn exchange, void* user, int64_t total_cells);
 /* 0 (default): exp, pow and log10 of the rate constants and the step-size
  * factor from the C library, as micm calls them; 1: correctly rounded (quad
  * precision).  om_math_eval evaluates exp (0), log10 (1) or pow (2)
