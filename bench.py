@@ -604,6 +604,7 @@ def main():
         pres = solver.solve(cfg["dt"], pstate, method="plain", step_control="per_cell")
         torch.cuda.synchronize()
         pt = time.perf_counter() - t0
+        (pt,) = max_over_ranks([pt], dist, "cuda")
         plain_gbs = solve_bytes(bytes_per_solve_unit(mech, solver, cfg["stages"]), pres.stats) / pt / 1e9
         plain = {"value": pc * world / pt, "unit": UNIT, "cells_per_gpu": pc, "ms_per_step": 1000 * pt,
                  "attempts_per_cell": pres.stats["number_of_steps"] / pc,
@@ -614,14 +615,29 @@ def main():
                                       "(launches and host synchronisation included)"}}
         # the same kernels with micm's CUDA-path semantics: one step size for
         # all cells from the error norm over all cells (a different step
-        # sequence, so not bit-comparable with the per-cell solves)
+        # sequence, so not bit-comparable with the per-cell solves); under
+        # torchrun the step size is the whole job's: one 8-byte all-gather of
+        # the ranks' error sums per attempt (NCCL, on the state's stream)
+        if dist:
+            def nccl_allgather(send, recv, w, stream_ptr):
+                with torch.cuda.stream(torch.cuda.ExternalStream(stream_ptr)):
+                    dist.all_gather_into_tensor(torch.as_tensor(_DeviceArray(recv, w), device="cuda"),
+                                                torch.as_tensor(_DeviceArray(send, 1), device="cuda"))
+                return 0
+            pstate.set_global_exchange(nccl_allgather, world, pc * world)
         pview.copy_(p0)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         gres = solver.solve(cfg["dt"], pstate, method="plain", step_control="global")
         torch.cuda.synchronize()
         gt = time.perf_counter() - t0
+        if dist:
+            pstate.set_global_exchange(None, 1, 0)
+            (gt,) = max_over_ranks([gt], dist, "cuda")
         plain["global_step_size"] = {"value": pc * world / gt, "unit": UNIT, "ms_per_step": 1000 * gt,
+                                     "step_size": "one for the whole job" + (f" ({world} ranks, NCCL all-gather "
+                                                                             "of the error sums per attempt)"
+                                                                             if dist else ""),
                                      "attempts": gres.stats["number_of_steps"], "accepted": gres.stats["accepted"],
                                      "converged": bool(gres.converged),
                                      "fused_over_this": value / (pc * world / gt)}
