@@ -167,6 +167,9 @@ typedef struct micmb_mechanism_info {
   int32_t lu_levels;
   int32_t forward_levels;
   int32_t backward_levels;
+  int32_t blocked_schedules;  /* 1: the register-blocked LU and solves are in use (they
+                                 reproduced the serial schedules bit for bit when built) */
+  int32_t lu_blocked_ops;     /* shared-operand steps of the blocked LU */
 } micmb_mechanism_info;
 
 typedef struct micmb_mechanism micmb_mechanism;

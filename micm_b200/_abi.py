@@ -72,7 +72,7 @@ class MechanismInfo(C.Structure):
     _fields_ = [(n, C.c_int32) for n in (
         "n_species", "n_reactions", "n_custom_params", "jacobian_nnz", "jacobian_nnz_unfilled",
         "lu_updates", "lu_lower", "n_jacobian_terms", "n_forcing_terms", "n_jacobian_infos",
-        "lu_levels", "forward_levels", "backward_levels")]
+        "lu_levels", "forward_levels", "backward_levels", "blocked_schedules", "lu_blocked_ops")]
 
     def as_dict(self) -> Dict[str, int]:
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -316,7 +316,7 @@ namespace micmb
         // ---- the accepted step's factor, stages and stage inputs ----
         const double alpha = 1.0 / (H * P.gamma0);
         jacobian_rates<1>(M, kk, y, scr, 0);
-        lu_decompose_gathered(M, M.lu_s, M.diag_row_of, scr, alpha, LU, inv);  // -J + alpha I, then LU
+        thread_lu_gathered(M, scr, alpha, LU, inv);  // -J + alpha I, then LU
         if (A.ckpt_k)
         {
           // stages stored by the forward pass; stage inputs rebuilt from them
@@ -380,8 +380,7 @@ namespace micmb
                 v += coh[j] * K(j)[i];
               Ks[i] = v;
             }
-            solve_lower<1>(M.fwd_s, LU, Ks, 0);
-            solve_upper<1>(M.bwd_s, LU, Ks, 0);
+            thread_solve(M, LU, Ks);
           }
         }
         if (n == A.n_ckpt[cell] - 1)

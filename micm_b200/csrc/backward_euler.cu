@@ -76,11 +76,10 @@ namespace micmb
       forcing_gather<1>(M, scr, F, 0);
       jacobian_rates<1>(M, kk, Y, scr, 0);
       // J = -J(y) in micm's term order, then + 1/H on the diagonal (AddToDiagonal), then the LU
-      lu_decompose_gathered(M, M.lu_s, M.diag_row_of, scr, 1.0 / H, LU, inv);
+      thread_lu_gathered(M, scr, 1.0 / H, LU, inv);
       for (int32_t i = 0; i < S; ++i)
         F[i] = F[i] - (Y[i] - Yn[i]) / H;
-      solve_lower<1>(M.fwd_s, LU, F, 0);
-      solve_upper<1>(M.bwd_s, LU, F, 0);
+      thread_solve(M, LU, F);
       for (int32_t i = 0; i < S; ++i)
       {
         const double v = Y[i] + F[i];

@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <sstream>
@@ -153,6 +154,34 @@ namespace micmb
       return d;
     }
 
+    struct BlockedOffsets
+    {
+      size_t bl, tg, ax, op;
+      int32_t n_blocks;
+    };
+
+    BlockedOffsets AddBlocked(Packer& pk, const BlockedSchedule& b)
+    {
+      BlockedOffsets o;
+      o.bl = pk.add(b.block);
+      o.tg = pk.add(b.target);
+      o.ax = pk.add(b.aux);
+      o.op = pk.add(b.op);
+      o.n_blocks = b.n_blocks;
+      return o;
+    }
+
+    DevBlocked ResolveBlocked(const char* base, const BlockedOffsets& o)
+    {
+      DevBlocked d;
+      d.n_blocks = o.n_blocks;
+      d.block = reinterpret_cast<const int4*>(base + o.bl);
+      d.target = reinterpret_cast<const int4*>(base + o.tg);
+      d.aux = reinterpret_cast<const int4*>(base + o.ax);
+      d.op = reinterpret_cast<const uint4*>(base + o.op);
+      return d;
+    }
+
     DevSchedule Resolve(const char* base, const SchedOffsets& o)
     {
       DevSchedule d;
@@ -200,6 +229,13 @@ namespace micmb
                          bws = AddSchedule(pk, m.bwd_serial), fwts = AddSchedule(pk, m.fwd_t_serial),
                          bwts = AddSchedule(pk, m.bwd_t_serial);
       const size_t o_rd = pk.add(m.rate_desc), o_drd = pk.add(m.drate_desc);
+      BlockedOffsets blu{}, bfw{}, bbw{};
+      if (m.has_blocked)
+      {
+        blu = AddBlocked(pk, m.lu_blocked);
+        bfw = AddBlocked(pk, m.fwd_blocked);
+        bbw = AddBlocked(pk, m.bwd_blocked);
+      }
       WarpOffsets wl{}, wf{}, wb{}, wft{}, wbt{}, wfo{}, wj{};
       if (m.has_warp_tables)
       {
@@ -268,6 +304,13 @@ namespace micmb
       d.bwd_s = Resolve(b, bws);
       d.fwd_t_s = Resolve(b, fwts);
       d.bwd_t_s = Resolve(b, bwts);
+      d.has_blocked = (m.has_blocked && !std::getenv("MICMB_SERIAL_SCHEDULES")) ? 1 : 0;
+      if (m.has_blocked)
+      {
+        d.lu_b = ResolveBlocked(b, blu);
+        d.fwd_b = ResolveBlocked(b, bfw);
+        d.bwd_b = ResolveBlocked(b, bbw);
+      }
       s.diag_row_of = d.diag_row_of;
       d.has_warp = m.has_warp_tables ? 1 : 0;
       d.scratch_zero = m.scratch_zero;
@@ -363,6 +406,8 @@ extern "C"
       out->lu_levels = m.lu.n_levels();
       out->forward_levels = m.fwd.n_levels();
       out->backward_levels = m.bwd.n_levels();
+      out->blocked_schedules = m.has_blocked ? 1 : 0;
+      out->lu_blocked_ops = (int32_t)(m.lu_blocked.op.size() / 4);
     });
   }
 

@@ -34,6 +34,16 @@ namespace micmb
     const int32_t* tb;
   };
 
+  // register-blocked serial schedule (mechanism.hpp BlockedSchedule)
+  struct DevBlocked
+  {
+    int32_t n_blocks;
+    const int4* block;   // {first op, n ops, n slots | kind << 4 | (diag slot + 1) << 8, pivot row}
+    const int4* target;  // slot targets (-1 unused)
+    const int4* aux;     // backward solve: diagonal positions of the slot rows
+    const uint4* op;     // {shared index, slot mask, slot 0 | slot 1 << 16, slot 2 | slot 3 << 16}
+  };
+
   // lane-interleaved level schedule (mechanism.hpp WarpTable)
   struct DevWarpTable
   {
@@ -76,6 +86,8 @@ namespace micmb
     const int32_t* diag_row_of;  // [nnz] row i if the position holds a_ii, else -1
     DevSchedule lu, fwd, bwd, fwd_t, bwd_t;
     DevSchedule lu_s, fwd_s, bwd_s, fwd_t_s, bwd_t_s;  // serial forms (one thread per cell)
+    int32_t has_blocked;                                // register-blocked serial forms present
+    DevBlocked lu_b, fwd_b, bwd_b;
     // warp-interleaved tables (fused kernel); dummy slots: LU[nnz], x[S], scratch[scratch_zero]
     int32_t has_warp;
     int32_t scratch_zero;
@@ -346,6 +358,147 @@ namespace micmb
     }
   }
 
+  // ---------------------------------------------------------------------
+  // register-blocked serial LU and solves (one thread per cell): up to four
+  // entries of a block in registers; each op loads its shared operand once
+  // and updates the entries that use it.  Every entry receives its terms in
+  // the serial schedule's order, so results are bit-identical to
+  // lu_decompose / lu_decompose_gathered / solve_lower / solve_upper.
+  // ---------------------------------------------------------------------
+  __device__ __forceinline__ uint32_t blk_lo(uint32_t v)
+  {
+    return v & 0xFFFFu;
+  }
+  __device__ __forceinline__ uint32_t blk_hi(uint32_t v)
+  {
+    return v >> 16;
+  }
+
+  // GATHER: each entry starts from its -J gather (+ alpha on the diagonal),
+  // as lu_decompose_gathered; otherwise from the stored value, as lu_decompose.
+  template<bool GATHER, class DV, class AV, class IV>
+  __device__ __forceinline__ void lu_blocked(const DevMech& M, const DevBlocked& T, DV drate, double alpha, AV A,
+                                             IV inv)
+  {
+    auto init = [&](int32_t e) -> double {
+      if constexpr (GATHER)
+      {
+        double v = 0.0;
+        for (int32_t t = M.j_start[e]; t < M.j_start[e + 1]; ++t)
+          v += M.j_coef[t] * drate[M.j_info[t]];
+        if (M.diag_row_of[e] >= 0)
+          v += alpha;
+        return v;
+      }
+      else
+        return A[e];
+    };
+    for (int32_t k = 0; k < T.n_blocks; ++k)
+    {
+      const int4 bk = __ldg(T.block + k);
+      const int4 tg = __ldg(T.target + k);
+      const int32_t n = bk.z & 0xF, kind = (bk.z >> 4) & 0xF, diag = (bk.z >> 8) - 1;
+      double a0 = init(tg.x), a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      if (n > 1)
+        a1 = init(tg.y);
+      if (n > 2)
+        a2 = init(tg.z);
+      if (n > 3)
+        a3 = init(tg.w);
+      for (int32_t o = bk.x; o < bk.x + bk.y; ++o)
+      {
+        const uint4 op = __ldg(T.op + o);
+        const double sh = A[op.x];
+        if (op.y & 1u)
+          a0 -= sh * A[blk_lo(op.z)];
+        if (op.y & 2u)
+          a1 -= sh * A[blk_hi(op.z)];
+        if (op.y & 4u)
+          a2 -= sh * A[blk_lo(op.w)];
+        if (op.y & 8u)
+          a3 -= sh * A[blk_hi(op.w)];
+      }
+      if (kind == 1)  // L column: times 1/a_kk of the pivot
+      {
+        const double iv = inv[bk.w];
+        a0 *= iv;
+        a1 *= iv;
+        a2 *= iv;
+        a3 *= iv;
+      }
+      A[tg.x] = a0;
+      if (n > 1)
+        A[tg.y] = a1;
+      if (n > 2)
+        A[tg.z] = a2;
+      if (n > 3)
+        A[tg.w] = a3;
+      if (diag >= 0)
+        inv[bk.w] = 1.0 / (diag == 0 ? a0 : (diag == 1 ? a1 : (diag == 2 ? a2 : a3)));
+    }
+  }
+
+  // UPPER: U x = b with the division by the diagonal (solve_upper); else the
+  // unit-lower L y = b (solve_lower).  In place.
+  template<bool UPPER, class AV, class XV>
+  __device__ __forceinline__ void solve_blocked(const DevBlocked& T, AV A, XV x)
+  {
+    for (int32_t k = 0; k < T.n_blocks; ++k)
+    {
+      const int4 bk = __ldg(T.block + k);
+      const int4 tg = __ldg(T.target + k);
+      const int32_t n = bk.z & 0xF;
+      double a0 = x[tg.x], a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      if (n > 1)
+        a1 = x[tg.y];
+      if (n > 2)
+        a2 = x[tg.z];
+      if (n > 3)
+        a3 = x[tg.w];
+      for (int32_t o = bk.x; o < bk.x + bk.y; ++o)
+      {
+        const uint4 op = __ldg(T.op + o);
+        const double sh = x[op.x];
+        if (op.y & 1u)
+          a0 -= A[blk_lo(op.z)] * sh;
+        if (op.y & 2u)
+          a1 -= A[blk_hi(op.z)] * sh;
+        if (op.y & 4u)
+          a2 -= A[blk_lo(op.w)] * sh;
+        if (op.y & 8u)
+          a3 -= A[blk_hi(op.w)] * sh;
+      }
+      if constexpr (UPPER)
+      {
+        const int4 ax = __ldg(T.aux + k);
+        x[tg.x] = a0 / A[ax.x];
+        if (n > 1)
+          x[tg.y] = a1 / A[ax.y];
+        if (n > 2)
+          x[tg.z] = a2 / A[ax.z];
+        if (n > 3)
+          x[tg.w] = a3 / A[ax.w];
+      }
+      else
+      {
+        x[tg.x] = a0;
+        if (n > 1)
+          x[tg.y] = a1;
+        if (n > 2)
+          x[tg.z] = a2;
+        if (n > 3)
+          x[tg.w] = a3;
+      }
+    }
+  }
+
+  // The one-thread-per-cell LU and solves: blocked when the mechanism has
+  // the blocked forms, else the serial schedules.
+  template<class DV, class AV, class IV>
+  __device__ __forceinline__ void thread_lu_gathered(const DevMech& M, DV drate, double alpha, AV A, IV inv);
+  template<class AV, class XV>
+  __device__ __forceinline__ void thread_solve(const DevMech& M, AV A, XV x);
+
   // L y = b (unit diagonal), in place
   template<int NL, class AV, class XV>
   __device__ __forceinline__ void solve_lower(const DevSchedule& sch, AV A, XV x, int lane)
@@ -382,6 +535,40 @@ namespace micmb
         x[i] = aux >= 0 ? v / A[aux] : v;
       }
       lane_sync<NL>();
+    }
+  }
+
+  template<class DV, class AV, class IV>
+  __device__ __forceinline__ void thread_lu_gathered(const DevMech& M, DV drate, double alpha, AV A, IV inv)
+  {
+    if (M.has_blocked)
+      lu_blocked<true>(M, M.lu_b, drate, alpha, A, inv);
+    else
+      lu_decompose_gathered(M, M.lu_s, M.diag_row_of, drate, alpha, A, inv);
+  }
+
+  template<class AV, class IV>
+  __device__ __forceinline__ void thread_lu(const DevMech& M, AV A, IV inv)
+  {
+    if (M.has_blocked)
+      lu_blocked<false>(M, M.lu_b, A, 0.0, A, inv);
+    else
+      lu_decompose<1>(M.lu_s, M.diag_row_of, A, inv, 0);
+  }
+
+  // x = (LU)^-1 x: forward then backward substitution
+  template<class AV, class XV>
+  __device__ __forceinline__ void thread_solve(const DevMech& M, AV A, XV x)
+  {
+    if (M.has_blocked)
+    {
+      solve_blocked<false>(M.fwd_b, A, x);
+      solve_blocked<true>(M.bwd_b, A, x);
+    }
+    else
+    {
+      solve_lower<1>(M.fwd_s, A, x, 0);
+      solve_upper<1>(M.bwd_s, A, x, 0);
     }
   }
 

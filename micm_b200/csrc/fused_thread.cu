@@ -166,7 +166,7 @@ namespace micmb
         const double H = c.H;
         const double alpha = 1.0 / (H * P.gamma0);
         jacobian_rates<1>(M, kk, Y, scr, 0);
-        lu_decompose_gathered(M, M.lu_s, M.diag_row_of, scr, alpha, LU, inv);  // -J + alpha I, then LU
+        thread_lu_gathered(M, scr, alpha, LU, inv);  // -J + alpha I, then LU
         bool fc_is_src = false;
         for (int32_t st = 0; st < P.stages; ++st)
         {
@@ -195,8 +195,7 @@ namespace micmb
               v += coh[j] * Kv(j)[i];
             Ks[i] = v;
           }
-          solve_lower<1>(M.fwd_s, LU, Ks, 0);
-          solve_upper<1>(M.bwd_s, LU, Ks, 0);
+          thread_solve(M, LU, Ks);
         }
         // Ynew, and the error norm summed in species order (micm's order)
         double sum = 0.0;

@@ -2,6 +2,8 @@
 #include "mechanism.hpp"
 
 #include <algorithm>
+#include <array>
+#include <map>
 #include <cstring>
 #include <cmath>
 #include <numeric>
@@ -419,6 +421,292 @@ namespace micmb
     uint64_t FnvVec(uint64_t h, const std::vector<T>& v)
     {
       return v.empty() ? h : Fnv(h, v.data(), v.size() * sizeof(T));
+    }
+
+    // ------------------------------------------------------------------
+    // register-blocked serial schedules (mechanism.hpp BlockedSchedule)
+    // ------------------------------------------------------------------
+    using PosMap = std::map<std::pair<int32_t, int32_t>, int32_t>;
+
+    // One block: slots' targets and, per slot, its terms as (shared index,
+    // per-slot operand) in increasing shared-index order.
+    void EmitBlock(BlockedSchedule& b, int32_t kind, int32_t diag_slot, int32_t pivot,
+                   const std::vector<int32_t>& targets, const std::vector<int32_t>& aux,
+                   const std::vector<std::vector<std::pair<int32_t, int32_t>>>& terms,
+                   const std::vector<std::vector<int32_t>>& order_keys)
+    {
+      // union of the slots' terms, ordered by each slot's own term order (the
+      // order keys increase along every slot's list, so one merged order
+      // serves all slots)
+      std::map<int32_t, std::pair<int32_t, std::array<int32_t, kBlockSlots>>> ops;  // key -> shared, slot operands
+      for (size_t sl = 0; sl < targets.size(); ++sl)
+        for (size_t t = 0; t < terms[sl].size(); ++t)
+        {
+          auto f = ops.find(order_keys[sl][t]);
+          if (f == ops.end())
+          {
+            std::array<int32_t, kBlockSlots> none;
+            none.fill(-1);
+            f = ops.emplace(order_keys[sl][t], std::make_pair(terms[sl][t].first, none)).first;
+          }
+          if (f->second.first != terms[sl][t].first)
+            throw std::runtime_error("blocked schedule: slots disagree on a shared operand");
+          f->second.second[sl] = terms[sl][t].second;
+        }
+      const int32_t first_op = (int32_t)(b.op.size() / 4);
+      for (const auto& kv : ops)
+      {
+        int32_t mask = 0;
+        uint32_t p[kBlockSlots] = { 0, 0, 0, 0 };
+        for (int32_t sl = 0; sl < kBlockSlots; ++sl)
+          if (kv.second.second[sl] >= 0)
+          {
+            mask |= 1 << sl;
+            p[sl] = (uint32_t)kv.second.second[sl];
+          }
+        b.op.push_back(kv.second.first);
+        b.op.push_back(mask);
+        b.op.push_back((int32_t)(p[0] | (p[1] << 16)));
+        b.op.push_back((int32_t)(p[2] | (p[3] << 16)));
+      }
+      b.block.push_back(first_op);
+      b.block.push_back((int32_t)ops.size());
+      b.block.push_back((int32_t)targets.size() | (kind << 4) | ((diag_slot + 1) << 8));
+      b.block.push_back(pivot);
+      for (int32_t sl = 0; sl < kBlockSlots; ++sl)
+      {
+        b.target.push_back(sl < (int32_t)targets.size() ? targets[sl] : -1);
+        b.aux.push_back(sl < (int32_t)aux.size() ? aux[sl] : -1);
+      }
+      ++b.n_blocks;
+    }
+
+    // The LU of step 8 (Crout entries, pivot by pivot: the U row, then the L
+    // column) in blocks of up to kBlockSlots entries of one row or column.
+    BlockedSchedule BlockLu(int32_t S, const std::vector<std::set<int32_t>>& row_cols,
+                            const std::vector<std::set<int32_t>>& col_rows, const PosMap& position)
+    {
+      auto pos = [&](int32_t r, int32_t c) { return position.at({ r, c }); };
+      BlockedSchedule b;
+      for (int32_t mn = 0; mn < S; ++mn)
+      {
+        std::vector<int32_t> u_cols, l_rows;
+        for (int32_t k : row_cols[mn])
+          if (k >= mn)
+            u_cols.push_back(k);
+        for (int32_t j : col_rows[mn])
+          if (j > mn)
+            l_rows.push_back(j);
+        for (int32_t kind : { kBlockU, kBlockL })
+        {
+          const std::vector<int32_t>& list = kind == kBlockU ? u_cols : l_rows;
+          for (size_t c0 = 0; c0 < list.size(); c0 += kBlockSlots)
+          {
+            std::vector<int32_t> targets, none;
+            std::vector<std::vector<std::pair<int32_t, int32_t>>> terms;
+            std::vector<std::vector<int32_t>> keys;
+            int32_t diag_slot = -1;
+            for (size_t q = c0; q < std::min(list.size(), c0 + kBlockSlots); ++q)
+            {
+              const int32_t j = kind == kBlockU ? mn : list[q];
+              const int32_t k = kind == kBlockU ? list[q] : mn;
+              if (j == k)
+                diag_slot = (int32_t)targets.size();
+              targets.push_back(pos(j, k));
+              terms.emplace_back();
+              keys.emplace_back();
+              const int32_t lim = std::min(j, k);
+              for (int32_t i : row_cols[j])
+              {
+                if (i >= lim)
+                  break;
+                auto f = position.find({ i, k });
+                if (f == position.end())
+                  continue;
+                // term a_ji * a_ik: U row shares a_{mn,i}, L column shares a_{i,mn}
+                if (kind == kBlockU)
+                  terms.back().push_back({ pos(j, i), f->second });
+                else
+                  terms.back().push_back({ f->second, pos(j, i) });
+                keys.back().push_back(i);
+              }
+            }
+            EmitBlock(b, kind, diag_slot, mn, targets, none, terms, keys);
+          }
+        }
+      }
+      return b;
+    }
+
+    // A triangular solve in blocks of up to kBlockSlots rows of one
+    // dependency level (rows of a level do not read each other).  forward:
+    // rows ascending, terms j < i; backward: rows descending, terms j > i,
+    // then the division by the diagonal.
+    BlockedSchedule BlockSolve(int32_t S, const std::vector<std::set<int32_t>>& row_cols, const PosMap& position,
+                               bool forward)
+    {
+      auto pos = [&](int32_t r, int32_t c) { return position.at({ r, c }); };
+      std::vector<int32_t> level(S, 0);
+      int32_t max_level = 0;
+      for (int32_t v = 0; v < S; ++v)
+      {
+        const int32_t i = forward ? v : S - 1 - v;
+        int32_t l = 0;
+        for (int32_t j : row_cols[i])
+          if (forward ? j < i : j > i)
+            l = std::max(l, level[j] + 1);
+        level[i] = l;
+        max_level = std::max(max_level, l);
+      }
+      BlockedSchedule b;
+      for (int32_t l = 0; l <= max_level; ++l)
+      {
+        std::vector<int32_t> rows;
+        for (int32_t v = 0; v < S; ++v)
+        {
+          const int32_t i = forward ? v : S - 1 - v;
+          if (level[i] == l)
+            rows.push_back(i);
+        }
+        for (size_t c0 = 0; c0 < rows.size(); c0 += kBlockSlots)
+        {
+          std::vector<int32_t> targets, aux;
+          std::vector<std::vector<std::pair<int32_t, int32_t>>> terms;
+          std::vector<std::vector<int32_t>> keys;
+          for (size_t q = c0; q < std::min(rows.size(), c0 + kBlockSlots); ++q)
+          {
+            const int32_t i = rows[q];
+            targets.push_back(i);
+            aux.push_back(forward ? -1 : pos(i, i));
+            terms.emplace_back();
+            keys.emplace_back();
+            for (int32_t j : row_cols[i])
+              if (forward ? j < i : j > i)
+              {
+                terms.back().push_back({ j, pos(i, j) });
+                keys.back().push_back(j);
+              }
+          }
+          EmitBlock(b, kBlockSolve, -1, -1, targets, aux, terms, keys);
+        }
+      }
+      return b;
+    }
+
+    // Host check that the blocked forms give the serial forms' bits on random
+    // values (the same IEEE operations in the same order per entry).
+    bool BlockedMatchesSerial(const CompiledMechanism& m)
+    {
+      const int32_t S = m.S, nnz = m.nnz;
+      std::vector<double> A0(nnz), x0(S);
+      uint64_t st = 0x9E3779B97F4A7C15ull;
+      auto rnd = [&]() {
+        st ^= st << 13;
+        st ^= st >> 7;
+        st ^= st << 17;
+        return ((double)(st >> 11) / 9007199254740992.0) * 2.0 - 1.0;
+      };
+      for (auto& v : A0)
+        v = rnd();
+      for (int32_t i = 0; i < S; ++i)
+        A0[m.diag_pos[i]] = 4.0 + (double)S + rnd();
+      for (auto& v : x0)
+        v = rnd();
+      std::vector<int32_t> diag_row(nnz, -1);
+      for (int32_t i = 0; i < S; ++i)
+        diag_row[m.diag_pos[i]] = i;
+      // serial LU (lu_decompose with one lane)
+      std::vector<double> A = A0, inv(S, 0.0);
+      const LevelSchedule& ls = m.lu_serial;
+      for (size_t it = 0; it < ls.item_target.size(); ++it)
+      {
+        const int32_t e = ls.item_target[it];
+        double v = A[e];
+        for (int32_t t = ls.term_start[it]; t < ls.term_start[it + 1]; ++t)
+          v -= A[ls.term_a[t]] * A[ls.term_b[t]];
+        const int32_t aux = ls.item_aux[it];
+        if (aux >= 0)
+          v *= inv[diag_row[aux]];
+        A[e] = v;
+        if (aux != -2 && diag_row[e] >= 0)
+          inv[diag_row[e]] = 1.0 / v;
+      }
+      // blocked LU
+      std::vector<double> B = A0, binv(S, 0.0);
+      const BlockedSchedule& bl = m.lu_blocked;
+      for (int32_t k = 0; k < bl.n_blocks; ++k)
+      {
+        const int32_t* blk = &bl.block[4 * k];
+        const int32_t n = blk[2] & 0xF, kind = (blk[2] >> 4) & 0xF, diag = (blk[2] >> 8) - 1;
+        double acc[kBlockSlots] = { 0, 0, 0, 0 };
+        for (int32_t sl = 0; sl < n; ++sl)
+          acc[sl] = B[bl.target[4 * k + sl]];
+        for (int32_t o = blk[0]; o < blk[0] + blk[1]; ++o)
+        {
+          const int32_t* op = &bl.op[4 * o];
+          const double sh = B[op[0]];
+          const uint32_t p01 = (uint32_t)op[2], p23 = (uint32_t)op[3];
+          const uint32_t p[4] = { p01 & 0xFFFFu, p01 >> 16, p23 & 0xFFFFu, p23 >> 16 };
+          for (int32_t sl = 0; sl < kBlockSlots; ++sl)
+            if (op[1] & (1 << sl))
+              acc[sl] -= (kind == kBlockU ? sh * B[p[sl]] : B[p[sl]] * sh);
+        }
+        for (int32_t sl = 0; sl < n; ++sl)
+        {
+          double v = acc[sl];
+          if (kind == kBlockL)
+            v *= binv[blk[3]];
+          B[bl.target[4 * k + sl]] = v;
+          if (sl == diag)
+            binv[blk[3]] = 1.0 / v;
+        }
+      }
+      for (int32_t e = 0; e < nnz; ++e)
+        if (std::memcmp(&A[e], &B[e], sizeof(double)) != 0)
+          return false;
+      // solves on the factor
+      for (int fw = 1; fw >= 0; --fw)
+      {
+        const LevelSchedule& ss = fw ? m.fwd_serial : m.bwd_serial;
+        const BlockedSchedule& bs = fw ? m.fwd_blocked : m.bwd_blocked;
+        std::vector<double> x = x0, y = x0;
+        for (size_t it = 0; it < ss.item_target.size(); ++it)
+        {
+          const int32_t i = ss.item_target[it];
+          double v = x[i];
+          for (int32_t t = ss.term_start[it]; t < ss.term_start[it + 1]; ++t)
+            v -= A[ss.term_a[t]] * x[ss.term_b[t]];
+          const int32_t aux = ss.item_aux[it];
+          x[i] = aux >= 0 ? v / A[aux] : v;
+        }
+        for (int32_t k = 0; k < bs.n_blocks; ++k)
+        {
+          const int32_t* blk = &bs.block[4 * k];
+          const int32_t n = blk[2] & 0xF;
+          double acc[kBlockSlots] = { 0, 0, 0, 0 };
+          for (int32_t sl = 0; sl < n; ++sl)
+            acc[sl] = y[bs.target[4 * k + sl]];
+          for (int32_t o = blk[0]; o < blk[0] + blk[1]; ++o)
+          {
+            const int32_t* op = &bs.op[4 * o];
+            const double sh = y[op[0]];
+            const uint32_t p01 = (uint32_t)op[2], p23 = (uint32_t)op[3];
+            const uint32_t p[4] = { p01 & 0xFFFFu, p01 >> 16, p23 & 0xFFFFu, p23 >> 16 };
+            for (int32_t sl = 0; sl < kBlockSlots; ++sl)
+              if (op[1] & (1 << sl))
+                acc[sl] -= A[p[sl]] * sh;
+          }
+          for (int32_t sl = 0; sl < n; ++sl)
+          {
+            const int32_t aux = bs.aux[4 * k + sl];
+            y[bs.target[4 * k + sl]] = aux >= 0 ? acc[sl] / A[aux] : acc[sl];
+          }
+        }
+        for (int32_t i = 0; i < S; ++i)
+          if (std::memcmp(&x[i], &y[i], sizeof(double)) != 0)
+            return false;
+      }
+      return true;
     }
   }  // namespace
 
@@ -858,6 +1146,18 @@ namespace micmb
       }
       m.bwd_t = Schedule(bt);
       m.bwd_t_serial = SerialSchedule(bt);
+    }
+
+    // 9b. register-blocked serial forms (16-bit slot operands), kept only when
+    //     they reproduce the serial forms bit for bit
+    if (m.nnz <= 0xFFFF && S <= 0xFFFF)
+    {
+      m.lu_blocked = BlockLu(S, row_cols, col_rows, m.position);
+      m.fwd_blocked = BlockSolve(S, row_cols, m.position, true);
+      m.bwd_blocked = BlockSolve(S, row_cols, m.position, false);
+      m.has_blocked = BlockedMatchesSerial(m);
+      if (!m.has_blocked)
+        m.lu_blocked = m.fwd_blocked = m.bwd_blocked = BlockedSchedule{};
     }
 
     // 10. warp-interleaved tables for the fused kernel (16-bit operand positions)

@@ -101,6 +101,27 @@ namespace micmb
     StreamPhase forcing, jacobian, lu, fwd, bwd, fwd_t, bwd_t;
   };
 
+  // Register-blocked serial forms for one thread per cell.  Items that share
+  // an operand are grouped in blocks of up to kBlockSlots entries held in
+  // registers; each op of a block loads the shared operand once and updates
+  // the accumulators of the entries that use it, in increasing order of the
+  // shared index, so every entry's terms come in the serial schedule's order
+  // and every result is bit-identical to it.
+  //   LU:     the U-row entries of one pivot row (shared a_{mn,i}) or the
+  //           L-column entries of one pivot column (shared a_{i,mn}).
+  //   solves: up to kBlockSlots rows of one dependency level (shared x_j).
+  // block[4b..4b+3] = {first op, n ops, n slots | kind << 4 | (diag slot + 1) << 8, pivot row}
+  // target[4b + s] = the entry (LU position or vector row) of slot s, -1 if unused
+  // aux[4b + s]    = backward solve: position of the slot row's diagonal
+  // op[4o..4o+3]   = {shared index, slot mask, slot 0 | slot 1 << 16, slot 2 | slot 3 << 16}
+  constexpr int32_t kBlockSlots = 4;
+  constexpr int32_t kBlockU = 0, kBlockL = 1, kBlockSolve = 2;
+  struct BlockedSchedule
+  {
+    int32_t n_blocks = 0;
+    std::vector<int32_t> block, target, aux, op;
+  };
+
   struct RateDef
   {
     int32_t kind = 0;
@@ -152,6 +173,10 @@ namespace micmb
     // the same LU and solves as single-level lists in visiting order, every
     // item whole (no partial sums): the order one thread per cell runs them
     LevelSchedule lu_serial, fwd_serial, bwd_serial, fwd_t_serial, bwd_t_serial;
+    // register-blocked forms of lu_serial, fwd_serial, bwd_serial (empty
+    // unless every position fits 16 bits and the host check passed)
+    bool has_blocked = false;
+    BlockedSchedule lu_blocked, fwd_blocked, bwd_blocked;
 
     // warp-interleaved forms for the fused kernel (empty when the mechanism
     // exceeds 16-bit positions); dummy operands: LU slot nnz, vector slot S,

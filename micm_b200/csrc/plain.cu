@@ -149,7 +149,7 @@ namespace micmb
       const int32_t L = a.L;
       Strided J{ a.jac + cell_base(c, L, M.nnz), L };
       Strided inv{ a.inv + cell_base(c, L, M.S), L };
-      lu_decompose<1>(M.lu_s, M.diag_row_of, J, inv, 0);
+      thread_lu(M, J, inv);
     }
 
     // Ynew = Y + sum_j a_sj K_j ; Fcur = f(Ynew)
@@ -201,8 +201,7 @@ namespace micmb
         Ks[i] = v;
       }
       Strided J{ a.jac + cell_base(c, L, M.nnz), L };
-      solve_lower<1>(M.fwd_s, J, Ks, 0);
-      solve_upper<1>(M.bwd_s, J, Ks, 0);
+      thread_solve(M, J, Ks);
     }
 
     // Ynew = Y + sum m_s K_s ; Yerr = sum e_s K_s ; the cell's sum of scaled
@@ -674,7 +673,7 @@ namespace micmb
       const int32_t L = a.L;
       Strided J{ a.jac + cell_base(c, L, M.nnz), L };
       Strided inv{ a.inv + cell_base(c, L, M.S), L };
-      lu_decompose<1>(M.lu_s, M.diag_row_of, J, inv, 0);
+      thread_lu(M, J, inv);
     }
 
     __global__ void k_linear_solve_all(DevMech M, PlainArgs a)
@@ -685,8 +684,7 @@ namespace micmb
       const int32_t L = a.L;
       Strided J{ a.jac + cell_base(c, L, M.nnz), L };
       Strided x{ a.f0 + cell_base(c, L, M.S), L };
-      solve_lower<1>(M.fwd_s, J, x, 0);
-      solve_upper<1>(M.bwd_s, J, x, 0);
+      thread_solve(M, J, x);
     }
 
     // errors are in f0, y in variables, ynew in the ynew buffer

@@ -72,3 +72,17 @@ def test_invalid_mechanism_rejected():
     m.reactions[0].reactants = [7]
     with pytest.raises(MicmbError):
         CompiledMechanism(m)
+
+
+def test_register_blocked_schedules_are_kept_for_the_benchmark_mechanisms():
+    """The compiler keeps the register-blocked LU and solves only when they
+    reproduce the serial schedules bit for bit on random values (a host check
+    at build time); every benchmark mechanism passes it."""
+    from micm_b200 import micm_bench, synthetic
+    from micm_b200.solver import CompiledMechanism
+    mechs = [synthetic.CONFIGS[n]["mech"]() for n in ("readme", "c210", "c60_adjoint", "c600")]
+    mechs += [micm_bench.mechanism(n) for n in ("ts1", "chapman")]
+    for m in mechs:
+        info = CompiledMechanism(m).info
+        assert info["blocked_schedules"] == 1
+        assert info["lu_blocked_ops"] <= info["lu_updates"]

@@ -181,3 +181,30 @@ def test_uneven_1m_workload_sample_against_micm(cuda_device):
                        fused_config=dict(variant=2, lu_in_shared=0))
     _close(y, y_ref)
     assert np.mean(res[0].per_cell_accepted == st_ref[:, 3]) >= 0.999
+
+
+@pytest.mark.parametrize("method", ["plain", "fused"])
+def test_blocked_schedules_equal_serial_schedules_bitwise(cuda_device, method, monkeypatch):
+    """The register-blocked LU and triangular solves against the serial
+    schedules (selected by MICMB_SERIAL_SCHEDULES when the solver uploads its
+    tables): whole per-cell solves, identical bits and step counts."""
+    from micm_b200 import Solver
+    from gpu_helpers import make_state
+    cfg = synthetic.CONFIGS["c210_uneven"]
+    mech = cfg["mech"]()
+    inp = synthetic.cell_inputs(mech, 1024, cfg["seed"], **cfg["inputs"])
+    out = []
+    for serial in (False, True):
+        if serial:
+            monkeypatch.setenv("MICMB_SERIAL_SCHEDULES", "1")
+        else:
+            monkeypatch.delenv("MICMB_SERIAL_SCHEDULES", raising=False)
+        solver = Solver(mech, cfg["stages"], vector_length=128)
+        solver.set_fused_config(variant=2, lu_in_shared=0)
+        st = make_state(solver, inp)
+        solver.update_state_parameters(st)
+        res = solver.solve(cfg["dt"], st, method=method, step_control="per_cell", per_cell=True)
+        st.sync_outputs_to_host()
+        out.append((st.concentrations(), res.per_cell_accepted))
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
