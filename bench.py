@@ -55,7 +55,7 @@ WORKLOADS = {
                          "micm_bench's initial state on every cell, 3-stage Rosenbrock, dt=30 s, fused persistent "
                          "kernel",
                     l2="inputs exceed L2 (75 MB state + 59 MB rate constants + 25 MB parameters); no flush",
-                    adjoint=None, profile="k_fused_thread_chapman_1M.md"),
+                    adjoint=None, profile=None),
     "ts1": dict(cells=1048576, cpu_sample=65536,
                 text="micm's TS1 benchmark mechanism (209 species, 547 reactions) on {cells} cells per GPU, "
                      "micm_bench's initial state on every cell, 3-stage Rosenbrock, dt=30 s, fused persistent kernel",
@@ -331,7 +331,10 @@ def hbm_peak():
 
 
 def measured_traffic(profile, cells):
-    """DRAM bytes of one fused launch over `cells` cells, scaled from the committed capture."""
+    """DRAM bytes of one fused launch over `cells` cells, scaled from the committed capture
+    (None when the workload has no capture)."""
+    if not profile:
+        return None
     path = os.path.join(ROOT, "profiles", profile)
     try:
         with open(path) as f:
@@ -684,8 +687,9 @@ def main():
                          "kernel": KERNEL_OF_VARIANT.get(tuned["variant"], "fused") + " (one launch per step)",
                          "algorithmic_bytes_per_launch": algo_bytes, "kernel_ms_per_launch": kernel_ms / args.steps,
                          "peak_source": peak_src,
-                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of the capture in "
-                                           f"profiles/{W['profile']}, scaled by cells",
+                         "traffic_source": ("dram__bytes_read.sum + dram__bytes_write.sum of the capture in "
+                                            f"profiles/{W['profile']}, scaled by cells") if W["profile"]
+                                           else "no capture of this workload",
                          "fp64": {"achieved_tflops": flops / kernel_s / 1e12, "peak_tflops": fp64_peak(),
                                   "frac": flops / kernel_s / 1e12 / fp64_peak(), "flops_per_launch": flops,
                                   "peak_source": "nominal (SMs x 64 FMA/clk x 2 x max SM clock)"}},
