@@ -304,7 +304,11 @@ namespace micmb
       d.bwd_s = Resolve(b, bws);
       d.fwd_t_s = Resolve(b, fwts);
       d.bwd_t_s = Resolve(b, bwts);
-      d.has_blocked = (m.has_blocked && !std::getenv("MICMB_SERIAL_SCHEDULES")) ? 1 : 0;
+      // the register-blocked LU and solves are opt-in: on the 210-species
+      // mechanism they measured slower than the serial schedules (the operand
+      // re-reads they remove hit L1, and their accesses spread over more DRAM pages)
+      const char* blk = std::getenv("MICMB_BLOCKED_SCHEDULES");
+      d.has_blocked = (m.has_blocked && blk && blk[0] == '1') ? 1 : 0;
       if (m.has_blocked)
       {
         d.lu_b = ResolveBlocked(b, blu);

@@ -185,20 +185,20 @@ def test_uneven_1m_workload_sample_against_micm(cuda_device):
 
 @pytest.mark.parametrize("method", ["plain", "fused"])
 def test_blocked_schedules_equal_serial_schedules_bitwise(cuda_device, method, monkeypatch):
-    """The register-blocked LU and triangular solves against the serial
-    schedules (selected by MICMB_SERIAL_SCHEDULES when the solver uploads its
-    tables): whole per-cell solves, identical bits and step counts."""
+    """The register-blocked LU and triangular solves (selected by
+    MICMB_BLOCKED_SCHEDULES=1 when the solver uploads its tables) against the
+    serial schedules: whole per-cell solves, identical bits and step counts."""
     from micm_b200 import Solver
     from gpu_helpers import make_state
     cfg = synthetic.CONFIGS["c210_uneven"]
     mech = cfg["mech"]()
     inp = synthetic.cell_inputs(mech, 1024, cfg["seed"], **cfg["inputs"])
     out = []
-    for serial in (False, True):
-        if serial:
-            monkeypatch.setenv("MICMB_SERIAL_SCHEDULES", "1")
+    for blocked in (True, False):
+        if blocked:
+            monkeypatch.setenv("MICMB_BLOCKED_SCHEDULES", "1")
         else:
-            monkeypatch.delenv("MICMB_SERIAL_SCHEDULES", raising=False)
+            monkeypatch.delenv("MICMB_BLOCKED_SCHEDULES", raising=False)
         solver = Solver(mech, cfg["stages"], vector_length=128)
         solver.set_fused_config(variant=2, lu_in_shared=0)
         st = make_state(solver, inp)
