@@ -421,6 +421,8 @@ namespace micm
     std::array<Real, 6> e_{};
     std::array<Real, 6> alpha_{};
     std::array<Real, 6> gamma_{};
+    Index constraint_init_max_iterations_{ 10 };  // DAE constraint initialisation (rosenbrock_solver_parameters.hpp:43-44)
+    Real constraint_init_tolerance_{ 1e-10 };
 
     static RosenbrockSolverParameters TwoStageRosenbrockParameters()
     {
@@ -457,6 +459,8 @@ namespace micm
       p.h_max = h_max_;
       p.h_start = h_start_;
       p.estimator_of_local_order = estimator_of_local_order_;
+      p.constraint_init_max_iterations = (int32_t)constraint_init_max_iterations_;
+      p.constraint_init_tolerance = constraint_init_tolerance_;
       for (int i = 0; i < 6; ++i)
       {
         p.new_function_evaluation[i] = new_function_evaluation_[i] ? 1 : 0;
@@ -487,6 +491,8 @@ namespace micm
       r.rejection_factor_decrease_ = p.rejection_factor_decrease;
       r.safety_factor_ = p.safety_factor;
       r.estimator_of_local_order_ = p.estimator_of_local_order;
+      r.constraint_init_max_iterations_ = (Index)p.constraint_init_max_iterations;
+      r.constraint_init_tolerance_ = p.constraint_init_tolerance;
       for (int i = 0; i < 6; ++i)
       {
         r.new_function_evaluation_[i] = p.new_function_evaluation[i] != 0;

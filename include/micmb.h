@@ -54,6 +54,7 @@ extern "C" {
 #define MICMB_SOLVER_NAN_DETECTED 6
 #define MICMB_SOLVER_INF_DETECTED 7
 #define MICMB_SOLVER_ACCEPTING_UNCONVERGED 8 /* Backward Euler: AcceptingUnconvergedIntegration */
+#define MICMB_SOLVER_CONSTRAINT_INITIALIZATION_FAILED 9 /* DAE: ConstraintInitializationFailed */
 
 /* ------------------------------------------------------------------ */
 /* mechanism description                                               */
@@ -113,7 +114,28 @@ typedef struct micmb_mechanism_desc {
   int32_t n_parameterized;
   const double* parameterized_coef; /* [4 * n_parameterized] */
   int32_t reorder_state;            /* SolverBuilder::SetReorderState, default 1 */
+  /* Algebraic constraints (DAE form; include/micm/constraint/types/
+   * linear_constraint.hpp, equilibrium_constraint.hpp), as
+   * SolverBuilder::SetConstraints passes them.  Each constraint replaces the
+   * ODE row of its algebraic species (mass-matrix diagonal 0 there):
+   *   LINEAR       G = sum_t coef_t * y[species_t] - params[0]
+   *   EQUILIBRIUM  G = K_eq(T) * prod_reactants y^coef - prod_products y^coef,
+   *                the first n_reactants terms are reactants,
+   *                K_eq(T) = params[0] * exp((params[1] / params[2]) * (1/T - 1/params[3]))
+   *                (K_HLC_ref, delta_H [J mol-1], R [J mol-1 K-1], T_ref [K]).
+   * n_constraints = 0 (and null arrays) for a plain ODE mechanism. */
+  int32_t n_constraints;
+  const int32_t* constraint_type;         /* [n_constraints] MICMB_CONSTRAINT_* */
+  const int32_t* constraint_species;      /* [n_constraints] algebraic species */
+  const int32_t* constraint_term_start;   /* [n_constraints + 1] */
+  const int32_t* constraint_term_species; /* [constraint_term_start[n_constraints]] */
+  const double* constraint_term_coef;     /* coefficient (linear) or stoichiometry (equilibrium) */
+  const int32_t* constraint_n_reactants;  /* [n_constraints] equilibrium: leading reactant terms */
+  const double* constraint_params;        /* [n_constraints * 4], see above */
 } micmb_mechanism_desc;
+
+#define MICMB_CONSTRAINT_LINEAR 0
+#define MICMB_CONSTRAINT_EQUILIBRIUM 1
 
 /* Rosenbrock tableau and step control
  * (include/micm/solver/rosenbrock_solver_parameters.hpp:22-67). */
@@ -136,6 +158,11 @@ typedef struct micmb_rosenbrock_params {
   double e[6];
   double alpha[6];
   double gamma[6];
+  /* DAE constraint initialisation (Newton on the algebraic variables at the
+   * start of each Solve; rosenbrock.inl:407-576): iterations and tolerance on
+   * the largest |G| */
+  int32_t constraint_init_max_iterations; /* 10 */
+  double constraint_init_tolerance;       /* 1e-10 */
 } micmb_rosenbrock_params;
 
 /* micm::SolverStats (include/micm/solver/solver_result.hpp:37-57), summed

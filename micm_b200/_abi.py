@@ -24,6 +24,14 @@ class MechanismDesc(C.Structure):
         ("n_parameterized", C.c_int32),
         ("parameterized_coef", f64p),
         ("reorder_state", C.c_int32),
+        ("n_constraints", C.c_int32),
+        ("constraint_type", i32p),
+        ("constraint_species", i32p),
+        ("constraint_term_start", i32p),
+        ("constraint_term_species", i32p),
+        ("constraint_term_coef", f64p),
+        ("constraint_n_reactants", i32p),
+        ("constraint_params", f64p),
     ]
 
 
@@ -47,6 +55,8 @@ class RosenbrockParams(C.Structure):
         ("e", C.c_double * 6),
         ("alpha", C.c_double * 6),
         ("gamma", C.c_double * 6),
+        ("constraint_init_max_iterations", C.c_int32),
+        ("constraint_init_tolerance", C.c_double),
     ]
 
 
@@ -107,7 +117,17 @@ class DescHolder:
             n_parameterized=int(a["n_parameterized"]),
             parameterized_coef=ptr(a["parameterized_coef"], C.c_double),
             reorder_state=int(a["reorder_state"]),
+            n_constraints=int(a.get("n_constraints", 0)),
         )
+        if self.desc.n_constraints:
+            d = self.desc
+            d.constraint_type = ptr(a["constraint_type"], C.c_int32)
+            d.constraint_species = ptr(a["constraint_species"], C.c_int32)
+            d.constraint_term_start = ptr(a["constraint_term_start"], C.c_int32)
+            d.constraint_term_species = ptr(_nonempty(a, "constraint_term_species", np.int32), C.c_int32)
+            d.constraint_term_coef = ptr(_nonempty(a, "constraint_term_coef", np.float64), C.c_double)
+            d.constraint_n_reactants = ptr(a["constraint_n_reactants"], C.c_int32)
+            d.constraint_params = ptr(a["constraint_params"], C.c_double)
 
 
 def _nonempty(a, key, dtype):

@@ -508,6 +508,8 @@ extern "C"
       Need(out != nullptr, "null argument");
       micmb_rosenbrock_params p{};
       p.max_number_of_steps = 1000;
+      p.constraint_init_max_iterations = 10;  // rosenbrock_solver_parameters.hpp:43-44
+      p.constraint_init_tolerance = 1e-10;
       p.round_off = 2.220446049250313080847e-16;  // std::numeric_limits<double>::epsilon()
       p.factor_min = 0.2;
       p.factor_max = 6;

@@ -850,6 +850,51 @@ namespace micmb
         m.species_column[perm[i]] = i;
     }
 
+    // 2b. algebraic constraints (constraint_set.hpp:90-160): the algebraic
+    //     species' rows become algebraic (mass-matrix diagonal 0)
+    m.mass.assign(S, 1.0);
+    std::vector<char> algebraic(S, 0);
+    Require(d.n_constraints >= 0, "negative constraint count");
+    if (d.n_constraints > 0)
+    {
+      Require(d.constraint_type && d.constraint_species && d.constraint_term_start && d.constraint_n_reactants &&
+                  d.constraint_params,
+              "constraint arrays missing");
+      Require(d.constraint_term_start[0] == 0, "constraint_term_start[0] must be 0");
+      const int32_t n_terms = d.constraint_term_start[d.n_constraints];
+      Require(n_terms == 0 || (d.constraint_term_species && d.constraint_term_coef), "constraint terms missing");
+      for (int32_t c = 0; c < d.n_constraints; ++c)
+      {
+        CompiledMechanism::ConstraintDef cd;
+        cd.kind = d.constraint_type[c];
+        Require(cd.kind == MICMB_CONSTRAINT_LINEAR || cd.kind == MICMB_CONSTRAINT_EQUILIBRIUM, "unknown constraint kind");
+        const int32_t sp = d.constraint_species[c];
+        Require(sp >= 0 && sp < S, "constraint algebraic species out of range");
+        cd.row = m.species_column[sp];
+        Require(!algebraic[cd.row], "a species is the algebraic variable of two constraints");
+        algebraic[cd.row] = 1;
+        m.mass[cd.row] = 0.0;
+        const int32_t a = d.constraint_term_start[c], b = d.constraint_term_start[c + 1];
+        Require(a <= b && b <= n_terms && b > a, "constraint terms out of order or empty");
+        cd.t0 = (int32_t)m.c_term_col.size();
+        for (int32_t t = a; t < b; ++t)
+        {
+          const int32_t ts = d.constraint_term_species[t];
+          Require(ts >= 0 && ts < S, "constraint term species out of range");
+          m.c_term_col.push_back(m.species_column[ts]);
+          m.c_term_coef.push_back(d.constraint_term_coef[t]);
+        }
+        cd.t1 = (int32_t)m.c_term_col.size();
+        cd.n_react = cd.kind == MICMB_CONSTRAINT_EQUILIBRIUM ? d.constraint_n_reactants[c] : 0;
+        Require(cd.n_react >= 0 && cd.n_react <= b - a, "equilibrium reactant count out of range");
+        for (int i = 0; i < 4; ++i)
+          cd.p[i] = d.constraint_params[4 * (size_t)c + i];
+        if (cd.kind == MICMB_CONSTRAINT_EQUILIBRIUM)
+          cd.keq = m.n_eq++;
+        m.constraints.push_back(cd);
+      }
+    }
+
     // 3. rate definitions and reactant/product tables by rate column
     int32_t next_param = 0;
     m.param_column.assign(R, -1);
@@ -959,6 +1004,19 @@ namespace micmb
       }
     for (int32_t i = 0; i < S; ++i)
       nz.insert({ i, i });
+    if (!m.constraints.empty())
+    {
+      // kinetic entries of algebraic rows go (solver_builder.inl:377-389); the
+      // constraints' own entries and diagonals come in
+      for (auto it = nz.begin(); it != nz.end();)
+        it = algebraic[it->first] ? nz.erase(it) : std::next(it);
+      for (const CompiledMechanism::ConstraintDef& cd : m.constraints)
+      {
+        nz.insert({ cd.row, cd.row });
+        for (int32_t t = cd.t0; t < cd.t1; ++t)
+          nz.insert({ cd.row, m.c_term_col[t] });
+      }
+    }
     m.pattern_unfilled.assign(nz.begin(), nz.end());
     std::vector<std::set<int32_t>> row_cols(S), col_rows(S);
     for (const auto& e : nz)
@@ -1002,6 +1060,8 @@ namespace micmb
       m.f_start.push_back(0);
       for (int32_t s = 0; s < S; ++s)
       {
+        if (algebraic[s])
+          terms[s].clear();  // the constraint's residual replaces the row
         for (const auto& t : terms[s])
         {
           m.f_rxn.push_back(t.first);
@@ -1017,11 +1077,15 @@ namespace micmb
       for (int32_t info = 0; info < (int32_t)m.info_rxn.size(); ++info)
       {
         const int32_t ind = m.info_ind[info], rc = m.info_rxn[info];
+        // process terms of algebraic rows are skipped (process_set.hpp:623-660)
         for (int32_t i = m.info_dep_start[info]; i < m.info_dep_start[info + 1]; ++i)
-          terms[pos(m.info_dep_ids[i], ind)].push_back({ info, 1.0 });
-        terms[pos(ind, ind)].push_back({ info, 1.0 });
+          if (!algebraic[m.info_dep_ids[i]])
+            terms[pos(m.info_dep_ids[i], ind)].push_back({ info, 1.0 });
+        if (!algebraic[ind])
+          terms[pos(ind, ind)].push_back({ info, 1.0 });
         for (int32_t i = m.prod_start[rc]; i < m.prod_start[rc + 1]; ++i)
-          terms[pos(m.prod_ids[i], ind)].push_back({ info, -m.prod_yield[i] });
+          if (!algebraic[m.prod_ids[i]])
+            terms[pos(m.prod_ids[i], ind)].push_back({ info, -m.prod_yield[i] });
       }
       m.j_start.push_back(0);
       for (int32_t e = 0; e < m.nnz; ++e)
@@ -1032,6 +1096,28 @@ namespace micmb
           m.j_coef.push_back(t.second);
         }
         m.j_start.push_back((int32_t)m.j_info.size());
+      }
+    }
+
+    // 7b. constraint Jacobian positions, and per position the constraint
+    //     terms it receives in micm's order (constraint order; an equilibrium
+    //     constraint's reactants, then its products)
+    m.cj_start.assign(1, 0);
+    if (!m.constraints.empty())
+    {
+      m.c_term_pos.resize(m.c_term_col.size());
+      std::vector<std::vector<int32_t>> at(m.nnz);
+      for (const CompiledMechanism::ConstraintDef& cd : m.constraints)
+        for (int32_t t = cd.t0; t < cd.t1; ++t)
+        {
+          m.c_term_pos[t] = pos(cd.row, m.c_term_col[t]);
+          at[m.c_term_pos[t]].push_back(t);
+        }
+      for (int32_t e = 0; e < m.nnz; ++e)
+      {
+        for (int32_t t : at[e])
+          m.cj_term.push_back(t);
+        m.cj_start.push_back((int32_t)m.cj_term.size());
       }
     }
 
@@ -1259,6 +1345,14 @@ namespace micmb
     h = FnvVec(h, m.prod_yield);
     for (const auto& r : m.rates)
       h = Fnv(h, &r.kind, sizeof(r.kind));
+    h = FnvVec(h, m.c_term_col);
+    h = FnvVec(h, m.c_term_coef);
+    for (const auto& cd : m.constraints)
+    {
+      h = Fnv(h, &cd.kind, sizeof(cd.kind));
+      h = Fnv(h, &cd.row, sizeof(cd.row));
+      h = Fnv(h, cd.p, sizeof(cd.p));
+    }
     m.hash = h;
     return m;
   }

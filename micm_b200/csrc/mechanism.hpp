@@ -192,6 +192,29 @@ namespace micmb
     WarpTable w_lu, w_fwd, w_bwd, w_fwd_t, w_bwd_t, w_forcing, w_jacobian;
     StreamProgram stream;
 
+    // algebraic constraints (DAE form; constraint_set.hpp).  Each replaces the
+    // ODE row of its algebraic species: process terms are left out of that
+    // row's forcing and -J gathers, the constraint residual G overwrites the
+    // forcing, and -dG/dy fills the row's Jacobian entries.
+    struct ConstraintDef
+    {
+      int32_t kind = 0;     // MICMB_CONSTRAINT_*
+      int32_t row = 0;      // state column of the algebraic species
+      int32_t t0 = 0, t1 = 0;  // terms [t0, t1) of c_term_*
+      int32_t n_react = 0;  // equilibrium: leading reactant terms
+      int32_t keq = -1;     // equilibrium: index of its K_eq among the cell's K_eq values
+      double p[4] = { 0, 0, 0, 0 };
+    };
+    std::vector<ConstraintDef> constraints;  // input order
+    std::vector<int32_t> c_term_col;         // state column of each term
+    std::vector<double> c_term_coef;         // coefficient / stoichiometry
+    std::vector<int32_t> c_term_pos;         // LU position of (row, term column)
+    std::vector<double> mass;                // [S] mass-matrix diagonal: 1 ODE row, 0 algebraic row
+    int32_t n_eq = 0;                        // equilibrium constraints
+    // per LU position, the constraint terms whose derivative it receives, in
+    // the order micm applies them (constraint order, reactants then products)
+    std::vector<int32_t> cj_start, cj_term;
+
     int32_t lu_updates = 0;
     int32_t lu_lower = 0;
     uint64_t hash = 0;

@@ -93,6 +93,39 @@ class Reaction:
     label: Optional[str] = None            # custom parameter label (UD / surface)
 
 
+CONSTRAINT_LINEAR = 0
+CONSTRAINT_EQUILIBRIUM = 1
+
+
+@dataclasses.dataclass
+class Constraint:
+    """An algebraic constraint replacing the ODE row of `species`
+    (include/micm/constraint/types/linear_constraint.hpp,
+    equilibrium_constraint.hpp)."""
+    kind: int
+    species: int                              # algebraic species (system index)
+    terms: List[Tuple[int, float]]            # (species, coefficient or stoichiometry)
+    n_reactants: int = 0                      # equilibrium: leading reactant terms
+    params: Tuple[float, float, float, float] = (0.0, 0.0, 0.0, 0.0)
+    name: str = "constraint"
+
+
+def linear_constraint(species: int, terms: Sequence[Tuple[int, float]], constant: float, name="linear"):
+    """LinearConstraint: sum coef * [species] - constant = 0, replacing the row of `species`."""
+    return Constraint(CONSTRAINT_LINEAR, species, [(int(a), float(c)) for a, c in terms], 0,
+                      (float(constant), 0.0, 0.0, 0.0), name)
+
+
+def equilibrium_constraint(species: int, reactants: Sequence[Tuple[int, float]], products: Sequence[Tuple[int, float]],
+                           K_HLC_ref: float, delta_H: float = 0.0, R: float = GAS_CONSTANT, T_ref: float = 298.15,
+                           name="equilibrium"):
+    """EquilibriumConstraint: K_eq(T) prod [reactants]^a - prod [products]^b = 0 with the
+    Van't Hoff K_eq(T) = K_HLC_ref exp((delta_H / R)(1/T - 1/T_ref)), replacing the row of `species`."""
+    terms = [(int(a), float(c)) for a, c in reactants] + [(int(a), float(c)) for a, c in products]
+    return Constraint(CONSTRAINT_EQUILIBRIUM, species, terms, len(reactants),
+                      (float(K_HLC_ref), float(delta_H), float(R), float(T_ref)), name)
+
+
 @dataclasses.dataclass
 class Mechanism:
     species: List[str]
@@ -102,6 +135,7 @@ class Mechanism:
     relative_tolerance: float = 1e-6
     reorder_state: bool = True
     name: str = "mechanism"
+    constraints: List[Constraint] = dataclasses.field(default_factory=list)
 
     @property
     def n_species(self) -> int:
@@ -163,6 +197,29 @@ class Mechanism:
             n_parameterized=len(self.parameterized),
             parameterized_coef=pc if pc.size else np.zeros(1, dtype=np.float64),
             reorder_state=1 if self.reorder_state else 0,
+            **self._constraint_arrays(),
+        )
+
+    def _constraint_arrays(self) -> Dict[str, np.ndarray]:
+        n = len(self.constraints)
+        if n == 0:
+            return dict(n_constraints=0)
+        start = np.zeros(n + 1, dtype=np.int32)
+        tsp, tco = [], []
+        for i, c in enumerate(self.constraints):
+            for a, coef in c.terms:
+                tsp.append(a)
+                tco.append(coef)
+            start[i + 1] = len(tsp)
+        return dict(
+            n_constraints=n,
+            constraint_type=np.array([c.kind for c in self.constraints], dtype=np.int32),
+            constraint_species=np.array([c.species for c in self.constraints], dtype=np.int32),
+            constraint_term_start=start,
+            constraint_term_species=np.array(tsp, dtype=np.int32),
+            constraint_term_coef=np.array(tco, dtype=np.float64),
+            constraint_n_reactants=np.array([c.n_reactants for c in self.constraints], dtype=np.int32),
+            constraint_params=np.array([list(c.params) for c in self.constraints], dtype=np.float64).reshape(-1),
         )
 
     def atol(self) -> np.ndarray:

@@ -289,6 +289,11 @@ def _load_oracle():
         lib.om_replay_per_cell.argtypes = [C.c_void_p, C.c_void_p, C.c_int, _f64p, _f64p, _i32p, C.c_int, _f64p]
         lib.om_solve_global.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, _f64p, _f64p, C.c_double,
                                         _f64p, _i64p, C.c_int, _i32p, EXCHANGE_FN, C.c_void_p, C.c_int64]
+        lib.om_n_eq.argtypes = [C.c_void_p]
+        lib.om_constraint_params.argtypes = [C.c_void_p, C.c_int, _f64p, _f64p]
+        lib.om_constraint_params.restype = None
+        lib.om_solve_per_cell_keq.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, _f64p, _f64p, _f64p,
+                                              C.c_double, _f64p, _i64p, C.c_int]
         lib.om_set_correctly_rounded.argtypes = [C.c_void_p, C.c_int]
         lib.om_set_correctly_rounded.restype = None
         lib.om_math_eval.argtypes = [C.c_void_p, C.c_int, _f64p, _f64p, _f64p, C.c_int64]
@@ -370,15 +375,25 @@ class Restatement:
         return np.ascontiguousarray(self.rate_constants(inputs["temperature"], inputs["pressure"],
                                                         inputs["air_density"], inputs["custom_params"]))
 
+    def keq(self, temperature) -> np.ndarray:
+        """K_eq(T) of every equilibrium constraint per cell [n, n_eq] (this handle's exp)."""
+        T = np.ascontiguousarray(temperature, dtype=np.float64)
+        out = np.zeros((len(T), max(self.lib.om_n_eq(self.handle), 1)))
+        self.lib.om_constraint_params(self.handle, len(T), _p(T), _p(out))
+        return out
+
     def solve_per_cell(self, inputs, dt, threads=0, k=None):
+        """Per-cell step control; with constraints, micm's DAE Rosenbrock
+        (stats[:, 9] = constraint-initialisation iterations)."""
         y = np.zeros_like(inputs["concentrations"])
         y[:, self.species_columns] = inputs["concentrations"]
         n = len(y)
         k = self._k(inputs) if k is None else np.ascontiguousarray(k)
+        keq = self.keq(inputs["temperature"])
         stats = np.zeros((n, 10), np.int64)
-        rc = self.lib.om_solve_per_cell(self.handle, C.byref(self.params), n, float(dt), _p(k),
-                                        _p(self.atol_columns), self.mech.relative_tolerance, _p(y),
-                                        _p(stats, C.c_int64), int(threads or os.cpu_count() or 1))
+        rc = self.lib.om_solve_per_cell_keq(self.handle, C.byref(self.params), n, float(dt), _p(k), _p(keq),
+                                            _p(self.atol_columns), self.mech.relative_tolerance, _p(y),
+                                            _p(stats, C.c_int64), int(threads or os.cpu_count() or 1))
         if rc:
             raise RuntimeError(self.lib.om_last_error().decode())
         return np.ascontiguousarray(y[:, self.species_columns]), stats

@@ -39,6 +39,16 @@ struct om_mech
   int* pos; /* [S*S] storage position or -1 */
   int *nz_row, *nz_col;
   int cr; /* 0: the C library's exp/pow/log10 (micm's); 1: correctly rounded (quad precision) */
+  /* algebraic constraints (DAE form, constraint_set.hpp): each replaces the
+   * ODE row of its algebraic species (mass-matrix diagonal 0 there) */
+  int nc, n_eq, n_cterms;
+  int *c_kind, *c_row, *c_t0, *c_t1, *c_nreact, *c_keq;
+  double* c_par;   /* [nc][4] */
+  int* ct_col;     /* term state columns */
+  double* ct_coef; /* coefficient / stoichiometry */
+  int* ct_pos;     /* LU position of (row, term column) */
+  double* mass;    /* [S] 1 ODE row, 0 algebraic row */
+  char* alg;       /* [S] algebraic row */
 };
 
 #define NA 6.02214076e23
@@ -80,6 +90,18 @@ void om_destroy(om_mech* m)
   free(m->pos);
   free(m->nz_row);
   free(m->nz_col);
+  free(m->c_kind);
+  free(m->c_row);
+  free(m->c_t0);
+  free(m->c_t1);
+  free(m->c_nreact);
+  free(m->c_keq);
+  free(m->c_par);
+  free(m->ct_col);
+  free(m->ct_coef);
+  free(m->ct_pos);
+  free(m->mass);
+  free(m->alg);
   free(m);
 }
 
@@ -207,6 +229,52 @@ om_mech* om_create(const micmb_mechanism_desc* d)
   else
     for (int i = 0; i < S; ++i)
       m->species_col[i] = i;
+  /* 2b. constraints: algebraic rows (solver_builder.inl:345-393) */
+  m->mass = xcalloc(S, sizeof(double));
+  m->alg = xcalloc(S, 1);
+  for (int i = 0; i < S; ++i)
+    m->mass[i] = 1.0;
+  m->nc = d->n_constraints > 0 ? d->n_constraints : 0;
+  if (m->nc)
+  {
+    const int nt = d->constraint_term_start[m->nc];
+    m->n_cterms = nt;
+    m->c_kind = xcalloc(m->nc, sizeof(int));
+    m->c_row = xcalloc(m->nc, sizeof(int));
+    m->c_t0 = xcalloc(m->nc, sizeof(int));
+    m->c_t1 = xcalloc(m->nc, sizeof(int));
+    m->c_nreact = xcalloc(m->nc, sizeof(int));
+    m->c_keq = xcalloc(m->nc, sizeof(int));
+    m->c_par = xcalloc((size_t)m->nc * 4, sizeof(double));
+    m->ct_col = xcalloc(nt + 1, sizeof(int));
+    m->ct_coef = xcalloc(nt + 1, sizeof(double));
+    m->ct_pos = xcalloc(nt + 1, sizeof(int));
+    for (int c = 0; c < m->nc; ++c)
+    {
+      const int row = m->species_col[d->constraint_species[c]];
+      if (m->alg[row])
+      {
+        snprintf(g_err, sizeof g_err, "a species is the algebraic variable of two constraints");
+        free(order);
+        om_destroy(m);
+        return NULL;
+      }
+      m->alg[row] = 1;
+      m->mass[row] = 0.0;
+      m->c_kind[c] = d->constraint_type[c];
+      m->c_row[c] = row;
+      m->c_t0[c] = d->constraint_term_start[c];
+      m->c_t1[c] = d->constraint_term_start[c + 1];
+      m->c_nreact[c] = m->c_kind[c] == MICMB_CONSTRAINT_EQUILIBRIUM ? d->constraint_n_reactants[c] : 0;
+      m->c_keq[c] = m->c_kind[c] == MICMB_CONSTRAINT_EQUILIBRIUM ? m->n_eq++ : -1;
+      memcpy(m->c_par + 4 * (size_t)c, d->constraint_params + 4 * (size_t)c, 4 * sizeof(double));
+      for (int t = m->c_t0[c]; t < m->c_t1[c]; ++t)
+      {
+        m->ct_col[t] = m->species_col[d->constraint_term_species[t]];
+        m->ct_coef[t] = d->constraint_term_coef[t];
+      }
+    }
+  }
   /* 3. tables by rate column */
   m->kind = xcalloc(R, sizeof(int));
   m->rp = xcalloc((size_t)R * MICMB_RATE_PARAM_STRIDE, sizeof(double));
@@ -315,6 +383,16 @@ om_mech* om_create(const micmb_mechanism_desc* d)
     }
   for (int i = 0; i < S; ++i)
     M[(size_t)i * S + i] = 1;
+  /* algebraic rows: kinetic entries out, the constraint's entries and diagonal in */
+  for (int i = 0; i < S; ++i)
+    if (m->alg[i])
+      memset(M + (size_t)i * S, 0, S);
+  for (int c = 0; c < m->nc; ++c)
+  {
+    M[(size_t)m->c_row[c] * S + m->c_row[c]] = 1;
+    for (int t = m->c_t0[c]; t < m->c_t1[c]; ++t)
+      M[(size_t)m->c_row[c] * S + m->ct_col[t]] = 1;
+  }
   for (int i = 0; i < S; ++i)
     for (int k = i + 1; k < S; ++k)
       if (M[(size_t)i * S + k])
@@ -342,6 +420,9 @@ om_mech* om_create(const micmb_mechanism_desc* d)
         m->pos[(size_t)i * S + j] = -1;
     }
   m->nnz = nnz;
+  for (int c = 0; c < m->nc; ++c)
+    for (int t = m->c_t0[c]; t < m->c_t1[c]; ++t)
+      m->ct_pos[t] = m->pos[(size_t)m->c_row[c] * S + m->ct_col[t]];
   free(M);
   free(order);
   return m;
@@ -489,9 +570,11 @@ static void forcing(const om_mech* m, const double* k, const double* y, double* 
     for (int i = m->rs[r]; i < m->rs[r + 1]; ++i)
       rate *= y[m->rid[i]];
     for (int i = m->rs[r]; i < m->rs[r + 1]; ++i)
-      f[m->rid[i]] -= rate;
+      if (!m->alg[m->rid[i]])
+        f[m->rid[i]] -= rate;
     for (int i = m->ps[r]; i < m->ps[r + 1]; ++i)
-      f[m->pid[i]] += m->py[i] * rate;
+      if (!m->alg[m->pid[i]])
+        f[m->pid[i]] += m->py[i] * rate;
   }
 }
 
@@ -507,12 +590,105 @@ static void neg_jacobian(const om_mech* m, const double* k, const double* y, dou
     double d = k[rc];
     for (int i = m->info_ds[q]; i < m->info_ds[q + 1]; ++i)
       d *= y[m->info_dep[i]];
+    /* process terms of algebraic rows are skipped (process_set.hpp:623-660) */
     for (int i = m->info_ds[q]; i < m->info_ds[q + 1]; ++i)
-      jac[m->pos[(size_t)m->info_dep[i] * S + ind]] += d;
-    jac[m->pos[(size_t)ind * S + ind]] += d;
+      if (!m->alg[m->info_dep[i]])
+        jac[m->pos[(size_t)m->info_dep[i] * S + ind]] += d;
+    if (!m->alg[ind])
+      jac[m->pos[(size_t)ind * S + ind]] += d;
     for (int i = m->ps[rc]; i < m->ps[rc + 1]; ++i)
-      jac[m->pos[(size_t)m->pid[i] * S + ind]] -= m->py[i] * d;
+      if (!m->alg[m->pid[i]])
+        jac[m->pos[(size_t)m->pid[i] * S + ind]] -= m->py[i] * d;
   }
+}
+
+/* max(c, 0)^e, as the equilibrium constraint raises concentrations */
+static double cpow_clamped(const om_mech* m, double c, double e)
+{
+  return o_pow(m, (c > 0.0 ? c : 0.0), e);
+}
+
+/* constraint residuals overwrite the algebraic rows of f
+ * (linear_constraint.hpp:216-259, equilibrium_constraint.hpp:367-424) */
+static void constraint_forcing(const om_mech* m, const double* keq, const double* y, double* f)
+{
+  for (int c = 0; c < m->nc; ++c)
+  {
+    if (m->c_kind[c] == MICMB_CONSTRAINT_LINEAR)
+    {
+      double sum = 0.0;
+      for (int t = m->c_t0[c]; t < m->c_t1[c]; ++t)
+        sum += m->ct_coef[t] * y[m->ct_col[t]];
+      f[m->c_row[c]] = sum - m->c_par[4 * c];
+    }
+    else
+    {
+      double rp = keq[m->c_keq[c]], pp = 1.0;
+      const int tr = m->c_t0[c] + m->c_nreact[c];
+      for (int t = m->c_t0[c]; t < tr; ++t)
+        rp *= cpow_clamped(m, y[m->ct_col[t]], m->ct_coef[t]);
+      for (int t = tr; t < m->c_t1[c]; ++t)
+        pp *= cpow_clamped(m, y[m->ct_col[t]], m->ct_coef[t]);
+      f[m->c_row[c]] = rp - pp;
+    }
+  }
+}
+
+/* jac -= dG/dy for every constraint (linear_constraint.hpp:264-290,
+ * equilibrium_constraint.hpp:432-580) */
+static void constraint_neg_jacobian(const om_mech* m, const double* keq, const double* y, double* jac)
+{
+  for (int c = 0; c < m->nc; ++c)
+  {
+    if (m->c_kind[c] == MICMB_CONSTRAINT_LINEAR)
+    {
+      for (int t = m->c_t0[c]; t < m->c_t1[c]; ++t)
+        jac[m->ct_pos[t]] -= m->ct_coef[t];
+      continue;
+    }
+    const int t0 = m->c_t0[c], tr = t0 + m->c_nreact[c], t1 = m->c_t1[c];
+    const double K = keq[m->c_keq[c]];
+    for (int side = 0; side < 2; ++side)
+    {
+      const int a = side ? tr : t0, b = side ? t1 : tr;
+      for (int i = a; i < b; ++i)
+      {
+        double prod = side ? 1.0 : K;
+        for (int j = a; j < b; ++j)
+          if (j != i)
+            prod *= cpow_clamped(m, y[m->ct_col[j]], m->ct_coef[j]);
+        const double conc = y[m->ct_col[i]], st = m->ct_coef[i];
+        double partial;
+        if (st == 1.0)
+          partial = prod;
+        else if (conc > 0.0)
+          partial = st * prod * o_pow(m, conc, st - 1.0);
+        else
+          partial = 0.0;
+        if (side)
+          jac[m->ct_pos[i]] += partial;
+        else
+          jac[m->ct_pos[i]] -= partial;
+      }
+    }
+  }
+}
+
+/* K_eq(T) per equilibrium constraint (equilibrium_constraint.hpp:290-309) */
+void om_constraint_params(const om_mech* m, int n, const double* T, double* keq)
+{
+  for (int c0 = 0; c0 < n; ++c0)
+    for (int c = 0; c < m->nc; ++c)
+      if (m->c_kind[c] == MICMB_CONSTRAINT_EQUILIBRIUM)
+      {
+        const double* q = m->c_par + 4 * c;
+        keq[(size_t)c0 * m->n_eq + m->c_keq[c]] = q[0] * o_exp(m, (q[1] / q[2]) * (1.0 / T[c0] - 1.0 / q[3]));
+      }
+}
+
+int om_n_eq(const om_mech* m)
+{
+  return m->n_eq;
 }
 
 static void decompose(const om_mech* m, double* A)
@@ -635,9 +811,69 @@ static double dmax(double a, double b)
 }
 
 /* returns state; stats[0..6]; optionally records accepted (y_n, H_n) */
+/* micm's InitializeConstraints (rosenbrock.inl:407-576) for one cell: Newton
+ * iterations on the algebraic variables until max |G| over algebraic rows is
+ * below the tolerance.  Returns the solver state; counts its Jacobian
+ * updates, decompositions and solves, and the iterations in *iters. */
+static int initialize_constraints(const om_mech* m, const micmb_rosenbrock_params* p, const double* keq, double* Y,
+                                  work_t* w, int64_t* ju, int64_t* dec, int64_t* sol, int64_t* iters)
+{
+  const int S = m->S;
+  double* delta = w->F0;
+  for (int iter = 0; iter < p->constraint_init_max_iterations; ++iter)
+  {
+    for (int i = 0; i < S; ++i)
+      delta[i] = 0.0;
+    constraint_forcing(m, keq, Y, delta);
+    double max_res = 0.0;
+    int any_nan = 0, any_inf = 0;
+    for (int i = 0; i < S; ++i)
+      if (m->mass[i] == 0.0)
+      {
+        const double v = delta[i];
+        any_nan = any_nan || isnan(v);
+        any_inf = any_inf || isinf(v);
+        const double a = fabs(v);
+        if (!isnan(a) && !isinf(a))
+          max_res = (max_res > a ? max_res : a);
+      }
+    if (any_nan)
+      return MICMB_SOLVER_NAN_DETECTED;
+    if (any_inf)
+      return MICMB_SOLVER_INF_DETECTED;
+    *iters = iter + 1;
+    if (max_res < p->constraint_init_tolerance)
+      return MICMB_SOLVER_CONVERGED;
+    for (int e = 0; e < m->nnz; ++e)
+      w->J[e] = 0.0;
+    constraint_neg_jacobian(m, keq, Y, w->J);
+    (*ju)++;
+    for (int i = 0; i < S; ++i)
+      w->J[m->pos[(size_t)i * S + i]] += 1.0 * m->mass[i];
+    decompose(m, w->J);
+    (*dec)++;
+    lu_solve(m, w->J, delta);
+    (*sol)++;
+    for (int i = 0; i < S; ++i)
+      if (m->mass[i] == 0.0)
+      {
+        const double d = delta[i];
+        any_nan = any_nan || isnan(d);
+        any_inf = any_inf || isinf(d);
+        if (!isnan(d) && !isinf(d))
+          Y[i] += d;
+      }
+    if (any_nan)
+      return MICMB_SOLVER_NAN_DETECTED;
+    if (any_inf)
+      return MICMB_SOLVER_INF_DETECTED;
+  }
+  return MICMB_SOLVER_CONSTRAINT_INITIALIZATION_FAILED;
+}
+
 static int rosenbrock_cell(const om_mech* m, const micmb_rosenbrock_params* p, double dt, const double* k,
-                           const double* atol, double rtol, work_t* w, int64_t* stats, double* ck_y, double* ck_h,
-                           int max_ck, int* n_ck)
+                           const double* keq, const double* atol, double rtol, work_t* w, int64_t* stats, double* ck_y,
+                           double* ck_h, int max_ck, int* n_ck)
 {
   const int S = m->S, ns = p->stages;
   double* Y = w->Y;
@@ -647,10 +883,16 @@ static int rosenbrock_cell(const om_mech* m, const micmb_rosenbrock_params* p, d
   double H = dmin(dmax(h_min, fabs(h_start)), fabs(h_max));
   double t = 0.0;
   int reject_last = 0, reject_more = 0, state = MICMB_SOLVER_RUNNING;
-  int64_t fc = 0, ju = 0, nst = 0, acc = 0, rej = 0, dec = 0, sol = 0;
+  int64_t fc = 0, ju = 0, nst = 0, acc = 0, rej = 0, dec = 0, sol = 0, init_iters = 0;
   if (n_ck)
     *n_ck = 0;
-  while ((t - dt + p->round_off) <= 0 && state == MICMB_SOLVER_RUNNING)
+  if (m->nc)
+  {
+    const int st = initialize_constraints(m, p, keq, Y, w, &ju, &dec, &sol, &init_iters);
+    if (st != MICMB_SOLVER_CONVERGED)
+      state = st;
+  }
+  while (state == MICMB_SOLVER_RUNNING && (t - dt + p->round_off) <= 0)
   {
     if (nst > p->max_number_of_steps)
     {
@@ -664,15 +906,19 @@ static int rosenbrock_cell(const om_mech* m, const micmb_rosenbrock_params* p, d
     }
     H = dmin(H, fabs(dt - t));
     forcing(m, k, Y, w->F0);
+    if (m->nc)
+      constraint_forcing(m, keq, Y, w->F0);
     fc++;
     neg_jacobian(m, k, Y, w->J);
+    if (m->nc)
+      constraint_neg_jacobian(m, keq, Y, w->J);
     ju++;
     int accepted = 0;
     while (!accepted)
     {
       double alpha = 1.0 / (H * p->gamma[0]);
       for (int i = 0; i < S; ++i)
-        w->J[m->pos[(size_t)i * S + i]] += alpha;
+        w->J[m->pos[(size_t)i * S + i]] += alpha * m->mass[i]; /* alpha M - J */
       decompose(m, w->J);
       dec++;
       for (int s = 0; s < ns; ++s)
@@ -688,6 +934,8 @@ static int rosenbrock_cell(const om_mech* m, const micmb_rosenbrock_params* p, d
             for (int i = 0; i < S; ++i)
               w->Ynew[i] += p->a[sc + j] * w->K[(size_t)j * S + i];
           forcing(m, k, w->Ynew, Ks);
+          if (m->nc)
+            constraint_forcing(m, keq, w->Ynew, Ks);
           fc++;
         }
         if (s + 1 < ns && !p->new_function_evaluation[s + 1])
@@ -696,7 +944,8 @@ static int rosenbrock_cell(const om_mech* m, const micmb_rosenbrock_params* p, d
         {
           double coh = p->c[sc + j] / H;
           for (int i = 0; i < S; ++i)
-            Ks[i] += coh * w->K[(size_t)j * S + i];
+            if (m->mass[i] != 0.0) /* algebraic rows have no mass coupling */
+              Ks[i] += coh * w->K[(size_t)j * S + i];
         }
         lu_solve(m, w->J, Ks);
         sol++;
@@ -710,6 +959,8 @@ static int rosenbrock_cell(const om_mech* m, const micmb_rosenbrock_params* p, d
       for (int s = 0; s < ns; ++s)
         for (int i = 0; i < S; ++i)
           w->Yerr[i] += p->e[s] * w->K[(size_t)s * S + i];
+      for (int c = 0; c < m->nc; ++c) /* SetAlgebraicErrors: the step change */
+        w->Yerr[m->c_row[c]] = w->Ynew[m->c_row[c]] - Y[m->c_row[c]];
       double sum = 0.0;
       for (int i = 0; i < S; ++i)
       {
@@ -767,6 +1018,8 @@ static int rosenbrock_cell(const om_mech* m, const micmb_rosenbrock_params* p, d
         if (acc >= 1)
           rej++;
         neg_jacobian(m, k, Y, w->J);
+        if (m->nc)
+          constraint_neg_jacobian(m, keq, Y, w->J);
         ju++;
       }
     }
@@ -784,7 +1037,7 @@ static int rosenbrock_cell(const om_mech* m, const micmb_rosenbrock_params* p, d
     stats[6] = sol;
     stats[7] = state;
     memcpy(&stats[8], &t, sizeof(double));
-    stats[9] = 0;
+    stats[9] = init_iters;
   }
   return state;
 }
@@ -948,6 +1201,7 @@ typedef struct
   int n;
   double dt;
   const double *k, *atol;
+  const double* keq; /* [cell][n_eq] or NULL */
   double rtol;
   double* y;
   int64_t* stats;
@@ -991,8 +1245,8 @@ static void* worker(void* arg)
     if (!j->adjoint)
     {
       memcpy(w.Y, j->y + (size_t)c * S, sizeof(double) * S);
-      rosenbrock_cell(m, j->p, j->dt, k, j->atol, j->rtol, &w, j->stats ? j->stats + (size_t)c * 10 : NULL, NULL,
-                      NULL, 0, NULL);
+      rosenbrock_cell(m, j->p, j->dt, k, j->keq ? j->keq + (size_t)c * m->n_eq : NULL, j->atol, j->rtol, &w,
+                      j->stats ? j->stats + (size_t)c * 10 : NULL, NULL, NULL, 0, NULL);
       for (int i = 0; i < S; ++i)
         j->y[(size_t)c * S + i] = w.Y[i] < 0.0 ? 0.0 : w.Y[i];
     }
@@ -1000,7 +1254,7 @@ static void* worker(void* arg)
     {
       int n_ck = 0;
       memcpy(w.Y, j->y0 + (size_t)c * S, sizeof(double) * S);
-      int st = rosenbrock_cell(m, j->p, j->dt, k, j->atol, j->rtol, &w, NULL, ck_y, ck_h, j->max_ck, &n_ck);
+      int st = rosenbrock_cell(m, j->p, j->dt, k, NULL, j->atol, j->rtol, &w, NULL, ck_y, ck_h, j->max_ck, &n_ck);
       if (st != MICMB_SOLVER_CONVERGED)
         j->failed = 1;
       double* yb = j->ybar0 + (size_t)c * S;
@@ -1038,9 +1292,15 @@ static int run(job_t* j, int n_threads)
   return j->failed ? -1 : 0;
 }
 
-int om_solve_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n, double dt, const double* k,
-                      const double* atol, double rtol, double* y, int64_t* stats_out, int n_threads)
+int om_solve_per_cell_keq(const om_mech* m, const micmb_rosenbrock_params* p, int n, double dt, const double* k,
+                          const double* keq, const double* atol, double rtol, double* y, int64_t* stats_out,
+                          int n_threads)
 {
+  if (m->nc && m->n_eq && !keq)
+  {
+    snprintf(g_err, sizeof g_err, "equilibrium constraints need K_eq values");
+    return -1;
+  }
   job_t j;
   memset(&j, 0, sizeof j);
   j.m = m;
@@ -1048,11 +1308,18 @@ int om_solve_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n,
   j.n = n;
   j.dt = dt;
   j.k = k;
+  j.keq = m->nc ? keq : NULL;
   j.atol = atol;
   j.rtol = rtol;
   j.y = y;
   j.stats = stats_out;
   return run(&j, n_threads);
+}
+
+int om_solve_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n, double dt, const double* k,
+                      const double* atol, double rtol, double* y, int64_t* stats_out, int n_threads)
+{
+  return om_solve_per_cell_keq(m, p, n, dt, k, NULL, atol, rtol, y, stats_out, n_threads);
 }
 
 /* ---------------------------------------------------------------- */
@@ -1600,7 +1867,7 @@ int om_step_sizes_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, i
   {
     int nck = 0;
     memcpy(w.Y, y0 + (size_t)c * S, sizeof(double) * S);
-    rosenbrock_cell(m, p, dt, k + (size_t)c * m->R, atol, rtol, &w, NULL, ck_y, h + (size_t)c * max_steps, max_steps,
+    rosenbrock_cell(m, p, dt, k + (size_t)c * m->R, NULL, atol, rtol, &w, NULL, ck_y, h + (size_t)c * max_steps, max_steps,
                     &nck);
     n_steps[c] = nck;
   }

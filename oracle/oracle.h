@@ -72,6 +72,14 @@ typedef double (*om_exchange_fn)(double shard_sum, void* user);
 int om_solve_global(const om_mech* m, const micmb_rosenbrock_params* p, int n, double dt, const double* k,
                     const double* atol, double rtol, double* y, int64_t* stats_out, int n_shards,
                     const int* shard_start, om_exchange_fn exchange, void* user, int64_t total_cells);
+/* Algebraic constraints: K_eq(T) of every equilibrium constraint per cell
+ * ([cell][n_eq], Van't Hoff with the handle's exp), and the per-cell solve
+ * with those values (keq may be NULL without equilibrium constraints). */
+void om_constraint_params(const om_mech* m, int n, const double* T, double* keq);
+int om_n_eq(const om_mech* m);
+int om_solve_per_cell_keq(const om_mech* m, const micmb_rosenbrock_params* p, int n, double dt, const double* k,
+                          const double* keq, const double* atol, double rtol, double* y, int64_t* stats_out,
+                          int n_threads);
 /* 0 (default): exp, pow and log10 of the rate constants and the step-size
  * factor from the C library, as micm calls them; 1: correctly rounded (quad
  * precision).  om_math_eval evaluates exp (0), log10 (1) or pow (2)

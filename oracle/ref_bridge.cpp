@@ -18,6 +18,9 @@
 // after the type sort); the permutation getters map system order to it.
 
 #include <micm/CPU.hpp>
+#include <micm/constraint/constraint.hpp>
+#include <micm/constraint/types/equilibrium_constraint.hpp>
+#include <micm/constraint/types/linear_constraint.hpp>
 #include <micm/solver/solver_builder.hpp>
 
 #include "../include/micmb.h"
@@ -76,6 +79,14 @@ namespace
     int n_species = 0;
     int n_reactions = 0;
     std::vector<int> sorted_position;  // input reaction -> rate column
+    // algebraic constraints as the description gives them
+    struct ConstraintSpec
+    {
+      int kind = 0, species = 0, n_react = 0;
+      std::vector<std::pair<int, double>> terms;
+      double p[4] = { 0, 0, 0, 0 };
+    };
+    std::vector<ConstraintSpec> constraints;
   };
 
   std::string SpeciesName(int i)
@@ -208,7 +219,49 @@ namespace
     b.sorted_position.assign(d->n_reactions, 0);
     for (int i = 0; i < d->n_reactions; ++i)
       b.sorted_position[order[i]] = i;
+    for (int c = 0; c < d->n_constraints; ++c)
+    {
+      Built::ConstraintSpec cs;
+      cs.kind = d->constraint_type[c];
+      cs.species = d->constraint_species[c];
+      cs.n_react = d->constraint_n_reactants ? d->constraint_n_reactants[c] : 0;
+      for (int t = d->constraint_term_start[c]; t < d->constraint_term_start[c + 1]; ++t)
+        cs.terms.push_back({ d->constraint_term_species[t], d->constraint_term_coef[t] });
+      for (int i = 0; i < 4; ++i)
+        cs.p[i] = d->constraint_params[4 * c + i];
+      b.constraints.push_back(cs);
+    }
     return b;
+  }
+
+  // micm's constraint objects (linear_constraint.hpp:150-160,
+  // equilibrium_constraint.hpp:208-220) for matrices of vector length L
+  template<std::size_t L>
+  std::vector<micm::Constraint<DenseL<L>, SparseL<L>>> MakeConstraints(const Built& b)
+  {
+    std::vector<micm::Constraint<DenseL<L>, SparseL<L>>> out;
+    for (std::size_t c = 0; c < b.constraints.size(); ++c)
+    {
+      const auto& cs = b.constraints[c];
+      const std::string name = "c" + std::to_string(c);
+      std::vector<micm::StoichSpecies> terms;
+      for (const auto& t : cs.terms)
+        terms.emplace_back(b.species[t.first], t.second);
+      if (cs.kind == MICMB_CONSTRAINT_LINEAR)
+        out.emplace_back(micm::LinearConstraint<DenseL<L>, SparseL<L>>(name, b.species[cs.species], terms, cs.p[0]));
+      else
+      {
+        std::vector<micm::StoichSpecies> re(terms.begin(), terms.begin() + cs.n_react);
+        std::vector<micm::StoichSpecies> pr(terms.begin() + cs.n_react, terms.end());
+        typename micm::EquilibriumConstraint<DenseL<L>, SparseL<L>>::VantHoffParam vh{};
+        vh.K_HLC_ref_ = cs.p[0];
+        vh.delta_H_ = cs.p[1];
+        vh.R_ = cs.p[2];
+        vh.T_ref_ = cs.p[3];
+        out.emplace_back(micm::EquilibriumConstraint<DenseL<L>, SparseL<L>>(name, b.species[cs.species], re, pr, vh));
+      }
+    }
+    return out;
   }
 
   struct Handle
@@ -227,12 +280,11 @@ namespace
   template<std::size_t L>
   SolverL<L> MakeSolver(Handle& h)
   {
-    return BuilderL<L>(h.params)
-        .SetSystem(h.built.system)
-        .SetReactions(h.built.processes)
-        .SetReorderState(h.reorder)
-        .SetIgnoreUnusedSpecies(true)
-        .Build();
+    auto builder = BuilderL<L>(h.params);
+    builder.SetSystem(h.built.system).SetReactions(h.built.processes).SetReorderState(h.reorder).SetIgnoreUnusedSpecies(true);
+    if (!h.built.constraints.empty())
+      builder.SetConstraints(MakeConstraints<L>(h.built));
+    return builder.Build();
   }
 
   template<class State>
@@ -260,6 +312,7 @@ namespace
     out[7] = (int64_t)r.state_;
     double ft = r.stats_.final_time_;
     std::memcpy(&out[8], &ft, sizeof(double));
+    out[9] = (int64_t)r.stats_.constraint_init_iterations_;
   }
 
 #define GUARD_BEGIN \
@@ -301,7 +354,12 @@ extern "C"
       h->species_column.resize(d->n_species);
       for (int i = 0; i < d->n_species; ++i)
         h->species_column[i] = (int)state.variable_map_.at(SpeciesName(i));
-      h->n_params = (int)state.custom_rate_parameter_map_.size();
+      // user parameters only: micm appends one K_eq parameter per equilibrium
+      // constraint, which UpdateStateParameters fills from the temperature
+      int n_eq = 0;
+      for (const auto& cs : h->built.constraints)
+        n_eq += cs.kind == MICMB_CONSTRAINT_EQUILIBRIUM ? 1 : 0;
+      h->n_params = (int)state.custom_rate_parameter_map_.size() - n_eq;
       h->param_column.assign(d->n_reactions, -1);
       for (int r = 0; r < d->n_reactions; ++r)
       {
@@ -589,6 +647,7 @@ extern "C"
               acc[q] += one[q];
             acc[7] = one[7];
             acc[8] = one[8];
+            acc[9] += one[9];
           }
           for (int c = 0; c < count; ++c)
             for (int j = 0; j < S; ++j)
@@ -713,6 +772,7 @@ extern "C"
               acc[q] += one[q];
             acc[7] = one[7];
             acc[8] = one[8];
+            acc[9] += one[9];
           }
           for (int j = 0; j < S; ++j)
             y_inout[(size_t)c * S + j] = state.variables_[0][j];

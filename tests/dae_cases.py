@@ -1,0 +1,88 @@
+"""DAE test problems shaped after micm's constraint integration tests
+(test/integration/test_linear_constraint.cpp,
+test/integration/test_equilibrium_constraint.cpp): mechanisms, inputs and the
+driver that advances one state over a sequence of output times the way those
+tests do (Solve(time_step - advanced) until the output time is reached)."""
+import numpy as np
+
+from micm_b200.mechanism import (Mechanism, arrhenius, equilibrium_constraint, ideal_air_density, linear_constraint,
+                                 user_defined)
+
+
+def terminator_robertson():
+    """Cl2 -> 2 Cl, Cl + Cl -> Cl2 and Robertson's A, B, C with the linear
+    constraint A + B + C = 1 replacing C's row."""
+    atol = np.array([1e-20, 1e-20, 1e-3, 1e-3, 1e-3])
+    m = Mechanism(species=["Cl2", "Cl", "A", "B", "C"], reactions=[], name="terminator_robertson",
+                  reorder_state=False, absolute_tolerance=atol, relative_tolerance=1e-8)
+    m.add(user_defined("terminator_k1"), [0], [(1, 2.0)])
+    m.add(arrhenius(A=1.0), [1, 1], [(0, 1.0)])
+    m.add(user_defined("robertson_r1"), [2], [(3, 1.0)])
+    m.add(user_defined("robertson_r2"), [3, 3], [(3, 1.0), (4, 1.0)])
+    m.add(user_defined("robertson_r3"), [3, 4], [(2, 1.0), (4, 1.0)])
+    m.constraints.append(linear_constraint(4, [(2, 1.0), (3, 1.0), (4, 1.0)], 1.0, name="mass_conservation"))
+    return m
+
+
+def terminator_robertson_inputs(n=1):
+    T = np.full(n, 298.0)
+    P = np.full(n, 101300.0)
+    y = np.tile([1.8e-10, 1.2e-6, 1.0, 0.0, 0.0], (n, 1))
+    y[:, 1] *= np.linspace(1.0, 2.0, n)
+    # custom parameters in micm's order: terminator_k1, robertson_r1, r2, r3
+    params = np.tile([1.0e-4, 0.04, 3.0e7, 1.0e4], (n, 1))
+    return dict(temperature=T, pressure=P, air_density=np.full(n, 42.0), concentrations=y, custom_params=params)
+
+
+def equilibrium(stoich=1.0, two=False):
+    """A -> B (k = 0.1) with B <=> C in equilibrium (C algebraic); with
+    `two`, also D -> E with E <=> F.  `stoich` is B's exponent."""
+    names = ["A", "B", "C"] + (["D", "E", "F"] if two else [])
+    m = Mechanism(species=names, reactions=[], name="equilibrium", reorder_state=False,
+                  absolute_tolerance=np.full(len(names), 1e-3), relative_tolerance=1e-6)
+    m.add(arrhenius(A=0.1), [0], [(1, 1.0)])
+    m.constraints.append(equilibrium_constraint(2, [(1, stoich)], [(2, 1.0)], K_HLC_ref=0.034, delta_H=-2400.0,
+                                                name="B_C_eq"))
+    if two:
+        m.add(arrhenius(A=0.02, C=-300.0), [3], [(4, 1.0)])
+        m.constraints.append(equilibrium_constraint(5, [(4, 1.0)], [(5, 2.0)], K_HLC_ref=1.7, delta_H=1800.0,
+                                                    name="E_F_eq"))
+    return m
+
+
+def equilibrium_inputs(m, n=4, consistent=True, f0=0.0):
+    T = np.linspace(280.0, 310.0, n)
+    P = np.full(n, 101325.0)
+    S = m.n_species
+    y = np.zeros((n, S))
+    y[:, 0] = 1.0
+    y[:, 1] = 0.1
+    if S > 3:
+        y[:, 3] = 0.5
+        y[:, 4] = 0.05
+        y[:, 5] = f0
+    if consistent:
+        keq = 0.034 * np.exp((-2400.0 / (1.380649e-23 * 6.02214076e23)) * (1.0 / T - 1.0 / 298.15))
+        y[:, 2] = keq * y[:, 1] ** m.constraints[0].terms[0][1]
+    return dict(temperature=T, pressure=P, air_density=ideal_air_density(P, T), concentrations=y,
+                custom_params=np.zeros((n, 0)))
+
+
+def advance(solve, inputs, output_times):
+    """Advance every cell to each output time by repeated solves of the rest of
+    the interval; yields (y, per-call stats) per output time.  `solve(inputs,
+    dt)` returns (y [n, S], stats rows [n, 10])."""
+    t = 0.0
+    for target in output_times:
+        advanced = 0.0
+        calls = []
+        while advanced < target - t:
+            y, st = solve(inputs, (target - t) - advanced)
+            calls.append(st)
+            inputs = dict(inputs, concentrations=y)
+            ft = st[:, 8:9].view(np.float64)[:, 0]
+            if not np.all(ft == ft[0]) or ft[0] <= 0.0:
+                raise AssertionError("cells advanced unevenly or not at all")
+            advanced += ft[0]
+        t = target
+        yield inputs["concentrations"], calls

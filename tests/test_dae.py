@@ -1,0 +1,52 @@
+"""Algebraic constraints (DAE form): micm's Rosenbrock with linear and
+equilibrium constraints (include/micm/constraint/**, rosenbrock.inl:12-304 and
+InitializeConstraints :407-576), restated in the C oracle and pinned bit for
+bit against micm itself (oracle/_ref, micm's constraint classes through
+SolverBuilder::SetConstraints), on problems shaped after micm's
+test/integration/test_linear_constraint.cpp and test_equilibrium_constraint.cpp:
+every solve's final concentrations and statistics (constraint-initialisation
+iterations included) are identical."""
+import numpy as np
+import pytest
+
+import oracle
+from dae_cases import equilibrium, equilibrium_inputs, terminator_robertson, terminator_robertson_inputs
+
+pytestmark = pytest.mark.skipif(not (oracle.restatement_available() and oracle.reference_available()),
+                                reason="oracle not built")
+
+CASES = [
+    ("linear_4da", terminator_robertson, lambda m: terminator_robertson_inputs(3), 40, [1, 10, 100, 1e3, 1e4, 1e5]),
+    ("linear_6da", terminator_robertson, lambda m: terminator_robertson_inputs(2), 60, [1, 10, 100, 1e3]),
+    ("equilibrium_consistent", lambda: equilibrium(), lambda m: equilibrium_inputs(m, 4, True), 40, [1, 5, 20, 60]),
+    ("equilibrium_inconsistent_3stage", lambda: equilibrium(), lambda m: equilibrium_inputs(m, 4, False), 3,
+     [1, 5, 20]),
+    ("equilibrium_stoich2_two", lambda: equilibrium(2.0, True), lambda m: equilibrium_inputs(m, 3, False, 0.2), 40,
+     [1, 10, 50]),
+    # F = 0 with F^2 as the product: dG/dF = 0, the initialisation's matrix is
+    # singular and micm reports InfDetected
+    ("equilibrium_singular_init", lambda: equilibrium(2.0, True), lambda m: equilibrium_inputs(m, 3, False, 0.0), 40,
+     [1]),
+]
+
+
+@pytest.mark.parametrize("name,make_mech,make_inputs,tableau,outputs", CASES, ids=[c[0] for c in CASES])
+def test_restatement_equals_micm(name, make_mech, make_inputs, tableau, outputs):
+    m = make_mech()
+    inp = make_inputs(m)
+    R = oracle.Restatement(m, tableau_kind=tableau)
+    ref = oracle.Reference(m, tableau=tableau)
+    y_r, y_m = inp["concentrations"], inp["concentrations"]
+    t = 0.0
+    for target in outputs:
+        dt = target - t
+        y_r, st_r = R.solve_per_cell(dict(inp, concentrations=y_r), dt, threads=1)
+        y_m, st_m = ref.solve_per_cell(dict(inp, concentrations=y_m), dt, threads=1)
+        np.testing.assert_array_equal(y_r, y_m)
+        np.testing.assert_array_equal(st_r, st_m)
+        assert np.all(st_r[:, 7] == (7 if name == "equilibrium_singular_init" else 2)), st_r[:, 7]
+        t = target
+    if name.startswith("linear"):
+        np.testing.assert_allclose(y_r[:, 2] + y_r[:, 3] + y_r[:, 4], 1.0, rtol=0, atol=1e-10)
+    if "inconsistent" in name or "two" in name:
+        assert st_r[:, 9].max() >= 1  # the initialisation iterated
