@@ -178,6 +178,7 @@ typedef struct micmb_solver_stats {
   double final_time;
   int32_t state; /* MICMB_SOLVER_*: worst over cells in per-cell mode */
   int32_t cells_not_converged;
+  int64_t constraint_init_iterations; /* DAE: Newton iterations of the constraint initialisation */
 } micmb_solver_stats;
 
 typedef struct micmb_mechanism_info {

@@ -72,6 +72,7 @@ class SolverStats(C.Structure):
         ("final_time", C.c_double),
         ("state", C.c_int32),
         ("cells_not_converged", C.c_int32),
+        ("constraint_init_iterations", C.c_int64),
     ]
 
     def as_dict(self) -> Dict[str, float]:

@@ -648,6 +648,8 @@ namespace micmb
         !(params.small >= 0.0) || !(params.h_start >= 0.0))
       throw Error(MICMB_ERR_INVALID_ARGUMENT,
                   "Backward Euler parameters: max_number_of_steps >= 1, 0..8 reductions, small and h_start >= 0");
+    if (!s.mech->constraints.empty())
+      throw Error(MICMB_ERR_UNSUPPORTED, "Backward Euler takes no algebraic constraints (micm's applies none)");
     const BeParams P = ToDevice(params);
     if (step_control == MICMB_STEP_GLOBAL)
       SolveBackwardEulerGlobal(s, st, dt, P, stats, per_cell_status, per_cell_accepted);

@@ -83,6 +83,8 @@ namespace micmb
     }
     d.inv_order = 1 / p.estimator_of_local_order;
     d.gamma0 = p.gamma[0];
+    d.cinit_max_iter = p.constraint_init_max_iterations;
+    d.cinit_tol = p.constraint_init_tolerance;
     return d;
   }
 
@@ -229,6 +231,18 @@ namespace micmb
                          bws = AddSchedule(pk, m.bwd_serial), fwts = AddSchedule(pk, m.fwd_t_serial),
                          bwts = AddSchedule(pk, m.bwd_t_serial);
       const size_t o_rd = pk.add(m.rate_desc), o_drd = pk.add(m.drate_desc);
+      // algebraic constraints
+      std::vector<int32_t> con4, con2;
+      std::vector<double> conp;
+      for (const auto& cd : m.constraints)
+      {
+        con4.insert(con4.end(), { cd.kind, cd.row, cd.t0, cd.t1 });
+        con2.insert(con2.end(), { cd.n_react, cd.keq });
+        conp.insert(conp.end(), cd.p, cd.p + 4);
+      }
+      const size_t o_con = pk.add(con4), o_con2 = pk.add(con2), o_conp = pk.add(conp);
+      const size_t o_ctc = pk.add(m.c_term_col), o_ctf = pk.add(m.c_term_coef), o_mass = pk.add(m.mass);
+      const size_t o_cjs = pk.add(m.cj_start), o_cjt = pk.add(m.cj_term);
       BlockedOffsets blu{}, bfw{}, bbw{};
       if (m.has_blocked)
       {
@@ -309,6 +323,17 @@ namespace micmb
       // re-reads they remove hit L1, and their accesses spread over more DRAM pages)
       const char* blk = std::getenv("MICMB_BLOCKED_SCHEDULES");
       d.has_blocked = (m.has_blocked && blk && blk[0] == '1') ? 1 : 0;
+      d.n_constraints = (int32_t)m.constraints.size();
+      d.n_eq = m.n_eq;
+      d.n_cterms = (int32_t)m.c_term_col.size();
+      d.con = reinterpret_cast<const int4*>(b + o_con);
+      d.con_eq = reinterpret_cast<const int2*>(b + o_con2);
+      d.con_p = reinterpret_cast<const double*>(b + o_conp);
+      d.ct_col = reinterpret_cast<const int32_t*>(b + o_ctc);
+      d.ct_coef = reinterpret_cast<const double*>(b + o_ctf);
+      d.mass = reinterpret_cast<const double*>(b + o_mass);
+      d.cj_start = reinterpret_cast<const int32_t*>(b + o_cjs);
+      d.cj_term = reinterpret_cast<const int32_t*>(b + o_cjt);
       if (m.has_blocked)
       {
         d.lu_b = ResolveBlocked(b, blu);
@@ -765,6 +790,7 @@ extern "C"
       st->variables = DeviceMemory(st->dense_bytes(m.S));
       st->custom_params = DeviceMemory(st->dense_bytes(std::max<int32_t>(m.P, 1)));
       st->rate_constants = DeviceMemory(st->dense_bytes(std::max<int32_t>(m.R, 1)));
+      st->keq = DeviceMemory(st->dense_bytes(std::max<int32_t>(m.n_eq, 1)));
       st->conditions = DeviceMemory(st->dense_bytes(3));
       st->atol = DeviceMemory(sizeof(double) * m.S);
       st->counters = DeviceMemory(256);

@@ -88,6 +88,16 @@ namespace micmb
     DevSchedule lu_s, fwd_s, bwd_s, fwd_t_s, bwd_t_s;  // serial forms (one thread per cell)
     int32_t has_blocked;                                // register-blocked serial forms present
     DevBlocked lu_b, fwd_b, bwd_b;
+    // algebraic constraints (n_constraints = 0 for an ODE mechanism)
+    int32_t n_constraints, n_eq, n_cterms;
+    const int4* con;           // {kind, row, t0, t1}
+    const int2* con_eq;        // {n_react, K_eq index}
+    const double* con_p;       // [n_constraints * 4]
+    const int32_t* ct_col;     // term state columns
+    const double* ct_coef;     // coefficient / stoichiometry
+    const double* mass;        // [S] mass-matrix diagonal
+    const int32_t* cj_start;   // [nnz + 1] constraint terms received by each LU position
+    const int32_t* cj_term;
     // warp-interleaved tables (fused kernel); dummy slots: LU[nnz], x[S], scratch[scratch_zero]
     int32_t has_warp;
     int32_t scratch_zero;
@@ -107,6 +117,8 @@ namespace micmb
     int32_t new_f[6];
     double inv_order;  // 1 / estimator_of_local_order
     double a[15], c[15], m[6], e[6], gamma0;
+    int32_t cinit_max_iter;  // DAE constraint initialisation
+    double cinit_tol;
   };
 
   // column accessor with a runtime stride (global vector layout) or unit stride (shared)
@@ -266,6 +278,91 @@ namespace micmb
   }
 
   // ---------------------------------------------------------------------
+  // algebraic constraints, one cell (linear_constraint.hpp:216-290,
+  // equilibrium_constraint.hpp:290-580): keq holds the cell's K_eq values
+  // ---------------------------------------------------------------------
+  __device__ __forceinline__ double con_pow(double c, double e)
+  {
+    return cr_pow(c > 0.0 ? c : 0.0, e);
+  }
+
+  // f[row] = G(y) for every constraint: the residual overwrites the algebraic row
+  template<class KV, class YV, class FV>
+  __device__ __forceinline__ void constraint_forcing(const DevMech& M, KV keq, YV y, FV f)
+  {
+    for (int32_t c = 0; c < M.n_constraints; ++c)
+    {
+      const int4 cd = M.con[c];
+      if (cd.x == MICMB_CONSTRAINT_LINEAR)
+      {
+        double sum = 0.0;
+        for (int32_t t = cd.z; t < cd.w; ++t)
+          sum += M.ct_coef[t] * y[M.ct_col[t]];
+        f[cd.y] = sum - M.con_p[4 * c];
+      }
+      else
+      {
+        const int2 eq = M.con_eq[c];
+        double rp = keq[eq.y], pp = 1.0;
+        const int32_t tr = cd.z + eq.x;
+        for (int32_t t = cd.z; t < tr; ++t)
+          rp *= con_pow(y[M.ct_col[t]], M.ct_coef[t]);
+        for (int32_t t = tr; t < cd.w; ++t)
+          pp *= con_pow(y[M.ct_col[t]], M.ct_coef[t]);
+        f[cd.y] = rp - pp;
+      }
+    }
+  }
+
+  // cj[t] = what the Jacobian entry of constraint term t loses (jac -= cj[t]):
+  // the coefficient (linear), dG/dy (equilibrium reactant) or -dG/dy
+  // (equilibrium product, which micm adds: jac - (-p) == jac + p exactly)
+  template<class KV, class YV, class CV>
+  __device__ __forceinline__ void constraint_jacobian(const DevMech& M, KV keq, YV y, CV cj)
+  {
+    for (int32_t c = 0; c < M.n_constraints; ++c)
+    {
+      const int4 cd = M.con[c];
+      if (cd.x == MICMB_CONSTRAINT_LINEAR)
+      {
+        for (int32_t t = cd.z; t < cd.w; ++t)
+          cj[t] = M.ct_coef[t];
+        continue;
+      }
+      const int2 eq = M.con_eq[c];
+      const int32_t tr = cd.z + eq.x;
+      const double K = keq[eq.y];
+      for (int side = 0; side < 2; ++side)
+      {
+        const int32_t a = side ? tr : cd.z, b = side ? cd.w : tr;
+        for (int32_t i = a; i < b; ++i)
+        {
+          double prod = side ? 1.0 : K;
+          for (int32_t j = a; j < b; ++j)
+            if (j != i)
+              prod *= con_pow(y[M.ct_col[j]], M.ct_coef[j]);
+          const double conc = y[M.ct_col[i]], st = M.ct_coef[i];
+          double partial;
+          if (st == 1.0)
+            partial = prod;
+          else if (conc > 0.0)
+            partial = st * prod * cr_pow(conc, st - 1.0);
+          else
+            partial = 0.0;
+          cj[i] = side ? -partial : partial;
+        }
+      }
+    }
+  }
+
+  // K_eq(T) of every equilibrium constraint (Van't Hoff), in constraint order
+  __device__ __forceinline__ double constraint_keq(const DevMech& M, int32_t c, double T)
+  {
+    const double* q = M.con_p + 4 * c;
+    return q[0] * cr_exp((q[1] / q[2]) * (1.0 / T - 1.0 / q[3]));
+  }
+
+  // ---------------------------------------------------------------------
   // -J + alpha I: d_rate per info, then gather per nonzero
   // ---------------------------------------------------------------------
   template<int NL, class KV, class YV, class DV>
@@ -280,20 +377,31 @@ namespace micmb
     }
   }
 
-  // jac[e] = sum_terms coef * drate (+ alpha on the diagonal when add_alpha)
-  template<int NL, class DV, class JV>
+  // jac[e] = sum_terms coef * drate, minus its constraint terms cj (algebraic
+  // rows), plus alpha times the mass-matrix diagonal when add_alpha
+  template<int NL, class DV, class JV, class CV>
   __device__ __forceinline__ void jacobian_gather(const DevMech& M, DV drate, JV jac, double alpha, bool add_alpha,
-                                                  int lane)
+                                                  int lane, CV cj)
   {
     for (int32_t e = lane; e < M.nnz; e += NL)
     {
       double acc = 0.0;
       for (int32_t t = M.j_start[e]; t < M.j_start[e + 1]; ++t)
         acc += M.j_coef[t] * drate[M.j_info[t]];
-      if (add_alpha && M.diag_row_of[e] >= 0)
-        acc += alpha;
+      if (M.n_constraints)
+        for (int32_t t = M.cj_start[e]; t < M.cj_start[e + 1]; ++t)
+          acc -= cj[M.cj_term[t]];
+      const int32_t dr = M.diag_row_of[e];
+      if (add_alpha && dr >= 0)
+        acc += M.n_constraints ? alpha * M.mass[dr] : alpha;
       jac[e] = acc;
     }
+  }
+  template<int NL, class DV, class JV>
+  __device__ __forceinline__ void jacobian_gather(const DevMech& M, DV drate, JV jac, double alpha, bool add_alpha,
+                                                  int lane)
+  {
+    jacobian_gather<NL>(M, drate, jac, alpha, add_alpha, lane, drate);
   }
 
   // ---------------------------------------------------------------------
@@ -330,9 +438,14 @@ namespace micmb
   // the gathered sum, then + alpha on the diagonal -- instead of reading it
   // back, so the Jacobian never makes a round trip through memory.  Same
   // operations in the same order as the two passes.
-  template<class DV, class AV, class IV>
+  // With constraints, each entry also loses its constraint terms cj (micm
+  // subtracts the constraints' derivatives after the processes'), and the
+  // diagonal gains alpha times the mass-matrix diagonal.  PROCESS = false
+  // leaves the process gather out (the constraint initialisation's matrix).
+  template<bool PROCESS = true, class DV, class AV, class IV, class CV>
   __device__ __forceinline__ void lu_decompose_gathered(const DevMech& M, const DevSchedule& sch,
-                                                        const int32_t* diag_row, DV drate, double alpha, AV A, IV inv)
+                                                        const int32_t* diag_row, DV drate, double alpha, AV A, IV inv,
+                                                        CV cj)
   {
     for (int32_t l = 0; l < sch.n_levels; ++l)
     {
@@ -341,11 +454,15 @@ namespace micmb
       {
         const int32_t e = sch.target[it];
         double v = 0.0;
-        for (int32_t t = M.j_start[e]; t < M.j_start[e + 1]; ++t)
-          v += M.j_coef[t] * drate[M.j_info[t]];
+        if constexpr (PROCESS)
+          for (int32_t t = M.j_start[e]; t < M.j_start[e + 1]; ++t)
+            v += M.j_coef[t] * drate[M.j_info[t]];
+        if (M.n_constraints)
+          for (int32_t t = M.cj_start[e]; t < M.cj_start[e + 1]; ++t)
+            v -= cj[M.cj_term[t]];
         const int32_t dr = diag_row[e];
         if (dr >= 0)
-          v += alpha;
+          v += M.n_constraints ? alpha * M.mass[dr] : alpha;
         for (int32_t t = sch.term_start[it]; t < sch.term_start[it + 1]; ++t)
           v -= A[sch.ta[t]] * A[sch.tb[t]];
         const int32_t aux = sch.aux[it];
@@ -494,8 +611,8 @@ namespace micmb
 
   // The one-thread-per-cell LU and solves: blocked when the mechanism has
   // the blocked forms, else the serial schedules.
-  template<class DV, class AV, class IV>
-  __device__ __forceinline__ void thread_lu_gathered(const DevMech& M, DV drate, double alpha, AV A, IV inv);
+  template<class DV, class AV, class IV, class CV>
+  __device__ __forceinline__ void thread_lu_gathered(const DevMech& M, DV drate, double alpha, AV A, IV inv, CV cj);
   template<class AV, class XV>
   __device__ __forceinline__ void thread_solve(const DevMech& M, AV A, XV x);
 
@@ -538,13 +655,18 @@ namespace micmb
     }
   }
 
+  template<class DV, class AV, class IV, class CV>
+  __device__ __forceinline__ void thread_lu_gathered(const DevMech& M, DV drate, double alpha, AV A, IV inv, CV cj)
+  {
+    if (M.has_blocked && !M.n_constraints)
+      lu_blocked<true>(M, M.lu_b, drate, alpha, A, inv);
+    else
+      lu_decompose_gathered(M, M.lu_s, M.diag_row_of, drate, alpha, A, inv, cj);
+  }
   template<class DV, class AV, class IV>
   __device__ __forceinline__ void thread_lu_gathered(const DevMech& M, DV drate, double alpha, AV A, IV inv)
   {
-    if (M.has_blocked)
-      lu_blocked<true>(M, M.lu_b, drate, alpha, A, inv);
-    else
-      lu_decompose_gathered(M, M.lu_s, M.diag_row_of, drate, alpha, A, inv);
+    thread_lu_gathered(M, drate, alpha, A, inv, drate);
   }
 
   template<class AV, class IV>
@@ -745,6 +867,7 @@ namespace micmb
     int32_t state;  // MICMB_SOLVER_*
     int32_t new_step;
     int32_t function_calls, jacobian_updates, number_of_steps, accepted, rejected, decompositions, solves;
+    int32_t init_iterations;  // DAE constraint initialisation
   };
 
   struct StepBounds
@@ -776,6 +899,7 @@ namespace micmb
     c.new_step = 1;
     c.function_calls = c.jacobian_updates = c.number_of_steps = 0;
     c.accepted = c.rejected = c.decompositions = c.solves = 0;
+    c.init_iterations = 0;
   }
 
   // Top of micm's outer loop: returns false (and sets state) when the cell is done.
@@ -846,5 +970,66 @@ namespace micmb
     c.jacobian_updates += 1;
     c.new_step = 0;
     return 0;
+  }
+
+  // ---------------------------------------------------------------------
+  // InitializeConstraints for one cell (rosenbrock.inl:407-576): Newton on the
+  // algebraic variables until max |G| over the algebraic rows is below the
+  // tolerance.  delta (S), A (the LU), inv (S) and cj (constraint terms) are
+  // the cell's scratch.  Returns MICMB_SOLVER_CONVERGED or the failure state
+  // and counts into the cell's statistics.
+  // ---------------------------------------------------------------------
+  template<class KV, class YV, class DV, class AV, class IV, class CV>
+  __device__ __forceinline__ int32_t constraint_init_cell(const DevMech& M, const DevParams& P, KV keq, YV y,
+                                                          DV delta, AV A, IV inv, CV cj, CellCtl& c)
+  {
+    const int32_t S = M.S;
+    for (int32_t iter = 0; iter < P.cinit_max_iter; ++iter)
+    {
+      for (int32_t i = 0; i < S; ++i)
+        delta[i] = 0.0;
+      constraint_forcing(M, keq, y, delta);
+      double max_res = 0.0;
+      bool any_nan = false, any_inf = false;
+      for (int32_t i = 0; i < S; ++i)
+        if (M.mass[i] == 0.0)
+        {
+          const double v = delta[i];
+          any_nan = any_nan || isnan(v);
+          any_inf = any_inf || isinf(v);
+          const double a = fabs(v);
+          if (!isnan(a) && !isinf(a))
+            max_res = (max_res > a ? max_res : a);
+        }
+      if (any_nan)
+        return MICMB_SOLVER_NAN_DETECTED;
+      if (any_inf)
+        return MICMB_SOLVER_INF_DETECTED;
+      c.init_iterations = iter + 1;
+      if (max_res < P.cinit_tol)
+        return MICMB_SOLVER_CONVERGED;
+      // the constraints' -dG/dy, then alpha = 1 times the mass diagonal, then the LU
+      constraint_jacobian(M, keq, y, cj);
+      c.jacobian_updates += 1;
+      lu_decompose_gathered<false>(M, M.lu_s, M.diag_row_of, cj, 1.0, A, inv, cj);
+      c.decompositions += 1;
+      solve_lower<1>(M.fwd_s, A, delta, 0);
+      solve_upper<1>(M.bwd_s, A, delta, 0);
+      c.solves += 1;
+      for (int32_t i = 0; i < S; ++i)
+        if (M.mass[i] == 0.0)
+        {
+          const double d = delta[i];
+          any_nan = any_nan || isnan(d);
+          any_inf = any_inf || isinf(d);
+          if (!isnan(d) && !isinf(d))
+            y[i] = y[i] + d;
+        }
+      if (any_nan)
+        return MICMB_SOLVER_NAN_DETECTED;
+      if (any_inf)
+        return MICMB_SOLVER_INF_DETECTED;
+    }
+    return MICMB_SOLVER_CONSTRAINT_INITIALIZATION_FAILED;
   }
 }  // namespace micmb

@@ -312,6 +312,7 @@ namespace micmb
     }
     if (!A.rate_constants)
       A.rate_constants = st.rate_constants.as<double>();
+    A.keq = st.keq.as<double>();
     A.atol = st.atol.as<double>();
     A.rtol = st.rtol;
     char* cbase = st.counters.as<char>();
@@ -338,8 +339,16 @@ namespace micmb
       A.lu_global = st.lu_slots.as<double>();
       A.lu_slot_stride = stride;
     }
-    MICMB_CUDA(cudaMemsetAsync(cbase, 0, 128, st.stream));
-    if (n > 0)
+    MICMB_CUDA(cudaMemsetAsync(cbase, 0, 160, st.stream));
+    if (n > 0 && !m.constraints.empty())
+    {
+      // algebraic constraints: the one-cell-per-thread kernel is the fused form that has them
+      if (adj)
+        throw Error(MICMB_ERR_UNSUPPORTED, "the adjoint does not cover algebraic constraints");
+      if (!SolveFusedThread(s, st, A, dt))
+        throw Error(MICMB_ERR_UNSUPPORTED, "one-cell-per-thread kernel cannot be resident");
+    }
+    else if (n > 0)
     {
       bool done = false;
       if (s.fused.variant == 0)
@@ -357,7 +366,7 @@ namespace micmb
     }
     if (stats || per_cell_status || per_cell_accepted)
     {
-      unsigned long long hs[8];
+      unsigned long long hs[9];
       MICMB_CUDA(cudaMemcpyAsync(hs, A.stats, sizeof(hs), cudaMemcpyDeviceToHost, st.stream));
       if (per_cell_status)
         MICMB_CUDA(cudaMemcpyAsync(per_cell_status, A.cell_status, sizeof(int32_t) * n, cudaMemcpyDeviceToHost,
@@ -380,6 +389,7 @@ namespace micmb
         stats->decompositions = (int64_t)hs[5];
         stats->solves = (int64_t)hs[6];
         stats->cells_not_converged = (int32_t)hs[7];
+        stats->constraint_init_iterations = (int64_t)hs[8];
         stats->final_time = dt;
         stats->state = hs[7] ? MICMB_SOLVER_CONVERGENCE_EXCEEDED_MAX_STEPS : MICMB_SOLVER_CONVERGED;
         if (hs[7])

@@ -36,10 +36,12 @@ namespace micmb
     // entry offsets (each entry = 32 doubles, one per lane) of a thread's working set
     struct ThreadLayout
     {
-      int32_t oY, oYn, oF0, oFc, oK, oLU, oInv, oKk, oScr, per_slot;
+      int32_t oY, oYn, oF0, oFc, oK, oLU, oInv, oKk, oScr, oCj, oKeq, per_slot;
     };
 
-    ThreadLayout MakeThreadLayout(int32_t S, int32_t R, int32_t stages, int32_t n_info, int32_t nnz)
+    // oCj / oKeq: constraint Jacobian terms and K_eq values (DAE mechanisms only)
+    ThreadLayout MakeThreadLayout(int32_t S, int32_t R, int32_t stages, int32_t n_info, int32_t nnz,
+                                  int32_t n_cterms = 0, int32_t n_eq = 0)
     {
       ThreadLayout t;
       int32_t o = 0;
@@ -61,6 +63,10 @@ namespace micmb
       o += R;
       t.oScr = o;
       o += (R > n_info ? R : n_info);
+      t.oCj = o;
+      o += n_cterms;
+      t.oKeq = o;
+      o += n_eq;
       t.per_slot = o;
       return t;
     }
@@ -89,11 +95,13 @@ namespace micmb
       Strided inv{ w + (size_t)T.oInv * 32, 32 };
       Strided kk{ w + (size_t)T.oKk * 32, 32 };
       Strided scr{ w + (size_t)T.oScr * 32, 32 };
+      Strided cj{ w + (size_t)T.oCj * 32, 32 };
+      Strided kq{ w + (size_t)T.oKeq * 32, 32 };
       auto Kv = [&](int32_t st) { return Strided{ Kb + (size_t)st * S * 32, 32 }; };
 
       // solver statistics of the block's finished cells (one global atomic per block and counter)
-      __shared__ unsigned long long block_stats[8];
-      if (threadIdx.x < 8)
+      __shared__ unsigned long long block_stats[9];
+      if (threadIdx.x < 9)
         block_stats[threadIdx.x] = 0;
       __syncthreads();
       CellCtl c;
@@ -122,6 +130,8 @@ namespace micmb
         atomicAdd(block_stats + 6, (unsigned long long)c.solves);
         if (c.state != MICMB_SOLVER_CONVERGED)
           atomicAdd(block_stats + 7, 1ull);
+        if (c.init_iterations)
+          atomicAdd(block_stats + 8, (unsigned long long)c.init_iterations);
       };
       // take cells until one needs an attempt (or none are left)
       auto claim = [&]() {
@@ -141,6 +151,20 @@ namespace micmb
             kk[r] = A.rate_constants[bk + (size_t)r * L];
           ctl_init(c, B);
           n_ckpt = 0;
+          if (M.n_constraints)
+          {
+            // K_eq values, then micm's constraint initialisation of the algebraic variables
+            const size_t bq = cell_base(cell, L, M.n_eq);
+            for (int32_t q = 0; q < M.n_eq; ++q)
+              kq[q] = A.keq[bq + (size_t)q * L];
+            const int32_t st = constraint_init_cell(M, P, kq, Y, Fc, LU, inv, cj, c);
+            if (st != MICMB_SOLVER_CONVERGED)
+            {
+              c.state = st;
+              write_out();
+              continue;
+            }
+          }
           if (ctl_begin_step(c, P, B))
           {
             c.function_calls += 1;
@@ -162,11 +186,15 @@ namespace micmb
         {
           reaction_rates<1>(M, kk, Y, scr, 0);
           forcing_gather<1>(M, scr, F0, 0);
+          if (M.n_constraints)
+            constraint_forcing(M, kq, Y, F0);
         }
         const double H = c.H;
         const double alpha = 1.0 / (H * P.gamma0);
         jacobian_rates<1>(M, kk, Y, scr, 0);
-        thread_lu_gathered(M, scr, alpha, LU, inv);  // -J + alpha I, then LU
+        if (M.n_constraints)
+          constraint_jacobian(M, kq, Y, cj);
+        thread_lu_gathered(M, scr, alpha, LU, inv, cj);  // -J + alpha M, then LU
         bool fc_is_src = false;
         for (int32_t st = 0; st < P.stages; ++st)
         {
@@ -182,6 +210,8 @@ namespace micmb
             }
             reaction_rates<1>(M, kk, Yn, scr, 0);
             forcing_gather<1>(M, scr, Fc, 0);
+            if (M.n_constraints)
+              constraint_forcing(M, kq, Yn, Fc);
             fc_is_src = true;
           }
           double coh[6];
@@ -191,8 +221,9 @@ namespace micmb
           for (int32_t i = 0; i < S; ++i)
           {
             double v = fc_is_src ? Fc[i] : F0[i];
-            for (int32_t j = 0; j < st; ++j)
-              v += coh[j] * Kv(j)[i];
+            if (!M.n_constraints || M.mass[i] != 0.0)  // algebraic rows have no mass coupling
+              for (int32_t j = 0; j < st; ++j)
+                v += coh[j] * Kv(j)[i];
             Ks[i] = v;
           }
           thread_solve(M, LU, Ks);
@@ -210,6 +241,8 @@ namespace micmb
             e += P.e[st] * kv;
           }
           Yn[i] = v;
+          if (M.n_constraints && M.mass[i] == 0.0)
+            e = v - Y[i];  // SetAlgebraicErrors: the step change
           sum += scaled_sq(Y[i], v, e, A.atol[i], A.rtol);
         }
         const double error = error_from_sum(sum, (double)S);
@@ -262,7 +295,7 @@ namespace micmb
         }
       }
       __syncthreads();
-      if (threadIdx.x < 8 && block_stats[threadIdx.x])
+      if (threadIdx.x < 9 && block_stats[threadIdx.x])
         atomicAdd(A.stats + threadIdx.x, block_stats[threadIdx.x]);
     }
 
@@ -322,7 +355,8 @@ namespace micmb
   int64_t FusedThreadWorkspaceDoubles(const micmb_solver& s, int64_t n_cells)
   {
     const auto& m = *s.mech;
-    const ThreadLayout T = MakeThreadLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz);
+    const ThreadLayout T = MakeThreadLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz,
+                                            (int32_t)m.c_term_col.size(), m.n_eq);
     const int64_t threads = std::min<int64_t>(FusedThreadResidentCells(s),
                                               (n_cells + kThreadsPerBlock - 1) / kThreadsPerBlock * kThreadsPerBlock);
     return std::max<int64_t>(threads, kThreadsPerBlock) * (int64_t)T.per_slot;
@@ -331,7 +365,8 @@ namespace micmb
   bool SolveFusedThread(micmb_solver& s, micmb_state& st, const FusedArgs& A_in, double dt)
   {
     const auto& m = *s.mech;
-    const ThreadLayout T = MakeThreadLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz);
+    const ThreadLayout T = MakeThreadLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz,
+                                            (int32_t)m.c_term_col.size(), m.n_eq);
     const ThreadKernel kernel = ThreadKernelFor(s.fused);
     const int per_sm = ThreadBlocksPerSm(s);
     if (per_sm < 1)

@@ -47,7 +47,18 @@ namespace micmb
       CellCtl* ctl;
       int32_t* status;  // [n] (per-cell) or [1]
       int32_t scratch_cols;
+      const double* keq;  // K_eq per cell (equilibrium constraints)
+      double* cjac;       // constraint Jacobian terms per cell
     };
+
+    __device__ __forceinline__ Strided keq_of(const DevMech& M, const PlainArgs& a, int64_t c)
+    {
+      return Strided{ const_cast<double*>(a.keq) + cell_base(c, a.L, M.n_eq), a.L };
+    }
+    __device__ __forceinline__ Strided cjac_of(const DevMech& M, const PlainArgs& a, int64_t c)
+    {
+      return Strided{ a.cjac + cell_base(c, a.L, M.n_cterms), a.L };
+    }
 
     __device__ __forceinline__ CellCtl* ctl_of(const PlainArgs& a, int64_t c)
     {
@@ -74,6 +85,25 @@ namespace micmb
       const double* pb = params + (size_t)g * (size_t)M.P * L + l;
       auto param = [&](int32_t col) { return pb[(size_t)col * L]; };
       k[idx] = rate_constant(M, r, cb[0], cb[L], cb[2 * L], param);
+    }
+
+    // K_eq(T) per cell and equilibrium constraint (equilibrium_constraint.hpp:290-309;
+    // micm computes it in UpdateStateParameters)
+    __global__ void k_constraint_keq(DevMech M, const double* __restrict__ cond, double* __restrict__ keq,
+                                     int64_t n_pad, int32_t L)
+    {
+      const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+      const int64_t per_group = (int64_t)M.n_eq * L;
+      if (idx >= n_pad * M.n_eq)
+        return;
+      const int64_t g = idx / per_group;
+      const int64_t rem = idx - g * per_group;
+      const int32_t q = (int32_t)(rem / L);
+      const int32_t l = (int32_t)(rem - (int64_t)q * L);
+      const double T = cond[(size_t)g * 3 * L + l];
+      for (int32_t c = 0; c < M.n_constraints; ++c)
+        if (M.con[c].x == MICMB_CONSTRAINT_EQUILIBRIUM && M.con_eq[c].y == q)
+          keq[idx] = constraint_keq(M, c, T);
     }
 
     __global__ void k_init_ctl(CellCtl* ctl, int32_t* status, int64_t n, StepBounds b)
@@ -122,6 +152,8 @@ namespace micmb
       Strided f{ a.f0 + cell_base(c, L, M.S), L };
       reaction_rates<1>(M, k, y, rate, 0);
       forcing_gather<1>(M, rate, f, 0);
+      if (M.n_constraints)
+        constraint_forcing(M, keq_of(M, a, c), y, f);
     }
 
     // alpha I - J at Y for every running cell (micm re-assembles after a rejection)
@@ -138,7 +170,14 @@ namespace micmb
       Strided dr{ a.scratch + cell_base(c, L, a.scratch_cols), L };
       Strided J{ a.jac + cell_base(c, L, M.nnz), L };
       jacobian_rates<1>(M, k, y, dr, 0);
-      jacobian_gather<1>(M, dr, J, alpha, true, 0);
+      if (M.n_constraints)
+      {
+        const Strided cj = cjac_of(M, a, c);
+        constraint_jacobian(M, keq_of(M, a, c), y, cj);
+        jacobian_gather<1>(M, dr, J, alpha, true, 0, cj);
+      }
+      else
+        jacobian_gather<1>(M, dr, J, alpha, true, 0);
     }
 
     __global__ void k_decompose(DevMech M, PlainArgs a)
@@ -175,6 +214,8 @@ namespace micmb
       Strided f{ a.fcur + bs, L };
       reaction_rates<1>(M, k, yn, rate, 0);
       forcing_gather<1>(M, rate, f, 0);
+      if (M.n_constraints)
+        constraint_forcing(M, keq_of(M, a, c), yn, f);
     }
 
     // K_s = F + sum_j (c_sj / H) K_j ; K_s = (LU)^-1 K_s
@@ -196,8 +237,9 @@ namespace micmb
       for (int32_t i = 0; i < S; ++i)
       {
         double v = F[i];
-        for (int32_t j = 0; j < s; ++j)
-          v += coh[j] * a.K[bk + (size_t)(j * S + i) * L];
+        if (!M.n_constraints || M.mass[i] != 0.0)  // algebraic rows have no mass coupling
+          for (int32_t j = 0; j < s; ++j)
+            v += coh[j] * a.K[bk + (size_t)(j * S + i) * L];
         Ks[i] = v;
       }
       Strided J{ a.jac + cell_base(c, L, M.nnz), L };
@@ -225,9 +267,33 @@ namespace micmb
           e += P.e[st] * kv;
         }
         yn[i] = v;
+        if (M.n_constraints && M.mass[i] == 0.0)
+          e = v - y[i];  // SetAlgebraicErrors: the step change
         sum += scaled_sq(y[i], v, e, a.atol[i], a.rtol);
       }
       return sum;
+    }
+
+    // per-cell step control with constraints: micm's constraint initialisation of each cell
+    __global__ void k_constraint_init_per_cell(DevMech M, PlainArgs a, DevParams P)
+    {
+      const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+      if (c >= a.n)
+        return;
+      const int32_t L = a.L;
+      Strided y{ a.y + cell_base(c, L, M.S), L };
+      Strided delta{ a.f0 + cell_base(c, L, M.S), L };
+      Strided J{ a.jac + cell_base(c, L, M.nnz), L };
+      Strided inv{ a.inv + cell_base(c, L, M.S), L };
+      CellCtl cc = a.ctl[c];
+      const int32_t st = constraint_init_cell(M, P, keq_of(M, a, c), y, delta, J, inv, cjac_of(M, a, c), cc);
+      if (st != MICMB_SOLVER_CONVERGED)
+      {
+        cc.state = st;
+        cc.new_step = 0;
+        a.status[c] = st;
+      }
+      a.ctl[c] = cc;
     }
 
     __device__ __forceinline__ void count_attempt(CellCtl& cc, const DevParams& P)
@@ -384,7 +450,7 @@ namespace micmb
                                    unsigned long long* acc, int32_t* cell_status, int32_t* cell_accepted)
     {
       const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-      long long v[8] = { 0 };
+      long long v[9] = { 0 };
       if (i < n)
       {
         const CellCtl c = ctl[i];
@@ -396,13 +462,14 @@ namespace micmb
         v[5] = c.decompositions;
         v[6] = c.solves;
         v[7] = (status[i] == MICMB_SOLVER_CONVERGED) ? 0 : 1;
+        v[8] = c.init_iterations;
         if (cell_status)
           cell_status[i] = status[i];
         if (cell_accepted)
           cell_accepted[i] = c.accepted;
       }
 #pragma unroll
-      for (int q = 0; q < 8; ++q)
+      for (int q = 0; q < 9; ++q)
       {
         long long s = v[q];
         for (int off = 16; off > 0; off >>= 1)
@@ -434,6 +501,8 @@ namespace micmb
       a.ctl = st.ctl.as<CellCtl>();
       a.status = st.status.as<int32_t>();
       a.scratch_cols = std::max<int32_t>(m.R, (int32_t)m.info_rxn.size());
+      a.keq = st.keq.as<double>();
+      a.cjac = st.cjac.as<double>();
       return a;
     }
   }  // namespace
@@ -452,6 +521,8 @@ namespace micmb
       st.scratch = DeviceMemory(st.dense_bytes(std::max<int32_t>(std::max<int32_t>(m.R, (int32_t)m.info_rxn.size()), 1)));
       st.inv_diag = DeviceMemory(st.dense_bytes(S));
       st.err_cell = DeviceMemory(sizeof(double) * std::max<int64_t>(st.n_cells, 1));
+      if (!m.c_term_col.empty())
+        st.cjac = DeviceMemory(st.dense_bytes((int32_t)m.c_term_col.size()));
       MICMB_CUDA(cudaMemsetAsync(st.jacobian.p, 0, st.jacobian.bytes, st.stream));
       MICMB_CUDA(cudaMemsetAsync(st.forcing0.p, 0, st.forcing0.bytes, st.stream));
       MICMB_CUDA(cudaMemsetAsync(st.ynew.p, 0, st.ynew.bytes, st.stream));
@@ -466,12 +537,20 @@ namespace micmb
   void LaunchRateConstants(micmb_solver& s, micmb_state& st)
   {
     const int64_t total = st.n_pad * s.mech->R;
-    if (total == 0)
-      return;
-    k_rate_constants<<<Blocks(total), kBlock, 0, st.stream>>>(s.dev, st.conditions.as<double>(),
-                                                              st.custom_params.as<double>(),
-                                                              st.rate_constants.as<double>(), st.n_pad, st.L);
-    MICMB_CUDA(cudaGetLastError());
+    if (total > 0)
+    {
+      k_rate_constants<<<Blocks(total), kBlock, 0, st.stream>>>(s.dev, st.conditions.as<double>(),
+                                                                st.custom_params.as<double>(),
+                                                                st.rate_constants.as<double>(), st.n_pad, st.L);
+      MICMB_CUDA(cudaGetLastError());
+    }
+    const int64_t n_keq = st.n_pad * s.mech->n_eq;
+    if (n_keq > 0)
+    {
+      k_constraint_keq<<<Blocks(n_keq), kBlock, 0, st.stream>>>(s.dev, st.conditions.as<double>(),
+                                                                st.keq.as<double>(), st.n_pad, st.L);
+      MICMB_CUDA(cudaGetLastError());
+    }
   }
 
   void SolvePlain(micmb_solver& s, micmb_state& st, double dt, int32_t step_control, micmb_solver_stats* stats,
@@ -494,6 +573,14 @@ namespace micmb
     MICMB_CUDA(cudaGetLastError());
     if (n == 0)
       return;
+    if (!m.constraints.empty())
+    {
+      if (global)
+        throw Error(MICMB_ERR_UNSUPPORTED,
+                    "algebraic constraints are solved with per-cell step control (MICMB_STEP_PER_CELL)");
+      k_constraint_init_per_cell<<<Blocks(n), kBlock, 0, stream>>>(s.dev, a, P);
+      MICMB_CUDA(cudaGetLastError());
+    }
     // which forcing each stage's right-hand side reads (rosenbrock.inl:140-195)
     std::vector<int32_t> src_is_f0(P.stages, 1);
     {
@@ -558,10 +645,10 @@ namespace micmb
     }
     const int64_t total = st.n_pad * m.S;
     k_clamp<<<Blocks(total), kBlock, 0, stream>>>(a.y, n, st.L, m.S);
-    MICMB_CUDA(cudaMemsetAsync(dstats, 0, 8 * sizeof(unsigned long long), stream));
+    MICMB_CUDA(cudaMemsetAsync(dstats, 0, 9 * sizeof(unsigned long long), stream));
     k_reduce_stats<<<Blocks(n_ctl), kBlock, 0, stream>>>(a.ctl, a.status, n_ctl, dstats, nullptr, nullptr);
     MICMB_CUDA(cudaGetLastError());
-    unsigned long long hs[8];
+    unsigned long long hs[9];
     MICMB_CUDA(cudaMemcpyAsync(hs, dstats, sizeof(hs), cudaMemcpyDeviceToHost, stream));
     CellCtl c0{};
     if (global)
@@ -592,6 +679,7 @@ namespace micmb
       stats->decompositions = (int64_t)hs[5];
       stats->solves = (int64_t)hs[6];
       stats->cells_not_converged = global ? (hs[7] ? (int32_t)n : 0) : (int32_t)hs[7];
+      stats->constraint_init_iterations = (int64_t)hs[8];
       stats->final_time = global ? c0.t : dt;
       int32_t worst = MICMB_SOLVER_CONVERGED;
       if (global)

@@ -70,10 +70,12 @@ namespace micmb
     const double* rate_constants;
     const double* atol;
     double rtol;
+    const double* keq;           // [vector layout, n_eq columns] K_eq of the equilibrium constraints
     int32_t* next_cell;          // work-stealing counter
     int32_t* cell_status;        // [n_cells] or null
     int32_t* cell_accepted;      // [n_cells] or null
-    unsigned long long* stats;   // [8] accumulators
+    unsigned long long* stats;   // [9] accumulators (the seven counters, cells not converged,
+                                 // constraint-initialisation iterations)
     double* lu_global;           // per-warp LU slots when not staged in shared memory
     int64_t lu_slot_stride;      // doubles per slot
     // adjoint checkpoints (null for a plain forward solve)
@@ -117,6 +119,8 @@ struct micmb_state
   double rtol = 1e-6;
 
   micmb::DeviceMemory variables, custom_params, rate_constants, conditions, atol;
+  micmb::DeviceMemory keq;   // K_eq of the equilibrium constraints, vector layout (UpdateStateParameters)
+  micmb::DeviceMemory cjac;  // plain path: constraint Jacobian terms per cell
   // plain-path working set (allocated on first use)
   micmb::DeviceMemory jacobian, forcing0, fcur, ynew, stages, scratch, inv_diag, err_cell;
   micmb::DeviceMemory ctl, status, accepted;

@@ -50,3 +50,36 @@ def test_restatement_equals_micm(name, make_mech, make_inputs, tableau, outputs)
         np.testing.assert_allclose(y_r[:, 2] + y_r[:, 3] + y_r[:, 4], 1.0, rtol=0, atol=1e-10)
     if "inconsistent" in name or "two" in name:
         assert st_r[:, 9].max() >= 1  # the initialisation iterated
+
+
+@pytest.mark.parametrize("make_mech", [terminator_robertson, lambda: equilibrium(), lambda: equilibrium(2.0, True)],
+                         ids=["linear", "equilibrium", "two_equilibria"])
+def test_library_numbering_and_pattern_equal_micms(make_mech):
+    """The library's compile of a DAE mechanism: micm's species numbering, and
+    micm's Jacobian pattern with the algebraic rows' kinetic entries replaced
+    by the constraints' (solver_builder.inl:345-393), LU fill included."""
+    from micm_b200.solver import CompiledMechanism
+    m = make_mech()
+    cm = CompiledMechanism(m)
+    ref = oracle.Reference(m, tableau=40)
+    R = oracle.Restatement(m, tableau_kind=40)
+    np.testing.assert_array_equal(cm.species_columns, ref.species_columns)
+    np.testing.assert_array_equal(cm.rows, ref.rows)
+    np.testing.assert_array_equal(cm.cols, ref.cols)
+    np.testing.assert_array_equal(cm.rows, R.rows)
+    np.testing.assert_array_equal(cm.cols, R.cols)
+    assert cm.info["n_custom_params"] == ref.n_params
+
+
+def test_invalid_constraints_rejected():
+    from micm_b200._native import MicmbError
+    from micm_b200.mechanism import linear_constraint
+    from micm_b200.solver import CompiledMechanism
+    m = terminator_robertson()
+    m.constraints.append(linear_constraint(4, [(2, 1.0)], 0.5))  # C is already algebraic
+    with pytest.raises(MicmbError):
+        CompiledMechanism(m)
+    m = terminator_robertson()
+    m.constraints[0].terms.append((9, 1.0))  # no such species
+    with pytest.raises(MicmbError):
+        CompiledMechanism(m)
