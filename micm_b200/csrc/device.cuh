@@ -972,6 +972,16 @@ namespace micmb
     return 0;
   }
 
+  // Solver::PostSolveClamp (solver.hpp:275-297): std::max(y, 0) on every
+  // variable; with constraints only the ODE variables, by (y > 0 ? y : 0), and
+  // the algebraic ones are left as solved.
+  __device__ __forceinline__ double post_clamp(const DevMech& M, int32_t i, double v)
+  {
+    if (!M.n_constraints)
+      return (v < 0.0) ? 0.0 : v;
+    return M.mass[i] > 0.0 ? (v > 0.0 ? v : 0.0) : v;
+  }
+
   // ---------------------------------------------------------------------
   // InitializeConstraints for one cell (rosenbrock.inl:407-576): Newton on the
   // algebraic variables until max |G| over the algebraic rows is below the

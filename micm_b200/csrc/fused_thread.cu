@@ -114,8 +114,7 @@ namespace micmb
         const size_t by = cell_base(cell, L, S);
         for (int32_t i = 0; i < S; ++i)
         {
-          const double v = Y[i];
-          A.variables_out[by + (size_t)i * L] = (v < 0.0) ? 0.0 : v;
+          A.variables_out[by + (size_t)i * L] = post_clamp(M, i, Y[i]);
         }
         if (A.cell_status)
           A.cell_status[cell] = c.state;

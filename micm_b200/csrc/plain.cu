@@ -296,6 +296,179 @@ namespace micmb
       a.ctl[c] = cc;
     }
 
+    // Global step control with constraints: micm's InitializeConstraints on an
+    // n-cell State (rosenbrock.inl:407-576).  Iteration `it` has three words
+    // in `slots` (zeroed before the first): [3it] the largest finite |G| over
+    // every cell's algebraic rows (the bits of a non-negative double, so an
+    // integer atomicMax orders them), [3it+1] the residual's NaN (1) / Inf (2)
+    // flags, [3it+2] the Newton update's flags.  Every kernel replays the
+    // decisions of the iterations before its own from these words, so the
+    // grid agrees without a host round trip.
+    __device__ __forceinline__ bool cinit_continues(const unsigned long long* slots, int32_t it, double tol)
+    {
+      for (int32_t j = 0; j < it; ++j)
+        if (slots[3 * j + 1] || __longlong_as_double((long long)slots[3 * j]) < tol || slots[3 * j + 2])
+          return false;
+      return true;
+    }
+
+    __device__ __forceinline__ void warp_flags_max(unsigned long long* slot_max, unsigned long long* slot_flags,
+                                                   double v, unsigned flags)
+    {
+      for (int off = 16; off > 0; off >>= 1)
+      {
+        const double o = __shfl_xor_sync(0xffffffffu, v, off);
+        v = o > v ? o : v;
+        flags |= __shfl_xor_sync(0xffffffffu, flags, off);
+      }
+      if ((threadIdx.x & 31) == 0)
+      {
+        if (slot_max && v > 0.0)
+          atomicMax(slot_max, (unsigned long long)__double_as_longlong(v));
+        if (flags)
+          atomicOr(slot_flags, (unsigned long long)flags);
+      }
+    }
+
+    // G(y) per cell into f0; the grid's largest finite |G| and flags
+    __global__ void k_cinit_residual(DevMech M, PlainArgs a, DevParams P, unsigned long long* slots, int32_t it)
+    {
+      if (!cinit_continues(slots, it, P.cinit_tol))
+        return;  // uniform over the grid
+      const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+      double max_res = 0.0;
+      unsigned flags = 0;
+      if (c < a.n)
+      {
+        const int32_t L = a.L;
+        Strided y{ a.y + cell_base(c, L, M.S), L };
+        Strided delta{ a.f0 + cell_base(c, L, M.S), L };
+        for (int32_t i = 0; i < M.S; ++i)
+          delta[i] = 0.0;
+        constraint_forcing(M, keq_of(M, a, c), y, delta);
+        for (int32_t i = 0; i < M.S; ++i)
+          if (M.mass[i] == 0.0)
+          {
+            const double v = delta[i];
+            flags |= isnan(v) ? 1u : (isinf(v) ? 2u : 0u);
+            const double av = fabs(v);
+            if (!isnan(av) && !isinf(av))
+              max_res = (max_res > av ? max_res : av);
+          }
+      }
+      warp_flags_max(slots + 3 * it, slots + 3 * it + 1, max_res, flags);
+    }
+
+    // the Newton update of every cell when iteration `it` neither stopped nor converged
+    __global__ void k_cinit_update(DevMech M, PlainArgs a, DevParams P, unsigned long long* slots, int32_t it)
+    {
+      if (!cinit_continues(slots, it, P.cinit_tol) || slots[3 * it + 1] ||
+          __longlong_as_double((long long)slots[3 * it]) < P.cinit_tol)
+        return;  // uniform over the grid
+      const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+      unsigned flags = 0;
+      if (c < a.n)
+      {
+        const int32_t L = a.L;
+        Strided y{ a.y + cell_base(c, L, M.S), L };
+        Strided delta{ a.f0 + cell_base(c, L, M.S), L };
+        Strided A{ a.jac + cell_base(c, L, M.nnz), L };
+        Strided inv{ a.inv + cell_base(c, L, M.S), L };
+        const Strided cj = cjac_of(M, a, c);
+        constraint_jacobian(M, keq_of(M, a, c), y, cj);
+        lu_decompose_gathered<false>(M, M.lu_s, M.diag_row_of, cj, 1.0, A, inv, cj);
+        solve_lower<1>(M.fwd_s, A, delta, 0);
+        solve_upper<1>(M.bwd_s, A, delta, 0);
+        for (int32_t i = 0; i < M.S; ++i)
+          if (M.mass[i] == 0.0)
+          {
+            const double d = delta[i];
+            flags |= isnan(d) ? 1u : (isinf(d) ? 2u : 0u);
+            if (!isnan(d) && !isinf(d))
+              y[i] = y[i] + d;
+          }
+      }
+      warp_flags_max(nullptr, slots + 3 * it + 2, 0.0, flags);
+    }
+
+    // Several ranks: word `w` of iteration `it` encoded for the all-gather (NaN,
+    // +Inf, else the maximum; the update's word carries flags only) ...
+    __global__ void k_cinit_encode(const unsigned long long* slots, int32_t it, int32_t w, double* out)
+    {
+      const unsigned long long f = slots[3 * it + w];
+      const double mx = (w == 1) ? __longlong_as_double((long long)slots[3 * it]) : 0.0;
+      *out = (f & 1u) ? __longlong_as_double(0x7ff8000000000000LL)
+                      : ((f & 2u) ? __longlong_as_double(0x7ff0000000000000LL) : mx);
+    }
+
+    // ... and the ranks' values combined in rank order (NaN first, then +Inf,
+    // else the largest) back into the words, so every rank decides alike.
+    __global__ void k_cinit_decode(unsigned long long* slots, int32_t it, int32_t w, const double* gathered,
+                                   int32_t world)
+    {
+      double v = 0.0;
+      for (int32_t r = 0; r < world; ++r)
+      {
+        const double g = gathered[r];
+        if (isnan(v) || isnan(g))
+          v = __longlong_as_double(0x7ff8000000000000LL);
+        else if (isinf(v) || isinf(g))
+          v = __longlong_as_double(0x7ff0000000000000LL);
+        else
+          v = g > v ? g : v;
+      }
+      slots[3 * it + w] = isnan(v) ? 1ull : (isinf(v) ? 2ull : 0ull);
+      if (w == 1)
+        slots[3 * it] = (isnan(v) || isinf(v)) ? 0ull : (unsigned long long)__double_as_longlong(v);
+    }
+
+    // the State's outcome and counts from the words (one thread)
+    __global__ void k_cinit_finish(PlainArgs a, DevParams P, const unsigned long long* slots)
+    {
+      CellCtl cc = a.ctl[0];
+      int32_t state = MICMB_SOLVER_CONSTRAINT_INITIALIZATION_FAILED;
+      for (int32_t it = 0; it < P.cinit_max_iter; ++it)
+      {
+        const unsigned long long f = slots[3 * it + 1], u = slots[3 * it + 2];
+        if (f & 1u)
+        {
+          state = MICMB_SOLVER_NAN_DETECTED;
+          break;
+        }
+        if (f & 2u)
+        {
+          state = MICMB_SOLVER_INF_DETECTED;
+          break;
+        }
+        cc.init_iterations = it + 1;
+        if (__longlong_as_double((long long)slots[3 * it]) < P.cinit_tol)
+        {
+          state = MICMB_SOLVER_CONVERGED;
+          break;
+        }
+        cc.jacobian_updates += 1;
+        cc.decompositions += 1;
+        cc.solves += 1;
+        if (u & 1u)
+        {
+          state = MICMB_SOLVER_NAN_DETECTED;
+          break;
+        }
+        if (u & 2u)
+        {
+          state = MICMB_SOLVER_INF_DETECTED;
+          break;
+        }
+      }
+      if (state != MICMB_SOLVER_CONVERGED)
+      {
+        cc.state = state;
+        cc.new_step = 0;
+        a.status[0] = state;
+      }
+      a.ctl[0] = cc;
+    }
+
     __device__ __forceinline__ void count_attempt(CellCtl& cc, const DevParams& P)
     {
       cc.decompositions += 1;
@@ -432,17 +605,17 @@ namespace micmb
         atomicAdd(count, __popc(ballot));
     }
 
-    // y = max(y, 0) over real cells (Solver::PostSolveClamp, solver.hpp:275-297)
-    __global__ void k_clamp(double* y, int64_t n, int32_t L, int32_t S)
+    // Solver::PostSolveClamp (solver.hpp:275-297) over real cells
+    __global__ void k_clamp(DevMech M, double* y, int64_t n, int32_t L)
     {
       const int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-      const int64_t per_group = (int64_t)S * L;
+      const int64_t per_group = (int64_t)M.S * L;
       const int64_t g = idx / per_group;
       const int32_t l = (int32_t)(idx % L);
       if (g * L + l >= n)
         return;
-      const double v = y[idx];
-      y[idx] = (v < 0.0) ? 0.0 : v;
+      const int32_t i = (int32_t)((idx - g * per_group) / L);
+      y[idx] = post_clamp(M, i, y[idx]);
     }
 
     // stats reduction over per-cell controls
@@ -553,6 +726,21 @@ namespace micmb
     }
   }
 
+  namespace
+  {
+    // one word of a constraint-initialisation iteration through the state's all-gather hook
+    void ExchangeInitWord(micmb_state& st, unsigned long long* slots, int32_t it, int32_t w, cudaStream_t stream)
+    {
+      double* gx = st.gx_buf.as<double>();
+      k_cinit_encode<<<1, 1, 0, stream>>>(slots, it, w, gx);
+      MICMB_CUDA(cudaGetLastError());
+      if (st.gx_fn(gx, gx + 1, st.gx_world, stream, st.gx_user) != 0)
+        throw Error(MICMB_ERR_INTERNAL, "global step control: the all-gather of the constraint residuals failed");
+      k_cinit_decode<<<1, 1, 0, stream>>>(slots, it, w, gx + 1, st.gx_world);
+      MICMB_CUDA(cudaGetLastError());
+    }
+  }  // namespace
+
   void SolvePlain(micmb_solver& s, micmb_state& st, double dt, int32_t step_control, micmb_solver_stats* stats,
                   int32_t* per_cell_status, int32_t* per_cell_accepted)
   {
@@ -573,12 +761,31 @@ namespace micmb
     MICMB_CUDA(cudaGetLastError());
     if (n == 0)
       return;
-    if (!m.constraints.empty())
+    if (!m.constraints.empty() && !global)
     {
-      if (global)
-        throw Error(MICMB_ERR_UNSUPPORTED,
-                    "algebraic constraints are solved with per-cell step control (MICMB_STEP_PER_CELL)");
       k_constraint_init_per_cell<<<Blocks(n), kBlock, 0, stream>>>(s.dev, a, P);
+      MICMB_CUDA(cudaGetLastError());
+    }
+    else if (!m.constraints.empty())
+    {
+      const int32_t iters = std::max<int32_t>(P.cinit_max_iter, 0);
+      const size_t slot_bytes = sizeof(unsigned long long) * 3 * (size_t)std::max<int32_t>(iters, 1);
+      if (!st.cinit_slots.p || st.cinit_slots.bytes < slot_bytes)
+        st.cinit_slots = DeviceMemory(slot_bytes);
+      auto* slots = st.cinit_slots.as<unsigned long long>();
+      MICMB_CUDA(cudaMemsetAsync(slots, 0, slot_bytes, stream));
+      for (int32_t it = 0; it < iters; ++it)
+      {
+        k_cinit_residual<<<Blocks(n), kBlock, 0, stream>>>(s.dev, a, P, slots, it);
+        MICMB_CUDA(cudaGetLastError());
+        if (st.gx_fn)
+          ExchangeInitWord(st, slots, it, 1, stream);
+        k_cinit_update<<<Blocks(n), kBlock, 0, stream>>>(s.dev, a, P, slots, it);
+        MICMB_CUDA(cudaGetLastError());
+        if (st.gx_fn)
+          ExchangeInitWord(st, slots, it, 2, stream);
+      }
+      k_cinit_finish<<<1, 1, 0, stream>>>(a, P, slots);
       MICMB_CUDA(cudaGetLastError());
     }
     // which forcing each stage's right-hand side reads (rosenbrock.inl:140-195)
@@ -644,7 +851,7 @@ namespace micmb
       batch = std::min<int64_t>(batch * 2, 64);
     }
     const int64_t total = st.n_pad * m.S;
-    k_clamp<<<Blocks(total), kBlock, 0, stream>>>(a.y, n, st.L, m.S);
+    k_clamp<<<Blocks(total), kBlock, 0, stream>>>(s.dev, a.y, n, st.L);
     MICMB_CUDA(cudaMemsetAsync(dstats, 0, 9 * sizeof(unsigned long long), stream));
     k_reduce_stats<<<Blocks(n_ctl), kBlock, 0, stream>>>(a.ctl, a.status, n_ctl, dstats, nullptr, nullptr);
     MICMB_CUDA(cudaGetLastError());

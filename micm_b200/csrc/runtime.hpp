@@ -146,6 +146,7 @@ struct micmb_state
   int32_t gx_world = 1;
   int64_t gx_total_cells = 0;
   micmb::DeviceMemory gx_buf;     // [0]: this shard's sum; [1, 1 + world): the gathered sums
+  micmb::DeviceMemory cinit_slots;  // global constraint initialisation: 3 words per iteration
   micmb::DeviceMemory adj_order;  // backward sweep: cells by decreasing step count, then bins
   int64_t adj_ckpt_capacity = 0;  // doubles in adj_ckpt_y
   double dt_for_launch = 0.0;

@@ -88,6 +88,7 @@ def _stats_rows(raw: np.ndarray):
     for row in raw:
         d = {k: int(row[i]) for i, k in enumerate(STATS_FIELDS)}
         d["final_time"] = float(row[8:9].view(np.float64)[0])
+        d["constraint_init_iterations"] = int(row[9])
         out.append(d)
     return out
 
@@ -264,8 +265,27 @@ class Reference:
 _om = None
 
 
-# double exchange(double shard_sum, void* user): the job's sum of the shards' error sums
-EXCHANGE_FN = C.CFUNCTYPE(C.c_double, C.c_double, C.c_void_p)
+# double exchange(double value, int op, void* user): op EXCHANGE_SUM, the job's sum
+# of the shards' error sums in rank order; op EXCHANGE_MAX, the job's combination
+# of the shards' encoded maxima (max_combine)
+EXCHANGE_FN = C.CFUNCTYPE(C.c_double, C.c_double, C.c_int, C.c_void_p)
+EXCHANGE_SUM, EXCHANGE_MAX = 0, 1
+
+
+def max_combine(values):
+    """The shards' encoded maxima of the constraint initialisation combined in
+    rank order: NaN when any is NaN, +Inf when any is infinite, else the largest
+    (oracle.c om_max_combine)."""
+    out = 0.0
+    for v in values:
+        v = float(v)
+        if np.isnan(out) or np.isnan(v):
+            out = float("nan")
+        elif np.isinf(out) or np.isinf(v):
+            out = float("inf")
+        else:
+            out = max(out, v)
+    return out
 
 
 def _load_oracle():
@@ -287,8 +307,8 @@ def _load_oracle():
         lib.om_adjoint_per_cell.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, _f64p, _f64p,
                                             C.c_double, _f64p, _f64p, _f64p, _f64p, _f64p, C.c_int, C.c_int]
         lib.om_replay_per_cell.argtypes = [C.c_void_p, C.c_void_p, C.c_int, _f64p, _f64p, _i32p, C.c_int, _f64p]
-        lib.om_solve_global.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, _f64p, _f64p, C.c_double,
-                                        _f64p, _i64p, C.c_int, _i32p, EXCHANGE_FN, C.c_void_p, C.c_int64]
+        lib.om_solve_global.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double, _f64p, _f64p, _f64p,
+                                        C.c_double, _f64p, _i64p, C.c_int, _i32p, EXCHANGE_FN, C.c_void_p, C.c_int64]
         lib.om_n_eq.argtypes = [C.c_void_p]
         lib.om_constraint_params.argtypes = [C.c_void_p, C.c_int, _f64p, _f64p]
         lib.om_constraint_params.restype = None
@@ -415,10 +435,13 @@ class Restatement:
 
     def solve_global(self, inputs, dt, k=None, shards=None, exchange=None, total_cells=0):
         """Global step control (one step size for all cells), the error sum in
-        the fixed order a GPU reproduces.  shards: cell counts of consecutive
-        shards (default one); exchange(shard_sum) -> job sum makes the cells
-        this rank's shard of a job over total_cells.  (y_final [n,S] system
-        order, stats [10])."""
+        the fixed order a GPU reproduces; with constraints, micm's DAE
+        Rosenbrock on an n-cell State (one initialisation for all cells).
+        shards: cell counts of consecutive shards (default one);
+        exchange(value, op) makes the cells this rank's shard of a job over
+        total_cells: op EXCHANGE_SUM returns the job's sum of the shard sums in
+        rank order, op EXCHANGE_MAX the max_combine of the ranks' values.
+        (y_final [n,S] system order, stats [10])."""
         y = np.zeros_like(inputs["concentrations"])
         y[:, self.species_columns] = inputs["concentrations"]
         y = np.ascontiguousarray(y)
@@ -428,8 +451,10 @@ class Restatement:
         sizes = [n] if shards is None else list(shards)
         assert sum(sizes) == n
         starts = np.ascontiguousarray(np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32))
-        cb = EXCHANGE_FN(lambda v, _u: float(exchange(v))) if exchange else EXCHANGE_FN()
-        rc = self.lib.om_solve_global(self.handle, C.byref(self.params), n, float(dt), _p(k), _p(self.atol_columns),
+        keq = self.keq(inputs["temperature"])
+        cb = EXCHANGE_FN(lambda v, op, _u: float(exchange(v, op))) if exchange else EXCHANGE_FN()
+        rc = self.lib.om_solve_global(self.handle, C.byref(self.params), n, float(dt), _p(k), _p(keq),
+                                      _p(self.atol_columns),
                                       self.mech.relative_tolerance, _p(y), _p(stats, C.c_int64), len(sizes),
                                       _p(starts, C.c_int32), cb, None, int(total_cells or n))
         if rc:

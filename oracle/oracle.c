@@ -810,6 +810,16 @@ static double dmax(double a, double b)
   return (a < b) ? b : a; /* std::max */
 }
 
+/* Solver::PostSolveClamp (solver.hpp:275-297): std::max(y, 0) on every
+ * variable; with constraints only the ODE variables are clamped, by
+ * (y > 0 ? y : 0), and the algebraic ones are left as solved. */
+static double post_clamp(const om_mech* m, int i, double v)
+{
+  if (!m->nc)
+    return (v < 0.0) ? 0.0 : v;
+  return m->mass[i] > 0.0 ? (v > 0.0 ? v : 0.0) : v;
+}
+
 /* returns state; stats[0..6]; optionally records accepted (y_n, H_n) */
 /* micm's InitializeConstraints (rosenbrock.inl:407-576) for one cell: Newton
  * iterations on the algebraic variables until max |G| over algebraic rows is
@@ -1248,7 +1258,7 @@ static void* worker(void* arg)
       rosenbrock_cell(m, j->p, j->dt, k, j->keq ? j->keq + (size_t)c * m->n_eq : NULL, j->atol, j->rtol, &w,
                       j->stats ? j->stats + (size_t)c * 10 : NULL, NULL, NULL, 0, NULL);
       for (int i = 0; i < S; ++i)
-        j->y[(size_t)c * S + i] = w.Y[i] < 0.0 ? 0.0 : w.Y[i];
+        j->y[(size_t)c * S + i] = post_clamp(m, i, w.Y[i]);
     }
     else
     {
@@ -1489,17 +1499,130 @@ static double shard_error_sum(const double* cell_sum, int n)
   return tree256(red);
 }
 
+/* A shard's flags and maximum as one value for the exchange: NaN when any
+ * value was NaN, +Inf when any was infinite, else the maximum.  Combining
+ * encoded values by om_max_combine keeps micm's order of checks (NaN first). */
+static double encode_max(int any_nan, int any_inf, double max_value)
+{
+  if (any_nan)
+    return NAN;
+  if (any_inf)
+    return INFINITY;
+  return max_value;
+}
+
+double om_max_combine(double a, double b)
+{
+  if (isnan(a) || isnan(b))
+    return NAN;
+  if (isinf(a) || isinf(b))
+    return INFINITY;
+  return a > b ? a : b;
+}
+
+/* micm's InitializeConstraints (rosenbrock.inl:407-576) on an n-cell State:
+ * the largest |G| over every cell's algebraic rows decides convergence, and
+ * while it is not met every cell takes the Newton update (one Jacobian
+ * update, decomposition and solve counted per iteration for the State).
+ * With `exchange`, the shard's encoded maximum goes through exchange(v,
+ * OM_EXCHANGE_MAX, user) and the job's comes back. */
+static int initialize_constraints_global(const om_mech* m, const micmb_rosenbrock_params* p, int n,
+                                         const double* keq, double* y, double* delta, double* J,
+                                         om_exchange_fn exchange, void* user, int64_t* ju, int64_t* dec,
+                                         int64_t* sol, int64_t* iters)
+{
+  const int S = m->S;
+  for (int iter = 0; iter < p->constraint_init_max_iterations; ++iter)
+  {
+    int any_nan = 0, any_inf = 0;
+    double max_res = 0.0;
+    for (int c = 0; c < n; ++c)
+    {
+      double* d = delta + (size_t)c * S;
+      for (int i = 0; i < S; ++i)
+        d[i] = 0.0;
+      constraint_forcing(m, keq + (size_t)c * m->n_eq, y + (size_t)c * S, d);
+      for (int i = 0; i < S; ++i)
+        if (m->mass[i] == 0.0)
+        {
+          const double v = d[i];
+          any_nan = any_nan || isnan(v);
+          any_inf = any_inf || isinf(v);
+          const double a = fabs(v);
+          if (!isnan(a) && !isinf(a))
+            max_res = (max_res > a ? max_res : a);
+        }
+    }
+    double v = encode_max(any_nan, any_inf, max_res);
+    if (exchange)
+      v = exchange(v, OM_EXCHANGE_MAX, user);
+    if (isnan(v))
+      return MICMB_SOLVER_NAN_DETECTED;
+    if (isinf(v))
+      return MICMB_SOLVER_INF_DETECTED;
+    *iters = iter + 1;
+    if (v < p->constraint_init_tolerance)
+      return MICMB_SOLVER_CONVERGED;
+    for (int c = 0; c < n; ++c)
+    {
+      double* Jc = J + (size_t)c * m->nnz;
+      double* d = delta + (size_t)c * S;
+      for (int e = 0; e < m->nnz; ++e)
+        Jc[e] = 0.0;
+      constraint_neg_jacobian(m, keq + (size_t)c * m->n_eq, y + (size_t)c * S, Jc);
+      for (int i = 0; i < S; ++i)
+        Jc[m->pos[(size_t)i * S + i]] += 1.0 * m->mass[i];
+      decompose(m, Jc);
+      lu_solve(m, Jc, d);
+    }
+    (*ju)++;
+    (*dec)++;
+    (*sol)++;
+    any_nan = any_inf = 0;
+    for (int c = 0; c < n; ++c)
+    {
+      const double* d = delta + (size_t)c * S;
+      double* yc = y + (size_t)c * S;
+      for (int i = 0; i < S; ++i)
+        if (m->mass[i] == 0.0)
+        {
+          any_nan = any_nan || isnan(d[i]);
+          any_inf = any_inf || isinf(d[i]);
+          if (!isnan(d[i]) && !isinf(d[i]))
+            yc[i] += d[i];
+        }
+    }
+    v = encode_max(any_nan, any_inf, 0.0);
+    if (exchange)
+      v = exchange(v, OM_EXCHANGE_MAX, user);
+    if (isnan(v))
+      return MICMB_SOLVER_NAN_DETECTED;
+    if (isinf(v))
+      return MICMB_SOLVER_INF_DETECTED;
+  }
+  return MICMB_SOLVER_CONSTRAINT_INITIALIZATION_FAILED;
+}
+
 /* y [cell][column] in/out, k [cell][R]; stats_out [10] as one row of
  * om_solve_per_cell's.  n_shards / shard_start: the cells split into shards
  * (shard_start[0] = 0, shard_start[n_shards] = n), the job's sum is the
  * shards' sums in shard order.  With `exchange` set, the n cells are this
- * rank's shard only: exchange(this shard's sum, user) returns the job's sum,
+ * rank's shard only: exchange(this shard's sum, OM_EXCHANGE_SUM, user) returns the job's sum,
  * and total_cells counts every rank's cells. */
 int om_solve_global(const om_mech* m, const micmb_rosenbrock_params* p, int n, double dt, const double* k,
-                    const double* atol, double rtol, double* y, int64_t* stats_out, int n_shards,
+                    const double* keq, const double* atol, double rtol, double* y, int64_t* stats_out, int n_shards,
                     const int* shard_start, om_exchange_fn exchange, void* user, int64_t total_cells)
 {
   const int S = m->S, ns = p->stages;
+  if (m->nc && m->n_eq && !keq)
+  {
+    snprintf(g_err, sizeof g_err, "equilibrium constraints need K_eq values");
+    return -1;
+  }
+  const double* kq = keq;
+  double kq_none = 0.0;
+  if (!kq)
+    kq = &kq_none;
   const size_t nS = (size_t)n * S;
   double* F0 = xcalloc(nS + 1, sizeof(double));
   double* Ynew = xcalloc(nS + 1, sizeof(double));
@@ -1513,8 +1636,15 @@ int om_solve_global(const om_mech* m, const micmb_rosenbrock_params* p, int n, d
   double H = dmin(dmax(h_min, fabs(h_start)), fabs(h_max));
   double t = 0.0;
   int reject_last = 0, reject_more = 0, state = MICMB_SOLVER_RUNNING;
-  int64_t fc = 0, ju = 0, nst = 0, acc = 0, rej = 0, dec = 0, sol = 0;
+  int64_t fc = 0, ju = 0, nst = 0, acc = 0, rej = 0, dec = 0, sol = 0, init_iters = 0;
   const double n_values = (double)(exchange ? total_cells : n) * (double)S;
+  if (m->nc)
+  {
+    const int st = initialize_constraints_global(m, p, n, kq, y, F0, J, exchange, user, &ju, &dec, &sol,
+                                                 &init_iters);
+    if (st != MICMB_SOLVER_CONVERGED)
+      state = st;
+  }
   while ((t - dt + p->round_off) <= 0 && state == MICMB_SOLVER_RUNNING)
   {
     if (nst > p->max_number_of_steps)
@@ -1529,10 +1659,18 @@ int om_solve_global(const om_mech* m, const micmb_rosenbrock_params* p, int n, d
     }
     H = dmin(H, fabs(dt - t));
     for (int c = 0; c < n; ++c)
+    {
       forcing(m, k + (size_t)c * m->R, y + (size_t)c * S, F0 + (size_t)c * S);
+      if (m->nc)
+        constraint_forcing(m, kq + (size_t)c * m->n_eq, y + (size_t)c * S, F0 + (size_t)c * S);
+    }
     fc++;
     for (int c = 0; c < n; ++c)
-      neg_jacobian(m, k + (size_t)c * m->R, y + (size_t)c * S, J + (size_t)c * m->nnz);
+      {
+        neg_jacobian(m, k + (size_t)c * m->R, y + (size_t)c * S, J + (size_t)c * m->nnz);
+        if (m->nc)
+          constraint_neg_jacobian(m, kq + (size_t)c * m->n_eq, y + (size_t)c * S, J + (size_t)c * m->nnz);
+      }
     ju++;
     int accepted = 0;
     while (!accepted)
@@ -1542,7 +1680,7 @@ int om_solve_global(const om_mech* m, const micmb_rosenbrock_params* p, int n, d
       {
         double* Jc = J + (size_t)c * m->nnz;
         for (int i = 0; i < S; ++i)
-          Jc[m->pos[(size_t)i * S + i]] += alpha;
+          Jc[m->pos[(size_t)i * S + i]] += alpha * m->mass[i]; /* alpha M - J */
         decompose(m, Jc);
       }
       dec++;
@@ -1563,6 +1701,8 @@ int om_solve_global(const om_mech* m, const micmb_rosenbrock_params* p, int n, d
               for (int i = 0; i < S; ++i)
                 Yn[i] += p->a[sc + j] * K[((size_t)j * n + c) * S + i];
             forcing(m, k + (size_t)c * m->R, Yn, Ks);
+            if (m->nc)
+              constraint_forcing(m, kq + (size_t)c * m->n_eq, Yn, Ks);
           }
           if (s + 1 < ns && !p->new_function_evaluation[s + 1])
             memcpy(K + ((size_t)(s + 1) * n + c) * S, Ks, sizeof(double) * S);
@@ -1570,7 +1710,8 @@ int om_solve_global(const om_mech* m, const micmb_rosenbrock_params* p, int n, d
           {
             const double coh = p->c[sc + j] / H;
             for (int i = 0; i < S; ++i)
-              Ks[i] += coh * K[((size_t)j * n + c) * S + i];
+              if (m->mass[i] != 0.0) /* algebraic rows have no mass coupling */
+                Ks[i] += coh * K[((size_t)j * n + c) * S + i];
           }
           lu_solve(m, J + (size_t)c * m->nnz, Ks);
         }
@@ -1592,6 +1733,8 @@ int om_solve_global(const om_mech* m, const micmb_rosenbrock_params* p, int n, d
         for (int s = 0; s < ns; ++s)
           for (int i = 0; i < S; ++i)
             Ye[i] += p->e[s] * K[((size_t)s * n + c) * S + i];
+        for (int q = 0; q < m->nc; ++q) /* SetAlgebraicErrors: the step change */
+          Ye[m->c_row[q]] = Yn[m->c_row[q]] - Yc[m->c_row[q]];
         double sum = 0.0;
         for (int i = 0; i < S; ++i)
         {
@@ -1604,7 +1747,7 @@ int om_solve_global(const om_mech* m, const micmb_rosenbrock_params* p, int n, d
       }
       double total = 0.0;
       if (exchange)
-        total = exchange(shard_error_sum(cell_sum, n), user);
+        total = exchange(shard_error_sum(cell_sum, n), OM_EXCHANGE_SUM, user);
       else
         for (int r = 0; r < n_shards; ++r)
           total += shard_error_sum(cell_sum + shard_start[r], shard_start[r + 1] - shard_start[r]);
@@ -1646,7 +1789,11 @@ int om_solve_global(const om_mech* m, const micmb_rosenbrock_params* p, int n, d
         if (acc >= 1)
           rej++;
         for (int c = 0; c < n; ++c)
-          neg_jacobian(m, k + (size_t)c * m->R, y + (size_t)c * S, J + (size_t)c * m->nnz);
+          {
+        neg_jacobian(m, k + (size_t)c * m->R, y + (size_t)c * S, J + (size_t)c * m->nnz);
+        if (m->nc)
+          constraint_neg_jacobian(m, kq + (size_t)c * m->n_eq, y + (size_t)c * S, J + (size_t)c * m->nnz);
+      }
         ju++;
       }
     }
@@ -1654,7 +1801,7 @@ int om_solve_global(const om_mech* m, const micmb_rosenbrock_params* p, int n, d
   if (state == MICMB_SOLVER_RUNNING)
     state = MICMB_SOLVER_CONVERGED;
   for (size_t e = 0; e < nS; ++e)
-    y[e] = (y[e] < 0.0) ? 0.0 : y[e]; /* Solver::PostSolveClamp */
+    y[e] = post_clamp(m, (int)(e % (size_t)(S > 0 ? S : 1)), y[e]);
   if (stats_out)
   {
     stats_out[0] = fc;
@@ -1666,7 +1813,7 @@ int om_solve_global(const om_mech* m, const micmb_rosenbrock_params* p, int n, d
     stats_out[6] = sol;
     stats_out[7] = state;
     memcpy(&stats_out[8], &t, sizeof(double));
-    stats_out[9] = 0;
+    stats_out[9] = init_iters;
   }
   free(F0);
   free(Ynew);

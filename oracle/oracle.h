@@ -67,11 +67,20 @@ int om_replay_per_cell(const om_mech* m, const micmb_rosenbrock_params* p, int n
 /* Global step control (one step size for all n cells) with the error sum in
  * the fixed order a GPU reproduces (per cell, per 256-cell block tree, per
  * shard, shards in order).  exchange != NULL: the cells are this rank's
- * shard; exchange(shard sum, user) returns the job's sum over total_cells. */
-typedef double (*om_exchange_fn)(double shard_sum, void* user);
+ * shard; exchange(shard sum, OM_EXCHANGE_SUM, user) returns the job's sum over
+ * total_cells, and exchange(v, OM_EXCHANGE_MAX, user) the job's combination of
+ * every rank's encoded maximum (om_max_combine in rank order: NaN when any is
+ * NaN, +Inf when any is infinite, else the largest), which the constraint
+ * initialisation uses.  keq [cell][n_eq] may be NULL without equilibrium
+ * constraints. */
+#define OM_EXCHANGE_SUM 0
+#define OM_EXCHANGE_MAX 1
+typedef double (*om_exchange_fn)(double value, int op, void* user);
+double om_max_combine(double a, double b);
 int om_solve_global(const om_mech* m, const micmb_rosenbrock_params* p, int n, double dt, const double* k,
-                    const double* atol, double rtol, double* y, int64_t* stats_out, int n_shards,
-                    const int* shard_start, om_exchange_fn exchange, void* user, int64_t total_cells);
+                    const double* keq, const double* atol, double rtol, double* y, int64_t* stats_out,
+                    int n_shards, const int* shard_start, om_exchange_fn exchange, void* user,
+                    int64_t total_cells);
 /* Algebraic constraints: K_eq(T) of every equilibrium constraint per cell
  * ([cell][n_eq], Van't Hoff with the handle's exp), and the per-cell solve
  * with those values (keq may be NULL without equilibrium constraints). */

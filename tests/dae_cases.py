@@ -34,6 +34,26 @@ def terminator_robertson_inputs(n=1):
     return dict(temperature=T, pressure=P, air_density=np.full(n, 42.0), concentrations=y, custom_params=params)
 
 
+def negative_algebraic():
+    """A -> B (k = 0.1) with the linear constraint A + B + C = 1 replacing C's
+    row; started from A + B = 1.5 the initialisation sets C to -0.5, which
+    micm's post-solve clamp leaves as solved (only ODE variables are clamped)."""
+    m = Mechanism(species=["A", "B", "C"], reactions=[], name="negative_algebraic", reorder_state=False,
+                  absolute_tolerance=np.full(3, 1e-6), relative_tolerance=1e-6)
+    m.add(arrhenius(A=0.1), [0], [(1, 1.0)])
+    m.constraints.append(linear_constraint(2, [(0, 1.0), (1, 1.0), (2, 1.0)], 1.0, name="total"))
+    return m
+
+
+def negative_algebraic_inputs(n=3):
+    T = np.full(n, 298.0)
+    P = np.full(n, 101325.0)
+    y = np.tile([1.0, 0.5, 0.0], (n, 1))
+    y[:, 0] *= np.linspace(1.0, 1.5, n)
+    return dict(temperature=T, pressure=P, air_density=ideal_air_density(P, T), concentrations=y,
+                custom_params=np.zeros((n, 0)))
+
+
 def equilibrium(stoich=1.0, two=False):
     """A -> B (k = 0.1) with B <=> C in equilibrium (C algebraic); with
     `two`, also D -> E with E <=> F.  `stoich` is B's exponent."""

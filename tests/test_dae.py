@@ -10,7 +10,8 @@ import numpy as np
 import pytest
 
 import oracle
-from dae_cases import equilibrium, equilibrium_inputs, terminator_robertson, terminator_robertson_inputs
+from dae_cases import (equilibrium, equilibrium_inputs, negative_algebraic, negative_algebraic_inputs,
+                       terminator_robertson, terminator_robertson_inputs)
 
 pytestmark = pytest.mark.skipif(not (oracle.restatement_available() and oracle.reference_available()),
                                 reason="oracle not built")
@@ -23,6 +24,7 @@ CASES = [
      [1, 5, 20]),
     ("equilibrium_stoich2_two", lambda: equilibrium(2.0, True), lambda m: equilibrium_inputs(m, 3, False, 0.2), 40,
      [1, 10, 50]),
+    ("negative_algebraic", negative_algebraic, lambda m: negative_algebraic_inputs(3), 40, [1, 10, 30]),
     # F = 0 with F^2 as the product: dG/dF = 0, the initialisation's matrix is
     # singular and micm reports InfDetected
     ("equilibrium_singular_init", lambda: equilibrium(2.0, True), lambda m: equilibrium_inputs(m, 3, False, 0.0), 40,
@@ -83,3 +85,29 @@ def test_invalid_constraints_rejected():
     m.constraints[0].terms.append((9, 1.0))  # no such species
     with pytest.raises(MicmbError):
         CompiledMechanism(m)
+
+
+@pytest.mark.parametrize("name,make_mech,make_inputs,tableau,outputs", CASES, ids=[c[0] for c in CASES])
+def test_global_restatement_follows_micms_multicell_state(name, make_mech, make_inputs, tableau, outputs):
+    """One n-cell State (micm's global step size): the constraint
+    initialisation iterates all cells until the largest residual of any cell
+    meets the tolerance, then one step size serves every cell.  The
+    restatement sums the error norm in the GPU's fixed order and micm with one
+    accumulator, so values agree to rounding and the counts exactly."""
+    m = make_mech()
+    inp = make_inputs(m)
+    R = oracle.Restatement(m, tableau_kind=tableau)
+    ref = oracle.Reference(m, tableau=tableau)
+    y_r, y_m = inp["concentrations"], inp["concentrations"]
+    t = 0.0
+    for target in outputs:
+        dt = target - t
+        y_r, st_r = R.solve_global(dict(inp, concentrations=y_r), dt)
+        y_m, st_m = ref.solve_global(dict(inp, concentrations=y_m), dt)
+        for q, key in enumerate(oracle.STATS_FIELDS):
+            assert st_r[q] == st_m[0][key], key
+        assert st_r[9] == st_m[0]["constraint_init_iterations"]
+        np.testing.assert_allclose(y_r, y_m, rtol=1e-9, atol=1e-300)
+        t = target
+    if name == "negative_algebraic":
+        assert np.all(y_r[:, 2] < 0.0)  # algebraic variables are not clamped

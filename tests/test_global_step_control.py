@@ -66,34 +66,55 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _rank_main(rank, world, port, out_path):
+def _dae_case():
+    """two equilibrium constraints, inconsistent start: the constraint
+    initialisation iterates, and its residual maximum crosses the ranks"""
+    from dae_cases import equilibrium, equilibrium_inputs
+    m = equilibrium(2.0, True)
+    inp = equilibrium_inputs(m, 5, False, 0.2)
+    inp["concentrations"][3:, 1] *= 3.0  # rank 1's cells start further from equilibrium
+    return m, inp
+
+
+# kind: (case, shard sizes, tableau, dt)
+KINDS = {"kinetic": (_case, SHARDS, 4, 600.0), "dae": (_dae_case, [2, 3], 40, 10.0)}
+
+
+def _rank_main(rank, world, port, out_path, kind="kinetic"):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        m, inp = _case()
-        mine = _split(inp, SHARDS)[rank]
+        make_case, shards, tableau, dt = KINDS[kind]
+        m, inp = make_case()
+        mine = _split(inp, shards)[rank]
 
-        def exchange(shard_sum):
+        def exchange(value, op):
             gathered = [torch.zeros(1, dtype=torch.float64) for _ in range(world)]
-            dist.all_gather(gathered, torch.tensor([shard_sum], dtype=torch.float64))
+            dist.all_gather(gathered, torch.tensor([value], dtype=torch.float64))
+            if op == oracle.EXCHANGE_MAX:
+                return oracle.max_combine(g.item() for g in gathered)
             total = 0.0
             for g in gathered:  # rank order
                 total += g.item()
             return total
 
-        y, st = oracle.Restatement(m, 4).solve_global(mine, 600.0, exchange=exchange, total_cells=sum(SHARDS))
+        y, st = oracle.Restatement(m, tableau).solve_global(mine, dt, exchange=exchange, total_cells=sum(shards))
         np.savez(f"{out_path}.{rank}.npz", y=y, stats=st)
         dist.barrier()
     finally:
         dist.destroy_process_group()
 
 
-def test_two_gloo_ranks_equal_the_single_process_solve(tmp_path):
+@pytest.mark.parametrize("kind", ["kinetic", "dae"])
+def test_two_gloo_ranks_equal_the_single_process_solve(tmp_path, kind):
     out = str(tmp_path / "rank")
-    mp.start_processes(_rank_main, args=(2, _free_port(), out), nprocs=2, start_method="spawn")
+    mp.start_processes(_rank_main, args=(2, _free_port(), out, kind), nprocs=2, start_method="spawn")
     r0, r1 = (np.load(f"{out}.{r}.npz") for r in range(2))
-    m, inp = _case()
-    y, st = oracle.Restatement(m, 4).solve_global(inp, 600.0, shards=SHARDS)
+    make_case, shards, tableau, dt = KINDS[kind]
+    m, inp = make_case()
+    y, st = oracle.Restatement(m, tableau).solve_global(inp, dt, shards=shards)
+    if kind == "dae":
+        assert st[9] >= 2 and st[7] == 2  # the initialisation iterated, and the solve converged
     np.testing.assert_array_equal(np.concatenate([r0["y"], r1["y"]]), y)
     np.testing.assert_array_equal(r0["stats"], st)
     np.testing.assert_array_equal(r1["stats"], st)
@@ -168,21 +189,31 @@ def test_gpu_exchange_hook_with_one_rank_changes_nothing(cuda_device):
 
 
 @pytest.mark.gpu
-def test_gpu_two_ranks_on_host_threads_equal_two_shard_restatement(cuda_device):
+@pytest.mark.parametrize("kind", ["kinetic", "dae"])
+def test_gpu_two_ranks_on_host_threads_equal_two_shard_restatement(cuda_device, kind):
     """Two ranks as two host threads, each with its own state and stream on one
-    GPU.  The exchange reads this rank's sum on the host (after its stream is
+    GPU.  The exchange reads this rank's value on the host (after its stream is
     done), meets the other rank at a host barrier with a timeout, and writes
-    both sums back; no kernel ever waits on another rank's kernel."""
+    both values back; no kernel ever waits on another rank's kernel.  "dae":
+    the constraint initialisation's residual maxima and flags cross the ranks
+    through the same hook."""
     from micm_b200 import Solver
     from micm_b200._native import check, lib
-    m, inp = _case()
-    R = oracle.Restatement(m, 4, correctly_rounded=True)
+    from gpu_helpers import make_state
+    make_case, shards, tableau, dt = KINDS[kind]
+    m, inp = make_case()
+    R = oracle.Restatement(m, tableau, correctly_rounded=True)
     k = R._k(inp)
-    y_ref, st_ref = R.solve_global(inp, 600.0, k=k, shards=SHARDS)
-    solver = Solver(m, 4, vector_length=32)
-    parts = _split(inp, SHARDS)
-    kparts = np.split(k, np.cumsum(SHARDS)[:-1])
-    states = [_gpu_state(solver, p, kp) for p, kp in zip(parts, kparts)]
+    y_ref, st_ref = R.solve_global(inp, dt, k=k, shards=shards)
+    solver = Solver(m, tableau, vector_length=32)
+    parts = _split(inp, shards)
+    if kind == "dae":
+        states = [make_state(solver, p) for p in parts]
+        for st in states:
+            solver.update_state_parameters(st)
+    else:
+        kparts = np.split(k, np.cumsum(shards)[:-1])
+        states = [_gpu_state(solver, p, kp) for p, kp in zip(parts, kparts)]
     streams = [torch.cuda.Stream() for _ in range(2)]
     for st, s in zip(states, streams):
         check(lib().micmb_state_set_stream(st.handle, ctypes.c_void_p(s.cuda_stream)))
@@ -205,8 +236,8 @@ def test_gpu_two_ranks_on_host_threads_equal_two_shard_restatement(cuda_device):
     def run(rank):
         try:
             torch.cuda.set_device(0)
-            states[rank].set_global_exchange(make_exchange(rank), 2, sum(SHARDS))
-            results[rank] = solver.solve(600.0, states[rank], method="plain", step_control="global")
+            states[rank].set_global_exchange(make_exchange(rank), 2, sum(shards))
+            results[rank] = solver.solve(dt, states[rank], method="plain", step_control="global")
         except Exception as e:  # reported below
             errors.append(e)
             barrier.abort()
@@ -224,3 +255,4 @@ def test_gpu_two_ranks_on_host_threads_equal_two_shard_restatement(cuda_device):
     np.testing.assert_array_equal(np.concatenate(y), y_ref)
     for res in results:
         _stats_equal(res, st_ref)
+        assert res.stats["constraint_init_iterations"] == st_ref[9]
