@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <concepts>
 #include <cstddef>
 #include <cstdint>
 #include <iomanip>
@@ -697,6 +698,108 @@ namespace micm
   template<Index L>
   class Solver;
 
+  // ---------------------------------------------------------------- constraints
+  // micm's algebraic constraints (constraint/types/linear_constraint.hpp:150-172,
+  // equilibrium_constraint.hpp:41-47 and :208-245, constraint.hpp:26-45).  The
+  // matrix-policy parameters are kept so that micm code names the same types;
+  // the library evaluates the constraints on the device, so they select nothing.
+  template<class DenseMatrixPolicy = void, class SparseMatrixPolicy = void>
+  class LinearConstraint
+  {
+   public:
+    std::string name_;
+    Species algebraic_species_;
+    std::vector<StoichSpecies> terms_;
+    Real constant_{};
+
+    LinearConstraint(std::string name, const Species& algebraic_species, const std::vector<StoichSpecies>& terms,
+                     Real constant)
+        : name_(std::move(name)),
+          algebraic_species_(algebraic_species),
+          terms_(terms),
+          constant_(constant)
+    {
+      if (terms_.empty())
+        throw MicmException("MICM Constraint", 1, "Linear constraint requires at least one term");
+    }
+    const std::string& AlgebraicSpecies() const
+    {
+      return algebraic_species_.name_;
+    }
+  };
+
+  template<class DenseMatrixPolicy = void, class SparseMatrixPolicy = void>
+  class EquilibriumConstraint
+  {
+   public:
+    // Van't Hoff: K_eq(T) = K_HLC_ref * exp((delta_H / R) * (1/T - 1/T_ref))
+    struct VantHoffParam
+    {
+      Real K_HLC_ref_;
+      Real delta_H_;
+      Real R_ = constants::GAS_CONSTANT;
+      Real T_ref_ = 298.15;
+    };
+
+    std::string name_;
+    Species algebraic_species_;
+    std::vector<StoichSpecies> reactants_;
+    std::vector<StoichSpecies> products_;
+    VantHoffParam vant_hoff_param_{};
+
+    EquilibriumConstraint(const std::string& name, const Species& algebraic_species,
+                          std::vector<StoichSpecies> reactants, std::vector<StoichSpecies> products,
+                          VantHoffParam vant_hoff_param)
+        : name_(name),
+          algebraic_species_(algebraic_species),
+          reactants_(std::move(reactants)),
+          products_(std::move(products)),
+          vant_hoff_param_(vant_hoff_param)
+    {
+      if (reactants_.empty())
+        throw MicmException("MICM Constraint", 1, "Equilibrium constraint requires at least one reactant");
+      if (products_.empty())
+        throw MicmException("MICM Constraint", 1, "Equilibrium constraint requires at least one product");
+      for (const auto& s : reactants_)
+        if (s.coefficient_ <= 0)
+          throw MicmException("MICM Constraint", 2, "Stoichiometric coefficients must be positive");
+      for (const auto& s : products_)
+        if (s.coefficient_ <= 0)
+          throw MicmException("MICM Constraint", 2, "Stoichiometric coefficients must be positive");
+      if (vant_hoff_param_.K_HLC_ref_ <= 0)
+        throw MicmException("MICM Constraint", 3, "Equilibrium constant must be positive");
+    }
+    const std::string& AlgebraicSpecies() const
+    {
+      return algebraic_species_.name_;
+    }
+  };
+
+  template<class DenseMatrixPolicy = void, class SparseMatrixPolicy = void>
+  class Constraint
+  {
+   public:
+    using ConstraintVariant = std::variant<EquilibriumConstraint<DenseMatrixPolicy, SparseMatrixPolicy>,
+                                           LinearConstraint<DenseMatrixPolicy, SparseMatrixPolicy>>;
+    ConstraintVariant constraint_;
+
+    template<typename T>
+      requires std::same_as<std::decay_t<T>, EquilibriumConstraint<DenseMatrixPolicy, SparseMatrixPolicy>> ||
+               std::same_as<std::decay_t<T>, LinearConstraint<DenseMatrixPolicy, SparseMatrixPolicy>>
+    Constraint(T&& constraint)
+        : constraint_(std::forward<T>(constraint))
+    {
+    }
+    std::string GetName() const
+    {
+      return std::visit([](const auto& c) { return c.name_; }, constraint_);
+    }
+    const std::string& AlgebraicSpecies() const
+    {
+      return std::visit([](const auto& c) -> const std::string& { return c.AlgebraicSpecies(); }, constraint_);
+    }
+  };
+
   // ---------------------------------------------------------------- state
   template<Index L = MICM_DEFAULT_VECTOR_SIZE>
   class CudaState
@@ -716,6 +819,8 @@ namespace micm
     std::vector<std::string> variable_names_;
     Real relative_tolerance_{ 1e-6 };
     std::vector<Real> absolute_tolerance_;
+    Index constraint_size_{ 0 };
+    std::vector<Real> upper_left_identity_diagonal_;  // mass-matrix diagonal by variable: 1 ODE, 0 algebraic
 
     class VariableProxy
     {
@@ -867,6 +972,8 @@ namespace micm
     std::vector<std::string> param_labels_;
     std::vector<Real> atol_;  // by state column
     Index n_rate_constants_ = 0;
+    std::vector<Real> mass_;  // by state column: 1 ODE row, 0 algebraic row
+    Index n_constraints_ = 0;
     StepControl step_control_ = StepControl::Global;
     Method method_ = Method::Plain;
 
@@ -926,6 +1033,8 @@ namespace micm
         st.custom_rate_parameter_map_[param_labels_[i]] = i;
       st.absolute_tolerance_ = atol_;
       st.relative_tolerance_ = 1e-6;
+      st.constraint_size_ = n_constraints_;
+      st.upper_left_identity_diagonal_ = mass_.empty() ? std::vector<Real>(variable_names_.size(), 1.0) : mass_;
       return st;
     }
 
@@ -967,8 +1076,16 @@ namespace micm
       r.stats_.rejected_ = (Index)st.rejected;
       r.stats_.decompositions_ = (Index)st.decompositions;
       r.stats_.solves_ = (Index)st.solves;
+      r.stats_.constraint_init_iterations_ = (Index)st.constraint_init_iterations;
       r.stats_.final_time_ = st.final_time;
       return r;
+    }
+
+    // algebraic constraints: which rows are algebraic (set by the builder)
+    void SetConstraintRows(std::vector<Real> mass, Index n_constraints)
+    {
+      mass_ = std::move(mass);
+      n_constraints_ = n_constraints;
     }
 
     SolverResult Solve(Real time_step, CudaState<L>& state, const RosenbrockSolverParameters& params)
@@ -1036,6 +1153,16 @@ namespace micm
     bool ignore_unused_species_ = true;
     bool reorder_state_ = true;
     bool valid_system_ = false;
+    // constraints as the C description takes them (SetConstraints)
+    struct ConstraintRow
+    {
+      int32_t type;
+      std::string species;
+      std::vector<StoichSpecies> terms;  // equilibrium: reactants, then products
+      int32_t n_reactants;
+      double params[4];
+    };
+    std::vector<ConstraintRow> constraints_;
 
    public:
     CudaSolverBuilderInPlace(const SolverParametersPolicy& options)
@@ -1051,6 +1178,42 @@ namespace micm
     CudaSolverBuilderInPlace& SetReactions(const std::vector<Process>& reactions)
     {
       reactions_ = reactions;
+      return *this;
+    }
+    // SolverBuilder::SetConstraints (solver_builder.hpp:104-108): algebraic
+    // constraints, each replacing its algebraic species' ODE row.  micm's CUDA
+    // builder rejects them (solver_builder.inl:251-266); this one solves them
+    // on the device (plain and fused methods, both step controls).
+    template<class D, class S>
+    CudaSolverBuilderInPlace& SetConstraints(std::vector<Constraint<D, S>>&& constraints)
+    {
+      constraints_.clear();
+      for (const auto& c : constraints)
+        std::visit(
+            [&](const auto& v) {
+              using T = std::decay_t<decltype(v)>;
+              ConstraintRow row{};
+              row.species = v.AlgebraicSpecies();
+              if constexpr (std::is_same_v<T, LinearConstraint<D, S>>)
+              {
+                row.type = MICMB_CONSTRAINT_LINEAR;
+                row.terms = v.terms_;
+                row.params[0] = v.constant_;
+              }
+              else
+              {
+                row.type = MICMB_CONSTRAINT_EQUILIBRIUM;
+                row.terms = v.reactants_;
+                row.terms.insert(row.terms.end(), v.products_.begin(), v.products_.end());
+                row.n_reactants = (int32_t)v.reactants_.size();
+                row.params[0] = v.vant_hoff_param_.K_HLC_ref_;
+                row.params[1] = v.vant_hoff_param_.delta_H_;
+                row.params[2] = v.vant_hoff_param_.R_;
+                row.params[3] = v.vant_hoff_param_.T_ref_;
+              }
+              constraints_.push_back(std::move(row));
+            },
+            c.constraint_);
       return *this;
     }
     CudaSolverBuilderInPlace& SetIgnoreUnusedSpecies(bool ignore)
@@ -1176,6 +1339,28 @@ namespace micm
         }
         pstart.push_back((int32_t)pspecies.size());
       }
+      std::vector<int32_t> c_type, c_species, c_start{ 0 }, c_term_species, c_nreact;
+      std::vector<double> c_coef, c_params;
+      for (const auto& c : constraints_)
+      {
+        auto species_index = [&](const std::string& name) {
+          auto it = sys_index.find(name);
+          if (it == sys_index.end())
+            throw MicmException("MICM Constraint", 4, "Species '" + name + "' is not in the chemical system");
+          used.insert(name);
+          return it->second;
+        };
+        c_type.push_back(c.type);
+        c_species.push_back(species_index(c.species));
+        for (const auto& t : c.terms)
+        {
+          c_term_species.push_back(species_index(t.species_.name_));
+          c_coef.push_back(t.coefficient_);
+        }
+        c_start.push_back((int32_t)c_term_species.size());
+        c_nreact.push_back(c.n_reactants);
+        c_params.insert(c_params.end(), c.params, c.params + 4);
+      }
       if (!ignore_unused_species_)
         for (const auto& n : names)
           if (!used.count(n))
@@ -1193,6 +1378,17 @@ namespace micm
       d.n_parameterized = (int32_t)param_ids.size();
       d.parameterized_coef = pcoef.data();
       d.reorder_state = reorder_state_ ? 1 : 0;
+      d.n_constraints = (int32_t)constraints_.size();
+      if (!constraints_.empty())
+      {
+        d.constraint_type = c_type.data();
+        d.constraint_species = c_species.data();
+        d.constraint_term_start = c_start.data();
+        d.constraint_term_species = c_term_species.data();
+        d.constraint_term_coef = c_coef.data();
+        d.constraint_n_reactants = c_nreact.data();
+        d.constraint_params = c_params.data();
+      }
       micmb_mechanism* m = nullptr;
       detail::Check(micmb_mechanism_create(&d, &m));
       auto mech = std::shared_ptr<micmb_mechanism>(m, micmb_mechanism_destroy);
@@ -1231,7 +1427,15 @@ namespace micm
           labels[pcol[r] + 1] = b;
         }
       }
-      return Solver<L>(mech, options_, variable_names, labels, atol, R);
+      Solver<L> solver(mech, options_, variable_names, labels, atol, R);
+      if (!constraints_.empty())
+      {
+        std::vector<Real> mass(names.size(), 1.0);
+        for (const auto& c : constraints_)
+          mass[col[sys_index[c.species]]] = 0.0;
+        solver.SetConstraintRows(std::move(mass), constraints_.size());
+      }
+      return solver;
     }
   };
 

@@ -69,3 +69,58 @@ def test_micm_benchmark_mechanisms_build_unchanged(tmp_path):
     if not _has_gpu():
         r = subprocess.run([out], capture_output=True, text=True)
         assert r.returncode == 3 and "no CUDA device" in r.stderr
+
+
+@pytest.fixture(scope="module")
+def dae_binary(tmp_path_factory):
+    out = str(tmp_path_factory.mktemp("cpp") / "dae_example")
+    subprocess.run(["g++", "-std=c++20", "-O2", "-I" + os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "dae_example.cpp"), "-o", out, "-L" + LIB_DIR,
+                    "-lmicmb", "-Wl,-rpath," + LIB_DIR], check=True)
+    return out
+
+
+def test_cpp_constraints_api_compiles(dae_binary):
+    """micm's SetConstraints / EquilibriumConstraint / Constraint spelling builds
+    against micm.hpp (and reports the missing device without a GPU)."""
+    if _has_gpu():
+        pytest.skip("a GPU is present; covered by the gpu test")
+    r = subprocess.run([dae_binary], capture_output=True, text=True)
+    assert r.returncode == 3 and "no CUDA device" in r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method", ["plain", "fused"])
+def test_cpp_constraints_on_gpu_equal_restatement(cuda_device, dae_binary, method):
+    """The C++ DAE example (3 cells, equilibrium constraint started off
+    equilibrium) equals the restatement of micm's DAE Rosenbrock in its
+    correctly rounded mode bit for bit: global step control for "plain",
+    per-cell for "fused"."""
+    import sys
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    import oracle
+    from dae_cases import equilibrium, equilibrium_inputs
+    r = subprocess.run([dae_binary, method], capture_output=True, text=True)
+    assert r.returncode == 0, (r.returncode, r.stderr)
+    m = equilibrium()
+    inp = equilibrium_inputs(m, 3, False)
+    inp["temperature"] = np.array([280.0, 295.0, 310.0])
+    from micm_b200.mechanism import ideal_air_density
+    inp["air_density"] = ideal_air_density(inp["pressure"], inp["temperature"])
+    R = oracle.Restatement(m, tableau_kind=40, correctly_rounded=True)
+    y = inp["concentrations"]
+    t = 0.0
+    rows = [l.split() for l in r.stdout.strip().splitlines()]
+    assert [float(row[0]) for row in rows] == [1.0, 5.0, 20.0, 60.0]
+    for row in rows:
+        target = float(row[0])
+        if method == "plain":
+            y, st = R.solve_global(dict(inp, concentrations=y), target - t)
+            iters = st[9]
+        else:
+            y, st = R.solve_per_cell(dict(inp, concentrations=y), target - t, threads=1)
+            iters = st[:, 9].sum()
+        assert int(row[1]) == iters
+        np.testing.assert_array_equal(np.array([float(v) for v in row[2:]]).reshape(3, 3), y)
+        t = target
