@@ -79,6 +79,9 @@ namespace micmb
         cc.function_calls += P.new_f[s] ? 1 : 0;
     }
 
+    // DAE: the mechanism has algebraic constraints (a separate instantiation,
+    // so the constraint code costs the ODE kernels no registers)
+    template<bool DAE>
     __device__ __forceinline__ void fused_thread_body(const DevMech& M, const DevParams& P, const StepBounds& B,
                                                       const FusedArgs& A, double* ws, const ThreadLayout& T)
     {
@@ -108,7 +111,7 @@ namespace micmb
       ctl_init(c, B);
       int64_t cell = 0;
       int32_t n_ckpt = 0;
-      bool have = false, need_f0 = false;
+      bool have = false, need_f0 = false, need_init = false;
 
       auto write_out = [&]() {
         const size_t by = cell_base(cell, L, S);
@@ -150,19 +153,16 @@ namespace micmb
             kk[r] = A.rate_constants[bk + (size_t)r * L];
           ctl_init(c, B);
           n_ckpt = 0;
-          if (M.n_constraints)
+          if constexpr (DAE)
           {
-            // K_eq values, then micm's constraint initialisation of the algebraic variables
+            // K_eq values; the constraint initialisation runs in the attempt
+            // loop, outside this lambda, so that the lambda stays inlined
             const size_t bq = cell_base(cell, L, M.n_eq);
             for (int32_t q = 0; q < M.n_eq; ++q)
               kq[q] = A.keq[bq + (size_t)q * L];
-            const int32_t st = constraint_init_cell(M, P, kq, Y, Fc, LU, inv, cj, c);
-            if (st != MICMB_SOLVER_CONVERGED)
-            {
-              c.state = st;
-              write_out();
-              continue;
-            }
+            need_init = true;
+            have = true;
+            return;
           }
           if (ctl_begin_step(c, P, B))
           {
@@ -181,19 +181,42 @@ namespace micmb
       {
         if (!have)
           continue;
+        if (need_init)
+        {
+          // micm's constraint initialisation of the algebraic variables, then the first step
+          need_init = false;
+          const int32_t st = constraint_init_cell(M, P, kq, Y, Fc, LU, inv, cj, c);
+          if (st != MICMB_SOLVER_CONVERGED)
+            c.state = st;
+          else if (ctl_begin_step(c, P, B))
+          {
+            c.function_calls += 1;
+            c.jacobian_updates += 1;
+            need_f0 = true;
+          }
+          if (c.state != MICMB_SOLVER_RUNNING)
+          {
+            write_out();
+            claim();
+            continue;
+          }
+        }
         if (need_f0)
         {
           reaction_rates<1>(M, kk, Y, scr, 0);
           forcing_gather<1>(M, scr, F0, 0);
-          if (M.n_constraints)
+          if constexpr (DAE)
             constraint_forcing(M, kq, Y, F0);
         }
         const double H = c.H;
         const double alpha = 1.0 / (H * P.gamma0);
         jacobian_rates<1>(M, kk, Y, scr, 0);
-        if (M.n_constraints)
+        if constexpr (DAE)
           constraint_jacobian(M, kq, Y, cj);
-        thread_lu_gathered(M, scr, alpha, LU, inv, cj);  // -J + alpha M, then LU
+        if constexpr (DAE)
+          thread_lu_gathered(M, scr, alpha, LU, inv, cj);  // -J + alpha M, then LU
+        else
+          thread_lu_gathered(M, scr, alpha, LU, inv);  // -J + alpha I, then LU
         bool fc_is_src = false;
         for (int32_t st = 0; st < P.stages; ++st)
         {
@@ -209,7 +232,7 @@ namespace micmb
             }
             reaction_rates<1>(M, kk, Yn, scr, 0);
             forcing_gather<1>(M, scr, Fc, 0);
-            if (M.n_constraints)
+            if constexpr (DAE)
               constraint_forcing(M, kq, Yn, Fc);
             fc_is_src = true;
           }
@@ -220,7 +243,7 @@ namespace micmb
           for (int32_t i = 0; i < S; ++i)
           {
             double v = fc_is_src ? Fc[i] : F0[i];
-            if (!M.n_constraints || M.mass[i] != 0.0)  // algebraic rows have no mass coupling
+            if (!DAE || M.mass[i] != 0.0)  // algebraic rows have no mass coupling
               for (int32_t j = 0; j < st; ++j)
                 v += coh[j] * Kv(j)[i];
             Ks[i] = v;
@@ -240,7 +263,7 @@ namespace micmb
             e += P.e[st] * kv;
           }
           Yn[i] = v;
-          if (M.n_constraints && M.mass[i] == 0.0)
+          if (DAE && M.mass[i] == 0.0)
             e = v - Y[i];  // SetAlgebraicErrors: the step change
           sum += scaled_sq(Y[i], v, e, A.atol[i], A.rtol);
         }
@@ -298,48 +321,58 @@ namespace micmb
         atomicAdd(A.stats + threadIdx.x, block_stats[threadIdx.x]);
     }
 
+    template<bool DAE>
     __global__ void __launch_bounds__(kThreadsPerBlock, 5)
         k_fused_thread_r96(DevMech M, DevParams P, StepBounds B, FusedArgs A, double* ws, ThreadLayout T)
     {
-      fused_thread_body(M, P, B, A, ws, T);
+      fused_thread_body<DAE>(M, P, B, A, ws, T);
     }
 
+    template<bool DAE>
     __global__ void __launch_bounds__(kThreadsPerBlock, 8)
         k_fused_thread_r64(DevMech M, DevParams P, StepBounds B, FusedArgs A, double* ws, ThreadLayout T)
     {
-      fused_thread_body(M, P, B, A, ws, T);
+      fused_thread_body<DAE>(M, P, B, A, ws, T);
     }
 
+    template<bool DAE>
     __global__ void __launch_bounds__(kThreadsPerBlock, 12)
         k_fused_thread_r40(DevMech M, DevParams P, StepBounds B, FusedArgs A, double* ws, ThreadLayout T)
     {
-      fused_thread_body(M, P, B, A, ws, T);
+      fused_thread_body<DAE>(M, P, B, A, ws, T);
     }
 
+    template<bool DAE>
     __global__ void __launch_bounds__(kThreadsPerBlock, 16)
         k_fused_thread(DevMech M, DevParams P, StepBounds B, FusedArgs A, double* ws, ThreadLayout T)
     {
-      fused_thread_body(M, P, B, A, ws, T);
+      fused_thread_body<DAE>(M, P, B, A, ws, T);
     }
 
     using ThreadKernel = void (*)(DevMech, DevParams, StepBounds, FusedArgs, double*, ThreadLayout);
 
     // the build a configuration asks for (ctas_per_sm; 0 = full occupancy)
-    ThreadKernel ThreadKernelFor(const micmb_fused_config& cfg)
+    template<bool DAE>
+    ThreadKernel ThreadKernelBuild(const micmb_fused_config& cfg)
     {
       if (cfg.ctas_per_sm == 0 || cfg.ctas_per_sm > 12)
-        return k_fused_thread;
+        return k_fused_thread<DAE>;
       if (cfg.ctas_per_sm > 8)
-        return k_fused_thread_r40;
+        return k_fused_thread_r40<DAE>;
       if (cfg.ctas_per_sm > 5)
-        return k_fused_thread_r64;
-      return k_fused_thread_r96;
+        return k_fused_thread_r64<DAE>;
+      return k_fused_thread_r96<DAE>;
+    }
+
+    ThreadKernel ThreadKernelFor(const micmb_solver& s)
+    {
+      return s.mech->constraints.empty() ? ThreadKernelBuild<false>(s.fused) : ThreadKernelBuild<true>(s.fused);
     }
 
     int ThreadBlocksPerSm(const micmb_solver& s)
     {
       int per_sm = 0;
-      MICMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ThreadKernelFor(s.fused), kThreadsPerBlock, 0));
+      MICMB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ThreadKernelFor(s), kThreadsPerBlock, 0));
       if (s.fused.variant == 2 && s.fused.ctas_per_sm > 0)
         per_sm = std::min(per_sm, s.fused.ctas_per_sm);
       return per_sm;
@@ -366,7 +399,7 @@ namespace micmb
     const auto& m = *s.mech;
     const ThreadLayout T = MakeThreadLayout(m.S, m.R, s.params.stages, (int32_t)m.info_rxn.size(), m.nnz,
                                             (int32_t)m.c_term_col.size(), m.n_eq);
-    const ThreadKernel kernel = ThreadKernelFor(s.fused);
+    const ThreadKernel kernel = ThreadKernelFor(s);
     const int per_sm = ThreadBlocksPerSm(s);
     if (per_sm < 1)
       return false;
