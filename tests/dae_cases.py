@@ -106,3 +106,35 @@ def advance(solve, inputs, output_times):
             advanced += ft[0]
         t = target
         yield inputs["concentrations"], calls
+
+
+def simple_constrained():
+    """micm's constraint-initialisation unit-test system
+    (test/unit/solver/test_constraint_initialization.cpp:21-58): A -> B with
+    k = 0.5 and the equilibrium constraint C = K_eq B, K_eq = 2 with no
+    temperature dependence; micm's builder defaults (absolute tolerance 1e-3,
+    relative 1e-6), the species in system order."""
+    m = Mechanism(species=["A", "B", "C"], reactions=[], name="simple_constrained", reorder_state=False,
+                  absolute_tolerance=np.full(3, 1e-3), relative_tolerance=1e-6)
+    m.add(arrhenius(A=0.5), [0], [(1, 1.0)])
+    m.constraints.append(equilibrium_constraint(2, [(1, 1.0)], [(2, 1.0)], K_HLC_ref=2.0, delta_H=0.0,
+                                                name="B_C_eq"))
+    return m
+
+
+# the unit tests' initial states (A, B, C): consistent, mildly and severely
+# inconsistent (test_constraint_initialization.cpp:80-82, :117-119, :163-165),
+# and the multi-cell test's three cells (:246-259)
+SIMPLE_CONSISTENT = [1.0, 0.5, 1.0]
+SIMPLE_MILD = [1.0, 0.5, 5.0]
+SIMPLE_SEVERE = [1.0, 0.5, 1000.0]
+SIMPLE_MULTICELL = [[1.0, 0.5, 1.0], [2.0, 0.3, 5.0], [0.5, 0.1, 100.0]]
+
+
+def simple_inputs(rows):
+    y = np.array(rows, dtype=float).reshape(-1, 3)
+    n = len(y)
+    T = np.full(n, 298.15)
+    P = np.full(n, 101325.0)
+    return dict(temperature=T, pressure=P, air_density=ideal_air_density(P, T), concentrations=y,
+                custom_params=np.zeros((n, 0)))

@@ -10,8 +10,9 @@ import numpy as np
 import pytest
 
 import oracle
-from dae_cases import (equilibrium, equilibrium_inputs, negative_algebraic, negative_algebraic_inputs,
-                       terminator_robertson, terminator_robertson_inputs)
+from dae_cases import (SIMPLE_CONSISTENT, SIMPLE_MILD, SIMPLE_MULTICELL, SIMPLE_SEVERE, equilibrium,
+                       equilibrium_inputs, negative_algebraic, negative_algebraic_inputs, simple_constrained,
+                       simple_inputs, terminator_robertson, terminator_robertson_inputs)
 
 pytestmark = pytest.mark.skipif(not (oracle.restatement_available() and oracle.reference_available()),
                                 reason="oracle not built")
@@ -111,3 +112,53 @@ def test_global_restatement_follows_micms_multicell_state(name, make_mech, make_
         t = target
     if name == "negative_algebraic":
         assert np.all(y_r[:, 2] < 0.0)  # algebraic variables are not clamped
+
+
+
+def _residual(y):
+    return 2.0 * y[:, 1] - y[:, 2]
+
+
+@pytest.mark.parametrize("rows,max_iters,min_iters", [([SIMPLE_CONSISTENT], 1, 0), ([SIMPLE_MILD], 10, 1),
+                                                      ([SIMPLE_SEVERE], 10, 1)],
+                         ids=["consistent", "mildly_inconsistent", "severely_inconsistent"])
+def test_micm_constraint_initialisation_cases(rows, max_iters, min_iters):
+    """micm's ConstraintInitialization unit tests (3-stage tableau, one 1-cell
+    State, Solve(0.001)): the restatement equals micm bit for bit and both
+    meet the tests' expectations (converged, residual below 1e-6,
+    initialisation iterations as the tests bound them)."""
+    m = simple_constrained()
+    inp = simple_inputs(rows)
+    y_r, st_r = oracle.Restatement(m, tableau_kind=3).solve_per_cell(inp, 0.001, threads=1)
+    y_m, st_m = oracle.Reference(m, tableau=3).solve_per_cell(inp, 0.001, threads=1)
+    np.testing.assert_array_equal(y_r, y_m)
+    np.testing.assert_array_equal(st_r, st_m)
+    assert st_r[0, 7] == 2
+    assert min_iters <= st_r[0, 9] <= max_iters
+    assert abs(_residual(y_r)[0]) < 1e-6
+
+
+def test_micm_multicell_initialisation_and_reinitialisation():
+    """micm's MultiCellSystems test (one 3-cell State: consistent, mildly and
+    severely inconsistent cells) and SubsequentSolveCallsReinitialize (C
+    perturbed to 999 between solves), restatement against micm."""
+    m = simple_constrained()
+    inp = simple_inputs(SIMPLE_MULTICELL)
+    R = oracle.Restatement(m, tableau_kind=3)
+    ref = oracle.Reference(m, tableau=3)
+    y_r, st_r = R.solve_global(inp, 0.001)
+    y_m, st_m = ref.solve_global(inp, 0.001)
+    np.testing.assert_allclose(y_r, y_m, rtol=1e-12, atol=0)
+    for q, key in enumerate(oracle.STATS_FIELDS):
+        assert st_r[q] == st_m[0][key], key
+    assert st_r[7] == 2 and st_r[9] == st_m[0]["constraint_init_iterations"] >= 2
+    assert np.all(np.abs(_residual(y_r)) < 1e-5)
+    one = simple_inputs([SIMPLE_CONSISTENT])
+    y1, s1 = R.solve_per_cell(one, 0.001, threads=1)
+    y1[0, 2] = 999.0
+    y2, s2 = R.solve_per_cell(dict(one, concentrations=y1), 0.001, threads=1)
+    y2m, s2m = ref.solve_per_cell(dict(one, concentrations=y1), 0.001, threads=1)
+    np.testing.assert_array_equal(y2, y2m)
+    np.testing.assert_array_equal(s2, s2m)
+    assert s1[0, 7] == 2 and s2[0, 7] == 2 and s2[0, 9] >= 2
+    assert abs(_residual(y2)[0]) < 1e-6

@@ -96,3 +96,35 @@ def test_gpu_follows_micm(cuda_device, name, make_mech, make_inputs, tableau, ou
         total += len(st_m)
         t = target
     assert same >= 0.9 * total
+
+
+@pytest.mark.parametrize("method,step_control", [("plain", "global"), ("plain", "per_cell"), ("fused", "per_cell")])
+def test_gpu_micm_constraint_initialisation_cases(cuda_device, method, step_control):
+    """micm's ConstraintInitialization unit tests on the GPU: the three-cell
+    State (consistent, mildly and severely inconsistent cells), then C
+    perturbed to 999 in every cell and solved again; equal to the correctly
+    rounded restatement bit for bit, with the tests' expectations."""
+    from dae_cases import SIMPLE_MULTICELL, simple_constrained, simple_inputs
+    m = simple_constrained()
+    inp = simple_inputs(SIMPLE_MULTICELL)
+    R = oracle.Restatement(m, tableau_kind=3, correctly_rounded=True)
+    solver = Solver(m, 3, vector_length=4)
+    st = make_state(solver, inp)
+    solver.update_state_parameters(st)
+    y = inp["concentrations"]
+    for round_ in range(2):
+        if step_control == "global":
+            y, st_r = R.solve_global(dict(inp, concentrations=y), 0.001)
+            iters = st_r[9]
+        else:
+            y, st_r = R.solve_per_cell(dict(inp, concentrations=y), 0.001, threads=1)
+            iters = st_r[:, 9].sum()
+        res = solver.solve(0.001, st, method=method, step_control=step_control)
+        st.sync_outputs_to_host()
+        np.testing.assert_array_equal(st.concentrations(), y)
+        assert res.state == 2 and res.stats["constraint_init_iterations"] == iters
+        assert np.all(np.abs(2.0 * y[:, 1] - y[:, 2]) < 1e-5)
+        y = y.copy()
+        y[:, 2] = 999.0
+        st.set_concentrations(y)
+        st.sync_inputs_to_device()
