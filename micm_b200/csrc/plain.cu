@@ -140,6 +140,7 @@ namespace micmb
     }
 
     // F0 = f(Y) for cells starting a step
+    template<bool DAE>
     __global__ void k_forcing0(DevMech M, PlainArgs a)
     {
       const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -152,11 +153,12 @@ namespace micmb
       Strided f{ a.f0 + cell_base(c, L, M.S), L };
       reaction_rates<1>(M, k, y, rate, 0);
       forcing_gather<1>(M, rate, f, 0);
-      if (M.n_constraints)
+      if constexpr (DAE)
         constraint_forcing(M, keq_of(M, a, c), y, f);
     }
 
     // alpha I - J at Y for every running cell (micm re-assembles after a rejection)
+    template<bool DAE>
     __global__ void k_jacobian(DevMech M, PlainArgs a, double gamma0)
     {
       const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -170,7 +172,7 @@ namespace micmb
       Strided dr{ a.scratch + cell_base(c, L, a.scratch_cols), L };
       Strided J{ a.jac + cell_base(c, L, M.nnz), L };
       jacobian_rates<1>(M, k, y, dr, 0);
-      if (M.n_constraints)
+      if constexpr (DAE)
       {
         const Strided cj = cjac_of(M, a, c);
         constraint_jacobian(M, keq_of(M, a, c), y, cj);
@@ -192,6 +194,7 @@ namespace micmb
     }
 
     // Ynew = Y + sum_j a_sj K_j ; Fcur = f(Ynew)
+    template<bool DAE>
     __global__ void k_stage_forcing(DevMech M, PlainArgs a, DevParams P, int32_t s)
     {
       const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -214,11 +217,12 @@ namespace micmb
       Strided f{ a.fcur + bs, L };
       reaction_rates<1>(M, k, yn, rate, 0);
       forcing_gather<1>(M, rate, f, 0);
-      if (M.n_constraints)
+      if constexpr (DAE)
         constraint_forcing(M, keq_of(M, a, c), yn, f);
     }
 
     // K_s = F + sum_j (c_sj / H) K_j ; K_s = (LU)^-1 K_s
+    template<bool DAE>
     __global__ void k_stage_solve(DevMech M, PlainArgs a, DevParams P, int32_t s, int32_t src_is_f0)
     {
       const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -237,7 +241,7 @@ namespace micmb
       for (int32_t i = 0; i < S; ++i)
       {
         double v = F[i];
-        if (!M.n_constraints || M.mass[i] != 0.0)  // algebraic rows have no mass coupling
+        if (!DAE || M.mass[i] != 0.0)  // algebraic rows have no mass coupling
           for (int32_t j = 0; j < s; ++j)
             v += coh[j] * a.K[bk + (size_t)(j * S + i) * L];
         Ks[i] = v;
@@ -248,6 +252,7 @@ namespace micmb
 
     // Ynew = Y + sum m_s K_s ; Yerr = sum e_s K_s ; the cell's sum of scaled
     // squared errors in species order (micm's order).
+    template<bool DAE>
     __device__ double finish_cell(const DevMech& M, const PlainArgs& a, const DevParams& P, int64_t c)
     {
       const int32_t L = a.L, S = M.S;
@@ -267,7 +272,7 @@ namespace micmb
           e += P.e[st] * kv;
         }
         yn[i] = v;
-        if (M.n_constraints && M.mass[i] == 0.0)
+        if (DAE && M.mass[i] == 0.0)
           e = v - y[i];  // SetAlgebraicErrors: the step change
         sum += scaled_sq(y[i], v, e, a.atol[i], a.rtol);
       }
@@ -477,12 +482,13 @@ namespace micmb
         cc.function_calls += P.new_f[s] ? 1 : 0;
     }
 
+    template<bool DAE>
     __global__ void k_finish_per_cell(DevMech M, PlainArgs a, DevParams P, StepBounds b)
     {
       const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
       if (c >= a.n || !running(a, c))
         return;
-      const double error = error_from_sum(finish_cell(M, a, P, c), (double)M.S);
+      const double error = error_from_sum(finish_cell<DAE>(M, a, P, c), (double)M.S);
       CellCtl cc = a.ctl[c];
       count_attempt(cc, P);
       const int res = ctl_after_error(cc, P, b, error);
@@ -514,13 +520,14 @@ namespace micmb
     // Global mode, first level: each cell's sum in species order, then one
     // partial per block (fixed tree over its kBlock cells) in blk_err[block].
     // A single cell's error therefore equals micm's bit for bit.
+    template<bool DAE>
     __global__ void k_finish_partial(DevMech M, PlainArgs a, DevParams P, double* blk_err)
     {
       __shared__ double red[kBlock];
       const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
       if (a.status[0] != MICMB_SOLVER_RUNNING)
         return;  // uniform over the grid in global mode
-      const double v = (c < a.n) ? finish_cell(M, a, P, c) : 0.0;
+      const double v = (c < a.n) ? finish_cell<DAE>(M, a, P, c) : 0.0;
       const double t = block_tree_sum(v, red);
       if (threadIdx.x == 0)
         blk_err[blockIdx.x] = t;
@@ -800,6 +807,9 @@ namespace micmb
       }
     }
     const unsigned grid = Blocks(n);
+    // mechanisms with constraints run their own instantiations of the stage
+    // kernels, so the constraint code costs the ODE kernels no registers
+    const bool dae = !m.constraints.empty();
     int64_t attempts = 0;
     int64_t batch = 8;
     const int64_t max_attempts = (int64_t)(P.max_steps + 2) * 2000;
@@ -808,18 +818,20 @@ namespace micmb
       for (int64_t it = 0; it < batch; ++it)
       {
         k_step_begin<<<Blocks(n_ctl), kBlock, 0, stream>>>(a, P, b, n_ctl);
-        k_forcing0<<<grid, kBlock, 0, stream>>>(s.dev, a);
-        k_jacobian<<<grid, kBlock, 0, stream>>>(s.dev, a, P.gamma0);
+        (dae ? k_forcing0<true> : k_forcing0<false>)<<<grid, kBlock, 0, stream>>>(s.dev, a);
+        (dae ? k_jacobian<true> : k_jacobian<false>)<<<grid, kBlock, 0, stream>>>(s.dev, a, P.gamma0);
         k_decompose<<<grid, kBlock, 0, stream>>>(s.dev, a);
         for (int32_t stg = 0; stg < P.stages; ++stg)
         {
           if (stg > 0 && P.new_f[stg])
-            k_stage_forcing<<<grid, kBlock, 0, stream>>>(s.dev, a, P, stg);
-          k_stage_solve<<<grid, kBlock, 0, stream>>>(s.dev, a, P, stg, src_is_f0[stg]);
+            (dae ? k_stage_forcing<true> : k_stage_forcing<false>)<<<grid, kBlock, 0, stream>>>(s.dev, a, P, stg);
+          (dae ? k_stage_solve<true> : k_stage_solve<false>)<<<grid, kBlock, 0, stream>>>(s.dev, a, P, stg,
+                                                                                          src_is_f0[stg]);
         }
         if (global)
         {
-          k_finish_partial<<<grid, kBlock, 0, stream>>>(s.dev, a, P, a.err_cell);
+          (dae ? k_finish_partial<true> : k_finish_partial<false>)<<<grid, kBlock, 0, stream>>>(s.dev, a, P,
+                                                                                                a.err_cell);
           if (st.gx_fn)
           {
             double* gx = st.gx_buf.as<double>();
@@ -835,7 +847,7 @@ namespace micmb
           k_global_apply<<<grid, kBlock, 0, stream>>>(s.dev, a, last_accept);
         }
         else
-          k_finish_per_cell<<<grid, kBlock, 0, stream>>>(s.dev, a, P, b);
+          (dae ? k_finish_per_cell<true> : k_finish_per_cell<false>)<<<grid, kBlock, 0, stream>>>(s.dev, a, P, b);
         MICMB_CUDA(cudaGetLastError());
       }
       attempts += batch;
