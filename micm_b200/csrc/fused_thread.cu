@@ -33,13 +33,16 @@ namespace micmb
       return (size_t)(c / L) * (size_t)L * (size_t)ncol + (size_t)(c % L);
     }
 
+    static_assert(sizeof(CellCtl) == 8 * sizeof(double), "a lane's CellCtl record is 8 doubles");
+
     // entry offsets (each entry = 32 doubles, one per lane) of a thread's working set
     struct ThreadLayout
     {
-      int32_t oY, oYn, oF0, oFc, oK, oLU, oInv, oKk, oScr, oCj, oKeq, per_slot;
+      int32_t oY, oYn, oF0, oFc, oK, oLU, oInv, oKk, oScr, oCj, oKeq, oCtl, per_slot;
     };
 
-    // oCj / oKeq: constraint Jacobian terms and K_eq values (DAE mechanisms only)
+    // oCj / oKeq: constraint Jacobian terms and K_eq values (DAE mechanisms only);
+    // oCtl: 32 CellCtl records (8 doubles each), one per lane
     ThreadLayout MakeThreadLayout(int32_t S, int32_t R, int32_t stages, int32_t n_info, int32_t nnz,
                                   int32_t n_cterms = 0, int32_t n_eq = 0)
     {
@@ -67,6 +70,8 @@ namespace micmb
       o += n_cterms;
       t.oKeq = o;
       o += n_eq;
+      t.oCtl = o;
+      o += 8;  // the lanes' CellCtl records, 64 bytes each
       t.per_slot = o;
       return t;
     }
@@ -107,7 +112,12 @@ namespace micmb
       if (threadIdx.x < 9)
         block_stats[threadIdx.x] = 0;
       __syncthreads();
-      CellCtl c;
+      // The cell's step-control record stays in the warp's working-set slot
+      // (64 bytes per lane), not in registers: it is read a few times per
+      // attempt, and out of the register budget it no longer pushes the LU
+      // and solve loops' values into spills (+5 % at 1M cells, 210 species).
+      CellCtl& c = *reinterpret_cast<CellCtl*>(ws + (size_t)wslot * (size_t)T.per_slot * 32 + (size_t)T.oCtl * 32 +
+                                               (size_t)lane * 8);
       ctl_init(c, B);
       int64_t cell = 0;
       int32_t n_ckpt = 0;
