@@ -107,7 +107,7 @@ namespace micmb
 
     struct SchedOffsets
     {
-      size_t ls, tg, ax, ts, ta, tb;
+      size_t ls, tg, ax, ts, ta, tb, tab;
       int32_t n_levels;
     };
 
@@ -120,6 +120,13 @@ namespace micmb
       o.ts = pk.add(s.term_start);
       o.ta = pk.add(s.term_a);
       o.tb = pk.add(s.term_b);
+      std::vector<int32_t> tab(2 * s.term_a.size());
+      for (size_t t = 0; t < s.term_a.size(); ++t)
+      {
+        tab[2 * t] = s.term_a[t];
+        tab[2 * t + 1] = s.term_b[t];
+      }
+      o.tab = pk.add(tab);
       o.n_levels = s.n_levels();
       return o;
     }
@@ -194,6 +201,7 @@ namespace micmb
       d.term_start = reinterpret_cast<const int32_t*>(base + o.ts);
       d.ta = reinterpret_cast<const int32_t*>(base + o.ta);
       d.tb = reinterpret_cast<const int32_t*>(base + o.tb);
+      d.tab = reinterpret_cast<const int2*>(base + o.tab);
       return d;
     }
 

@@ -32,6 +32,7 @@ namespace micmb
     const int32_t* term_start;
     const int32_t* ta;
     const int32_t* tb;
+    const int2* tab;  // (ta, tb) of each term in one 8-byte load
   };
 
   // register-blocked serial schedule (mechanism.hpp BlockedSchedule)
@@ -419,7 +420,10 @@ namespace micmb
         const int32_t e = sch.target[it];
         double v = A[e];
         for (int32_t t = sch.term_start[it]; t < sch.term_start[it + 1]; ++t)
-          v -= A[sch.ta[t]] * A[sch.tb[t]];
+        {
+          const int2 ab = sch.tab[t];
+          v -= A[ab.x] * A[ab.y];
+        }
         const int32_t aux = sch.aux[it];  // -2: partial sum (stored, finalised by a later unit)
         if (aux >= 0)
           v *= inv[diag_row[aux]];
@@ -464,7 +468,10 @@ namespace micmb
         if (dr >= 0)
           v += M.n_constraints ? alpha * M.mass[dr] : alpha;
         for (int32_t t = sch.term_start[it]; t < sch.term_start[it + 1]; ++t)
-          v -= A[sch.ta[t]] * A[sch.tb[t]];
+        {
+          const int2 ab = sch.tab[t];
+          v -= A[ab.x] * A[ab.y];
+        }
         const int32_t aux = sch.aux[it];
         if (aux >= 0)
           v *= inv[diag_row[aux]];
@@ -628,7 +635,10 @@ namespace micmb
         const int32_t i = sch.target[it];
         double v = x[i];
         for (int32_t t = sch.term_start[it]; t < sch.term_start[it + 1]; ++t)
-          v -= A[sch.ta[t]] * x[sch.tb[t]];
+        {
+          const int2 ab = sch.tab[t];
+          v -= A[ab.x] * x[ab.y];
+        }
         x[i] = v;
       }
       lane_sync<NL>();
@@ -647,7 +657,10 @@ namespace micmb
         const int32_t i = sch.target[it];
         double v = x[i];
         for (int32_t t = sch.term_start[it]; t < sch.term_start[it + 1]; ++t)
-          v -= A[sch.ta[t]] * x[sch.tb[t]];
+        {
+          const int2 ab = sch.tab[t];
+          v -= A[ab.x] * x[ab.y];
+        }
         const int32_t aux = sch.aux[it];  // -2: partial sum
         x[i] = aux >= 0 ? v / A[aux] : v;
       }
