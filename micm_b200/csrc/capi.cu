@@ -107,7 +107,7 @@ namespace micmb
 
     struct SchedOffsets
     {
-      size_t ls, tg, ax, ts, ta, tb, tab;
+      size_t ls, tg, ax, ts, ta, tb, tab, item, item_j = 0;
       int32_t n_levels;
     };
 
@@ -127,6 +127,15 @@ namespace micmb
         tab[2 * t + 1] = s.term_b[t];
       }
       o.tab = pk.add(tab);
+      std::vector<int32_t> item(4 * s.item_target.size());
+      for (size_t it = 0; it < s.item_target.size(); ++it)
+      {
+        item[4 * it] = s.item_target[it];
+        item[4 * it + 1] = s.term_start[it];
+        item[4 * it + 2] = s.term_start[it + 1];
+        item[4 * it + 3] = s.item_aux[it];
+      }
+      o.item = pk.add(item);
       o.n_levels = s.n_levels();
       return o;
     }
@@ -202,6 +211,8 @@ namespace micmb
       d.ta = reinterpret_cast<const int32_t*>(base + o.ta);
       d.tb = reinterpret_cast<const int32_t*>(base + o.tb);
       d.tab = reinterpret_cast<const int2*>(base + o.tab);
+      d.item = reinterpret_cast<const int4*>(base + o.item);
+      d.item_j = o.item_j ? reinterpret_cast<const int4*>(base + o.item_j) : nullptr;
       return d;
     }
 
@@ -238,6 +249,29 @@ namespace micmb
       const SchedOffsets lus = AddSchedule(pk, m.lu_serial), fws = AddSchedule(pk, m.fwd_serial),
                          bws = AddSchedule(pk, m.bwd_serial), fwts = AddSchedule(pk, m.fwd_t_serial),
                          bwts = AddSchedule(pk, m.bwd_t_serial);
+      // the serial LU's per-item Jacobian gather range and diagonal rows
+      SchedOffsets lus_j = lus;
+      {
+        const auto& ls = m.lu_serial;
+        std::vector<int32_t> ij(4 * ls.item_target.size());
+        for (size_t it = 0; it < ls.item_target.size(); ++it)
+        {
+          const int32_t e = ls.item_target[it], aux = ls.item_aux[it];
+          ij[4 * it] = diag_row_of[e];
+          ij[4 * it + 1] = m.j_start[e];
+          ij[4 * it + 2] = m.j_start[e + 1];
+          ij[4 * it + 3] = aux >= 0 ? diag_row_of[aux] : -1;
+        }
+        lus_j.item_j = pk.add(ij);
+      }
+      std::vector<double> jterm(2 * m.j_info.size());
+      for (size_t t = 0; t < m.j_info.size(); ++t)
+      {
+        jterm[2 * t] = m.j_coef[t];
+        int64_t bits = (int64_t)(uint32_t)m.j_info[t];
+        std::memcpy(&jterm[2 * t + 1], &bits, sizeof bits);
+      }
+      const size_t o_jt = pk.add(jterm);
       const size_t o_rd = pk.add(m.rate_desc), o_drd = pk.add(m.drate_desc);
       // algebraic constraints
       std::vector<int32_t> con4, con2;
@@ -314,6 +348,7 @@ namespace micmb
       d.j_start = reinterpret_cast<const int32_t*>(b + o_js);
       d.j_info = reinterpret_cast<const int32_t*>(b + o_ji);
       d.j_coef = reinterpret_cast<const double*>(b + o_jc);
+      d.jterm = reinterpret_cast<const JTerm*>(b + o_jt);
       d.diag_pos = reinterpret_cast<const int32_t*>(b + o_dp);
       d.diag_row_of = reinterpret_cast<const int32_t*>(b + o_dro);
       d.lu = Resolve(b, lu);
@@ -321,7 +356,7 @@ namespace micmb
       d.bwd = Resolve(b, bw);
       d.fwd_t = Resolve(b, fwt);
       d.bwd_t = Resolve(b, bwt);
-      d.lu_s = Resolve(b, lus);
+      d.lu_s = Resolve(b, lus_j);
       d.fwd_s = Resolve(b, fws);
       d.bwd_s = Resolve(b, bws);
       d.fwd_t_s = Resolve(b, fwts);

@@ -33,6 +33,19 @@ namespace micmb
     const int32_t* ta;
     const int32_t* tb;
     const int2* tab;  // (ta, tb) of each term in one 8-byte load
+    // per item in one 16-byte load: {target, first term, end of terms, aux}
+    const int4* item;
+    // serial LU schedule only (else nullptr): per item {diag row of the
+    // target or -1, first Jacobian gather term, end of them, diag row of aux}
+    const int4* item_j;
+  };
+
+  // one Jacobian gather term (coefficient and Jacobian-info index) in one 16-byte load
+  struct alignas(16) JTerm
+  {
+    double coef;
+    int32_t info;
+    int32_t pad;
   };
 
   // register-blocked serial schedule (mechanism.hpp BlockedSchedule)
@@ -83,6 +96,7 @@ namespace micmb
     const int32_t* j_start;
     const int32_t* j_info;
     const double* j_coef;
+    const JTerm* jterm;  // j_coef and j_info together
     const int32_t* diag_pos;     // [S] storage position of a_ii
     const int32_t* diag_row_of;  // [nnz] row i if the position holds a_ii, else -1
     DevSchedule lu, fwd, bwd, fwd_t, bwd_t;
@@ -388,7 +402,10 @@ namespace micmb
     {
       double acc = 0.0;
       for (int32_t t = M.j_start[e]; t < M.j_start[e + 1]; ++t)
-        acc += M.j_coef[t] * drate[M.j_info[t]];
+      {
+        const JTerm jt = M.jterm[t];
+        acc += jt.coef * drate[jt.info];
+      }
       if (M.n_constraints)
         for (int32_t t = M.cj_start[e]; t < M.cj_start[e + 1]; ++t)
           acc -= cj[M.cj_term[t]];
@@ -417,14 +434,15 @@ namespace micmb
       const int32_t end = sch.level_start[l + 1];
       for (int32_t it = sch.level_start[l] + lane; it < end; it += NL)
       {
-        const int32_t e = sch.target[it];
+        const int4 rec = sch.item[it];
+        const int32_t e = rec.x;
         double v = A[e];
-        for (int32_t t = sch.term_start[it]; t < sch.term_start[it + 1]; ++t)
+        for (int32_t t = rec.y; t < rec.z; ++t)
         {
           const int2 ab = sch.tab[t];
           v -= A[ab.x] * A[ab.y];
         }
-        const int32_t aux = sch.aux[it];  // -2: partial sum (stored, finalised by a later unit)
+        const int32_t aux = rec.w;  // -2: partial sum (stored, finalised by a later unit)
         if (aux >= 0)
           v *= inv[diag_row[aux]];
         A[e] = v;
@@ -451,34 +469,38 @@ namespace micmb
                                                         const int32_t* diag_row, DV drate, double alpha, AV A, IV inv,
                                                         CV cj)
   {
-    for (int32_t l = 0; l < sch.n_levels; ++l)
+    // sch is the serial LU schedule (item_j present); diag_row is folded into item_j
+    (void)diag_row;
+    const int32_t n_items = sch.level_start[sch.n_levels];
+    for (int32_t it = 0; it < n_items; ++it)
     {
-      const int32_t end = sch.level_start[l + 1];
-      for (int32_t it = sch.level_start[l]; it < end; ++it)
-      {
-        const int32_t e = sch.target[it];
-        double v = 0.0;
-        if constexpr (PROCESS)
-          for (int32_t t = M.j_start[e]; t < M.j_start[e + 1]; ++t)
-            v += M.j_coef[t] * drate[M.j_info[t]];
-        if (M.n_constraints)
-          for (int32_t t = M.cj_start[e]; t < M.cj_start[e + 1]; ++t)
-            v -= cj[M.cj_term[t]];
-        const int32_t dr = diag_row[e];
-        if (dr >= 0)
-          v += M.n_constraints ? alpha * M.mass[dr] : alpha;
-        for (int32_t t = sch.term_start[it]; t < sch.term_start[it + 1]; ++t)
+      const int4 rec = sch.item[it];
+      const int4 rj = sch.item_j[it];
+      const int32_t e = rec.x;
+      double v = 0.0;
+      if constexpr (PROCESS)
+        for (int32_t t = rj.y; t < rj.z; ++t)
         {
-          const int2 ab = sch.tab[t];
-          v -= A[ab.x] * A[ab.y];
+          const JTerm jt = M.jterm[t];
+          v += jt.coef * drate[jt.info];
         }
-        const int32_t aux = sch.aux[it];
-        if (aux >= 0)
-          v *= inv[diag_row[aux]];
-        A[e] = v;
-        if (aux != -2 && dr >= 0)
-          inv[dr] = 1.0 / v;
+      if (M.n_constraints)
+        for (int32_t t = M.cj_start[e]; t < M.cj_start[e + 1]; ++t)
+          v -= cj[M.cj_term[t]];
+      const int32_t dr = rj.x;
+      if (dr >= 0)
+        v += M.n_constraints ? alpha * M.mass[dr] : alpha;
+      for (int32_t t = rec.y; t < rec.z; ++t)
+      {
+        const int2 ab = sch.tab[t];
+        v -= A[ab.x] * A[ab.y];
       }
+      const int32_t aux = rec.w;
+      if (aux >= 0)
+        v *= inv[rj.w];
+      A[e] = v;
+      if (aux != -2 && dr >= 0)
+        inv[dr] = 1.0 / v;
     }
   }
 
@@ -632,9 +654,10 @@ namespace micmb
       const int32_t end = sch.level_start[l + 1];
       for (int32_t it = sch.level_start[l] + lane; it < end; it += NL)
       {
-        const int32_t i = sch.target[it];
+        const int4 rec = sch.item[it];
+        const int32_t i = rec.x;
         double v = x[i];
-        for (int32_t t = sch.term_start[it]; t < sch.term_start[it + 1]; ++t)
+        for (int32_t t = rec.y; t < rec.z; ++t)
         {
           const int2 ab = sch.tab[t];
           v -= A[ab.x] * x[ab.y];
@@ -654,14 +677,15 @@ namespace micmb
       const int32_t end = sch.level_start[l + 1];
       for (int32_t it = sch.level_start[l] + lane; it < end; it += NL)
       {
-        const int32_t i = sch.target[it];
+        const int4 rec = sch.item[it];
+        const int32_t i = rec.x;
         double v = x[i];
-        for (int32_t t = sch.term_start[it]; t < sch.term_start[it + 1]; ++t)
+        for (int32_t t = rec.y; t < rec.z; ++t)
         {
           const int2 ab = sch.tab[t];
           v -= A[ab.x] * x[ab.y];
         }
-        const int32_t aux = sch.aux[it];  // -2: partial sum
+        const int32_t aux = rec.w;  // -2: partial sum
         x[i] = aux >= 0 ? v / A[aux] : v;
       }
       lane_sync<NL>();
