@@ -437,6 +437,7 @@ namespace micmb
         const int4 rec = sch.item[it];
         const int32_t e = rec.x;
         double v = A[e];
+#pragma unroll 2
         for (int32_t t = rec.y; t < rec.z; ++t)
         {
           const int2 ab = sch.tab[t];
@@ -490,6 +491,8 @@ namespace micmb
       const int32_t dr = rj.x;
       if (dr >= 0)
         v += M.n_constraints ? alpha * M.mass[dr] : alpha;
+      // two terms per iteration: their four operand loads issue together
+#pragma unroll 2
       for (int32_t t = rec.y; t < rec.z; ++t)
       {
         const int2 ab = sch.tab[t];
@@ -657,6 +660,7 @@ namespace micmb
         const int4 rec = sch.item[it];
         const int32_t i = rec.x;
         double v = x[i];
+#pragma unroll 2
         for (int32_t t = rec.y; t < rec.z; ++t)
         {
           const int2 ab = sch.tab[t];
@@ -680,6 +684,7 @@ namespace micmb
         const int4 rec = sch.item[it];
         const int32_t i = rec.x;
         double v = x[i];
+#pragma unroll 2
         for (int32_t t = rec.y; t < rec.z; ++t)
         {
           const int2 ab = sch.tab[t];
