@@ -286,6 +286,7 @@ namespace micmb
     for (int32_t s = lane; s < M.S; s += NL)
     {
       double acc = 0.0;
+#pragma unroll 2
       for (int32_t t = M.f_start[s]; t < M.f_start[s + 1]; ++t)
         acc += M.f_coef[t] * rate[M.f_rxn[t]];
       f[s] = acc;
@@ -480,6 +481,7 @@ namespace micmb
       const int32_t e = rec.x;
       double v = 0.0;
       if constexpr (PROCESS)
+#pragma unroll 2
         for (int32_t t = rj.y; t < rj.z; ++t)
         {
           const JTerm jt = M.jterm[t];
