@@ -402,6 +402,7 @@ namespace micmb
     for (int32_t e = lane; e < M.nnz; e += NL)
     {
       double acc = 0.0;
+#pragma unroll 2
       for (int32_t t = M.j_start[e]; t < M.j_start[e + 1]; ++t)
       {
         const JTerm jt = M.jterm[t];
