@@ -138,3 +138,41 @@ def simple_inputs(rows):
     P = np.full(n, 101325.0)
     return dict(temperature=T, pressure=P, air_density=ideal_air_density(P, T), concentrations=y,
                 custom_params=np.zeros((n, 0)))
+
+
+def overshoot_linear():
+    """micm's DAE overshoot case (test/integration/test_dae_constraint_overshoot.cpp:44-129):
+    a fast A -> B (k = 1e4) with the conservation A + B + C = 1e-6 replacing
+    C's row; absolute tolerance 1e-12, relative 1e-6."""
+    m = Mechanism(species=["A", "B", "C"], reactions=[], name="overshoot_linear", reorder_state=False,
+                  absolute_tolerance=np.full(3, 1e-12), relative_tolerance=1e-6)
+    m.add(arrhenius(A=1.0e4), [0], [(1, 1.0)])
+    m.constraints.append(linear_constraint(2, [(0, 1.0), (1, 1.0), (2, 1.0)], 1.0e-6, name="mass_conservation"))
+    return m
+
+
+def overshoot_linear_inputs():
+    return dict(temperature=np.array([298.0]), pressure=np.array([101325.0]),
+                air_density=ideal_air_density(np.array([101325.0]), np.array([298.0])),
+                concentrations=np.array([[0.9e-6, 0.0, 0.1e-6]]), custom_params=np.zeros((1, 0)))
+
+
+def overshoot_equilibrium():
+    """micm's equilibrium-plus-conservation overshoot case (:131-234): A_aq -> P
+    (k = 1e3), A_aq held at K_eq = 10 times A_gas, and A_aq + P + A_gas = 1e-6
+    replacing A_gas's row; absolute tolerances 1e-8 for the two A species,
+    1e-12 for P."""
+    m = Mechanism(species=["A_gas", "A_aq", "P"], reactions=[], name="overshoot_equilibrium", reorder_state=False,
+                  absolute_tolerance=np.array([1e-8, 1e-8, 1e-12]), relative_tolerance=1e-6)
+    m.add(arrhenius(A=1.0e3), [1], [(2, 1.0)])
+    m.constraints.append(equilibrium_constraint(1, [(0, 1.0)], [(1, 1.0)], K_HLC_ref=10.0, delta_H=0.0,
+                                                name="gas_aq_eq"))
+    m.constraints.append(linear_constraint(0, [(1, 1.0), (2, 1.0), (0, 1.0)], 1.0e-6, name="mass_conservation"))
+    return m
+
+
+def overshoot_equilibrium_inputs():
+    a_gas = 1.0e-6 / 11.0
+    return dict(temperature=np.array([298.0]), pressure=np.array([101325.0]),
+                air_density=ideal_air_density(np.array([101325.0]), np.array([298.0])),
+                concentrations=np.array([[a_gas, 10.0 * a_gas, 0.0]]), custom_params=np.zeros((1, 0)))
