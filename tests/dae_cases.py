@@ -176,3 +176,22 @@ def overshoot_equilibrium_inputs():
     return dict(temperature=np.array([298.0]), pressure=np.array([101325.0]),
                 air_density=ideal_air_density(np.array([101325.0]), np.array([298.0])),
                 concentrations=np.array([[a_gas, 10.0 * a_gas, 0.0]]), custom_params=np.zeros((1, 0)))
+
+
+def cascade(balance_atol, k, K1, K2):
+    """micm's algebraic-error cascade (test/integration/
+    test_dae_algebraic_error_insensitivity.cpp:43-170): B_aq -> P with rate k,
+    A_aq = K1 A_gas and B_aq = K2 A_aq held by equilibrium constraints, and
+    A_aq + B_aq + P + A_gas = 1e-6 replacing A_gas's row; A_gas's absolute
+    tolerance is `balance_atol`.  Returns (mechanism, consistent inputs)."""
+    m = Mechanism(species=["A_gas", "A_aq", "B_aq", "P"], reactions=[], name="cascade", reorder_state=False,
+                  absolute_tolerance=np.array([balance_atol, 1e-8, 1e-8, 1e-12]), relative_tolerance=1e-6)
+    m.add(arrhenius(A=k), [2], [(3, 1.0)])
+    m.constraints.append(equilibrium_constraint(1, [(0, 1.0)], [(1, 1.0)], K_HLC_ref=K1, delta_H=0.0, name="eq1"))
+    m.constraints.append(equilibrium_constraint(2, [(1, 1.0)], [(2, 1.0)], K_HLC_ref=K2, delta_H=0.0, name="eq2"))
+    m.constraints.append(linear_constraint(0, [(1, 1.0), (2, 1.0), (3, 1.0), (0, 1.0)], 1.0e-6, name="mass"))
+    ag0 = 1.0e-6 / (1.0 + K1 + K1 * K2)
+    inputs = dict(temperature=np.array([298.0]), pressure=np.array([101325.0]),
+                  air_density=ideal_air_density(np.array([101325.0]), np.array([298.0])),
+                  concentrations=np.array([[ag0, K1 * ag0, K2 * K1 * ag0, 0.0]]), custom_params=np.zeros((1, 0)))
+    return m, inputs

@@ -206,3 +206,35 @@ def test_micm_overshoot_equilibrium_plus_conservation():
     for s in states:
         assert abs(s.sum() - 1.0e-6) < 1e-12
         assert s[0] >= -1.0e-8
+
+
+def _accepted(m, inp, dt):
+    """restatement == micm on every call of micm's loop; (states, accepted steps)"""
+    R = oracle.Restatement(m, tableau_kind=40)
+    ref = oracle.Reference(m, tableau=40)
+    y, advanced, states, acc = inp["concentrations"], 0.0, [], 0
+    while advanced < dt:
+        y_r, st_r = R.solve_per_cell(dict(inp, concentrations=y), dt - advanced, threads=1)
+        y_m, st_m = ref.solve_per_cell(dict(inp, concentrations=y), dt - advanced, threads=1)
+        np.testing.assert_array_equal(y_r, y_m)
+        np.testing.assert_array_equal(st_r, st_m)
+        assert st_r[0, 7] == 2
+        advanced += float(st_r[0:1, 8:9].view(np.float64)[0, 0])
+        acc += int(st_r[0, 3])
+        y = y_r
+        states.append(y[0].copy())
+    return states, acc
+
+
+def test_micm_algebraic_error_cascade():
+    """micm's DAEAlgebraicError tests: a tight absolute tolerance on the
+    balance variable takes more steps than a loose one (the algebraic rows'
+    step-change error counts), and the ultra-stiff cascade does not overshoot;
+    the restatement equals micm on every call of each run."""
+    from dae_cases import cascade
+    _, loose = _accepted(*cascade(1e-3, 100.0, 2.0, 2.0), 30.0)
+    _, tight = _accepted(*cascade(1e-8, 100.0, 2.0, 2.0), 30.0)
+    assert tight > loose
+    states, _ = _accepted(*cascade(1e-8, 1.0e4, 100.0, 50.0), 30.0)
+    assert min(s[0] for s in states) >= -1.0e-8
+    assert abs(states[-1][3] - 1.0e-6) < 1e-8 and abs(states[-1][0]) < 1e-10
