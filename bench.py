@@ -228,7 +228,7 @@ def cpu_reference(mech, cfg, inputs, sample: int, uniform: bool = False):
 
 def parity_summary(y_gpu, acc_gpu, y_ref, acc_ref, rtol=1e-6, atol=1e-12):
     """The GPU's final concentrations and accepted-step counts against micm's on
-    the same cells: the north-star criterion (every species within rtol / atol,
+    the same cells: the parity criterion (every species within rtol / atol,
     identical step counts in at least 99.9 % of cells)."""
     d = np.abs(y_gpu - y_ref)
     bound = atol + rtol * np.abs(y_ref)

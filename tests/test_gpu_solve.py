@@ -172,7 +172,8 @@ def test_c2_size_against_micm(cuda_device, method):
 
 def test_uneven_1m_workload_sample_against_micm(cuda_device):
     """8,192 cells of the 1,048,576-cell benchmark workload (half night,
-    T ~ U(200, 310) K), fused against micm: the north-star criterion."""
+    T ~ U(200, 310) K), fused against micm: every species within rtol 1e-6 /
+    atol 1e-12, identical accepted-step counts in at least 99.9 % of cells."""
     cfg = synthetic.CONFIGS["c210_uneven"]
     mech = cfg["mech"]()
     inp = synthetic.cell_inputs(mech, 8192, cfg["seed"], **cfg["inputs"])

@@ -12,7 +12,7 @@ last bit of the step-size factor pow(error, 1/order): glibc's pow rounds
 wrongly in about one call in a thousand, the GPU's pow (and the restatement's
 correctly rounded mode) round correctly.  So the GPU equals the restatement in
 its correctly rounded mode bit for bit, accepted-step counts and values at
-every output; against micm it meets the north-star criterion micm's own CUDA
+every output; against micm it meets the criterion micm's own CUDA
 Robertson test uses (values within rtol 1e-6 at every output,
 test/integration/cuda/test_cuda_analytical_rosenbrock.cpp:185-196), with the
 number of outputs at identical step counts recorded.  Tableaus that cover every
