@@ -305,7 +305,12 @@ int micmb_update_state_parameters(micmb_solver* solver, micmb_state* state);
  * Solver::PostSolveClamp (include/micm/solver/solver.hpp:133-142, 275-297,
  * include/micm/solver/rosenbrock.inl:12-304).  per_cell_status (device
  * results copied to host, may be NULL) receives MICMB_SOLVER_* per cell and
- * per_cell_steps the accepted-step count per cell. */
+ * per_cell_steps the accepted-step count per cell.  With algebraic
+ * constraints every solve starts with micm's constraint initialisation
+ * (rosenbrock.inl:407-576; over all cells of the state together under
+ * MICMB_STEP_GLOBAL, per cell under MICMB_STEP_PER_CELL), and the clamp
+ * leaves the algebraic variables as solved; the fused method takes them with
+ * per-cell step control. */
 int micmb_solve(micmb_solver* solver, micmb_state* state, double dt, int32_t method,
                 int32_t step_control, micmb_solver_stats* stats, int32_t* per_cell_status,
                 int32_t* per_cell_accepted);
