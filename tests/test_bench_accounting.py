@@ -48,3 +48,23 @@ def test_solve_bytes_and_flops_scale_with_statistics(c210):
 
 def test_job_throughput_counts_every_rank():
     assert bench.job_throughput(1000, 4, 2, 0.5) == 1000 * 4 * 2 / 0.5
+
+
+@pytest.mark.skipif(not __import__("oracle").reference_available(), reason="oracle/_ref not built")
+def test_reference_arm_prints_its_contract_line():
+    """`bench.py --impl reference` (micm on the host cores) on a small sample:
+    one JSON line with the contract's keys, its own e2e and cpu_baseline."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--cells", "2048", "--cpu-sample", "256",
+                        "--steps", "1", "--warmup", "1"], cwd=root, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "impl", "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["e2e"]["value"] == line["value"] and line["e2e"]["h2d_bytes_per_step"] == 0
+    assert line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["cores"] >= 1
