@@ -124,3 +124,15 @@ def test_cpp_constraints_on_gpu_equal_restatement(cuda_device, dae_binary, metho
         assert int(row[1]) == iters
         np.testing.assert_array_equal(np.array([float(v) for v in row[2:]]).reshape(3, 3), y)
         t = target
+
+
+def test_cpp_constraint_validation(tmp_path):
+    """micm.hpp's constraint classes and builder reject invalid constraints
+    with MicmException before any device call (CPU)."""
+    out = str(tmp_path / "constraint_errors")
+    subprocess.run(["g++", "-std=c++20", "-O1", "-I" + os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "constraint_errors.cpp"), "-o", out, "-L" + LIB_DIR,
+                    "-lmicmb", "-Wl,-rpath," + LIB_DIR], check=True)
+    r = subprocess.run([out], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.count(" ok") == 6, r.stdout
