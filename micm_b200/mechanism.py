@@ -245,7 +245,11 @@ def mechanism_from_dict(d: dict) -> Mechanism:
     helpers of this module take them; optional ``absolute_tolerance`` (one
     value or one per species; micm's builder default 1e-3 otherwise),
     ``relative_tolerance`` and ``reorder_state`` (micm's SetReorderState,
-    default true)."""
+    default true); optional ``constraints`` (micm's SetConstraints):
+    ``[{"type": "linear", "name", "algebraic_species", "terms": [[name,
+    coefficient]], "constant"}]`` or ``[{"type": "equilibrium", "name",
+    "algebraic_species", "reactants": [[name, stoichiometry]], "products":
+    [[name, stoichiometry]], "K_HLC_ref", "delta_H"?, "R"?, "T_ref"?}]``."""
     species = list(d["species"])
     index = {n: i for i, n in enumerate(species)}
     params = d.get("parameterized", [])
@@ -276,6 +280,25 @@ def mechanism_from_dict(d: dict) -> Mechanism:
             products.append((index[name], float(y)))
         m.reactions.append(Reaction(kind, [float(v) for v in rx["params"]],
                                     [reactant(n) for n in rx["reactants"]], products, rx.get("label")))
+
+    def species_index(name):
+        if name not in index:
+            raise ValueError(f"unknown constraint species '{name}'")
+        return index[name]
+
+    for c in d.get("constraints", []):
+        row = species_index(c["algebraic_species"])
+        if c["type"] == "linear":
+            m.constraints.append(linear_constraint(row, [(species_index(n), float(v)) for n, v in c["terms"]],
+                                                   float(c["constant"]), name=c.get("name", "linear")))
+        elif c["type"] == "equilibrium":
+            m.constraints.append(equilibrium_constraint(
+                row, [(species_index(n), float(v)) for n, v in c["reactants"]],
+                [(species_index(n), float(v)) for n, v in c["products"]], float(c["K_HLC_ref"]),
+                float(c.get("delta_H", 0.0)), float(c.get("R", GAS_CONSTANT)), float(c.get("T_ref", 298.15)),
+                name=c.get("name", "equilibrium")))
+        else:
+            raise ValueError(f"unknown constraint type '{c['type']}'")
     return m
 
 
@@ -306,6 +329,19 @@ def mechanism_to_dict(m: Mechanism, parameterized_names: Optional[Sequence[str]]
         out["absolute_tolerance"] = [float(v) for v in m.absolute_tolerance]
     if not m.reorder_state:
         out["reorder_state"] = False
+    constraints = []
+    for c in m.constraints:
+        terms = [[m.species[i], float(v)] for i, v in c.terms]
+        if c.kind == CONSTRAINT_LINEAR:
+            constraints.append({"type": "linear", "name": c.name, "algebraic_species": m.species[c.species],
+                                "terms": terms, "constant": float(c.params[0])})
+        else:
+            constraints.append({"type": "equilibrium", "name": c.name, "algebraic_species": m.species[c.species],
+                                "reactants": terms[:c.n_reactants], "products": terms[c.n_reactants:],
+                                "K_HLC_ref": float(c.params[0]), "delta_H": float(c.params[1]),
+                                "R": float(c.params[2]), "T_ref": float(c.params[3])})
+    if constraints:
+        out["constraints"] = constraints
     return out
 
 
