@@ -76,8 +76,20 @@ def _dae_case():
     return m, inp
 
 
+def _dae_singular_case():
+    """rank 1's cells start with the squared product at zero: dG/dF = 0, the
+    initialisation's matrix is singular there, its update infinite, and the
+    flag must reach rank 0 through the exchange (micm: InfDetected)"""
+    from dae_cases import equilibrium, equilibrium_inputs
+    m = equilibrium(2.0, True)
+    inp = equilibrium_inputs(m, 4, False, 0.2)
+    inp["concentrations"][2:, 5] = 0.0
+    return m, inp
+
+
 # kind: (case, shard sizes, tableau, dt)
-KINDS = {"kinetic": (_case, SHARDS, 4, 600.0), "dae": (_dae_case, [2, 3], 40, 10.0)}
+KINDS = {"kinetic": (_case, SHARDS, 4, 600.0), "dae": (_dae_case, [2, 3], 40, 10.0),
+         "dae_singular": (_dae_singular_case, [2, 2], 40, 10.0)}
 
 
 def _rank_main(rank, world, port, out_path, kind="kinetic"):
@@ -105,7 +117,7 @@ def _rank_main(rank, world, port, out_path, kind="kinetic"):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("kind", ["kinetic", "dae"])
+@pytest.mark.parametrize("kind", ["kinetic", "dae", "dae_singular"])
 def test_two_gloo_ranks_equal_the_single_process_solve(tmp_path, kind):
     out = str(tmp_path / "rank")
     mp.start_processes(_rank_main, args=(2, _free_port(), out, kind), nprocs=2, start_method="spawn")
@@ -115,6 +127,8 @@ def test_two_gloo_ranks_equal_the_single_process_solve(tmp_path, kind):
     y, st = oracle.Restatement(m, tableau).solve_global(inp, dt, shards=shards)
     if kind == "dae":
         assert st[9] >= 2 and st[7] == 2  # the initialisation iterated, and the solve converged
+    if kind == "dae_singular":
+        assert st[7] == 7  # InfDetected on both ranks, though only rank 1's cells are singular
     np.testing.assert_array_equal(np.concatenate([r0["y"], r1["y"]]), y)
     np.testing.assert_array_equal(r0["stats"], st)
     np.testing.assert_array_equal(r1["stats"], st)
