@@ -136,3 +136,29 @@ def test_cpp_constraint_validation(tmp_path):
     r = subprocess.run([out], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.count(" ok") == 6, r.stdout
+
+
+def test_c_abi_dae_mechanism_pattern_equals_micms(tmp_path):
+    """A DAE mechanism built through the plain C description (gcc, micmb.h
+    only): its LU-filled Jacobian pattern equals micm's for the same system
+    (micm built here, SetConstraints)."""
+    import sys
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    import oracle
+    if not oracle.reference_available():
+        pytest.skip("oracle/_ref not built")
+    from dae_cases import equilibrium
+    out = str(tmp_path / "dae_c_api")
+    subprocess.run(["gcc", "-std=c11", "-O1", "-I" + os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "dae_c_api.c"), "-o", out, "-L" + LIB_DIR, "-lmicmb",
+                    "-Wl,-rpath," + LIB_DIR], check=True)
+    r = subprocess.run([out], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    lines = r.stdout.strip().splitlines()
+    nnz = int(lines[0].split()[1])
+    pairs = np.array([[int(v) for v in l.split()] for l in lines[1:]])
+    assert len(pairs) == nnz
+    ref = oracle.Reference(equilibrium(), tableau=40)
+    np.testing.assert_array_equal(pairs[:, 0], ref.rows)
+    np.testing.assert_array_equal(pairs[:, 1], ref.cols)
