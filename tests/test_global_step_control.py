@@ -275,7 +275,7 @@ def test_gpu_two_ranks_on_host_threads_equal_two_shard_restatement(cuda_device, 
 def test_max_combine_keeps_micms_order_of_checks():
     """The encoded residual maxima of the constraint initialisation combine
     with NaN first, then +Inf, else the largest: micm checks NaN before Inf
-    (rosenbrock.inl:495-502), so any rank's NaN wins."""
+    (rosenbrock.inl:505-512, 564-571), so any rank's NaN wins."""
     nan, inf = float("nan"), float("inf")
     assert oracle.max_combine([1e-3, 2e-3]) == 2e-3
     assert oracle.max_combine([0.0, 0.0]) == 0.0
